@@ -1,0 +1,332 @@
+#!/usr/bin/env python
+"""Benchmark: PHOLD committed events/s on the 65,536-LP ring workload (local array queue).
+
+Workload (synthetic, seeded): 65,536 LPs x 64 initial events, lookahead 0.1 + Exp(1)
+float32 increments, 90% of destinations uniform within +-16 ring neighbours (self
+excluded) and 10% uniform, end time 1000.0, per-LP capacity 256, seed 7.
+One bench step = one complete run of that workload: populate the queues on the device,
+then drain safe windows until the minimum timestamp reaches the end time.
+
+  value  committed events / device time of the runs (CUDA events on the launching
+         stream, inputs already resident in HBM; the 268 MB queue array exceeds L2)
+  e2e    the same through the public C ABI with host buffers: per step the initial
+         events are copied from page-locked host memory, and the per-LP results
+         (count, checksum, order hash) are copied back
+
+`--impl reference` times the CPU port of the reference's window loop (per-LP
+std::priority_queue, all host threads) on a bounded sample of the same workload.
+
+Multi-GPU (torchrun): every rank runs its own replica (seed + rank); value = events
+of all ranks / max over ranks of the device time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(num_lps=65536, events_per_lp=64, lookahead=0.1, end_time=1000.0, seed=7, dest_mode=1,
+                ring_width=16, ring_frac=0.9)
+WORKLOAD_NAME = "phold_large_65536lp_x64_ring16_T1000"
+METRIC = "PHOLD committed events/s"
+UNIT = "events/s"
+# Algorithmic bytes: 48 B per committed event (16 B item read, 16 B child write, 16 B
+# per-LP state read-modify-write) + 4 B per LP per window (window minimum).
+BYTES_PER_EVENT = 48
+BYTES_PER_LP_WINDOW = 4
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_reference_run(cfgd, end_time, threads):
+    from oracle import oracle as O
+    c = O.make_cfg(num_lps=cfgd["num_lps"], events_per_lp=cfgd["events_per_lp"], lookahead=cfgd["lookahead"],
+                   end_time=end_time, seed=cfgd["seed"], dest_mode=cfgd["dest_mode"],
+                   ring_width=cfgd["ring_width"], ring_frac=cfgd["ring_frac"])
+    return O.phold(c, threads)
+
+
+CPU_SAMPLE_END = 12.0  # bounded sample: the first 12 of 1000 time units (~45 M events)
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    vals = []
+    committed = 0
+    for i in range(args.warmup + args.steps):
+        r = cpu_reference_run(WORKLOAD, CPU_SAMPLE_END, threads)
+        if i >= args.warmup:
+            vals.append(r["committed"] / r["seconds"])
+            committed = r["committed"]
+    v = statistics.median(vals)
+    sample = (f"end_time {CPU_SAMPLE_END} of {WORKLOAD['end_time']} ({committed} events), same LPs/population/seed; "
+              f"window-synchronous per-LP std::priority_queue port of the reference loop on {threads} threads")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * committed / v, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD_NAME, "queue": "per-LP std::priority_queue (CPU)", "sample_end_time": CPU_SAMPLE_END},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--queue", default="laq")
+    ap.add_argument("--loop", default="persistent", choices=["persistent", "plain"])
+    ap.add_argument("--end-time", type=float, default=None, help="override the workload end time (debug)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        return run_reference(args)
+
+    ws, rank, local = dist_env()
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    else:
+        os.environ.setdefault("CUDA_VISIBLE_DEVICES", os.environ.get("CUDA_VISIBLE_DEVICES", "0"))
+
+    import gpupq_b200 as G
+
+    cfgd = dict(WORKLOAD)
+    if args.end_time is not None:
+        cfgd["end_time"] = args.end_time
+    cfgd["seed"] = WORKLOAD["seed"] + rank
+    cfg = G.make_phold_config(**cfgd, queue=args.queue, capacity=256, insert_capacity=64, loop=args.loop)
+    h = G.Phold(cfg)
+
+    def barrier():
+        if dist is not None:
+            import torch
+            torch.cuda.synchronize()
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x):
+        if dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    # warm-up
+    ref_digest = None
+    for _ in range(args.warmup):
+        h.populate()
+        h.run()
+        r = h.result()
+        if r["status_code"] != 0:
+            raise SystemExit(f"run failed: {r}")
+        ref_digest = (r["digest"], r["committed"])
+
+    barrier()
+    sampler = ClockSampler(local if ws > 1 else 0)
+    sampler.start()
+    t_wall0 = time.perf_counter()
+    dev_ms = 0.0
+    committed = 0
+    windows = 0
+    for _ in range(args.steps):
+        h.populate()
+        h.run()
+        r = h.result()
+        if r["status_code"] != 0 or (r["digest"], r["committed"]) != ref_digest:
+            raise SystemExit(f"run failed or not reproducible: {r}")
+        dev_ms += r["elapsed_ms"]
+        committed += r["committed"]
+        windows += r["steps"]
+    barrier()
+    t_wall = time.perf_counter() - t_wall0
+    clocks = sampler.stop()
+    info = h.launch_info()
+
+    dev_ms_max = max_over_ranks(dev_ms)
+    committed_all = sum_over_ranks(committed)
+    value = committed_all / (dev_ms_max / 1e3)
+    ms_per_step = dev_ms_max / args.steps
+
+    # roofline of the dominant kernel (the persistent window loop = the whole run)
+    peak, peak_kind = load_peaks()
+    per_run_bytes = BYTES_PER_EVENT * (committed / args.steps) + BYTES_PER_LP_WINDOW * cfgd["num_lps"] * (windows / args.steps)
+    achieved = per_run_bytes / (dev_ms / args.steps / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        try:
+            t = json.load(open(tp))
+            key = f"{args.queue}_{args.loop}"
+            if key in t:
+                traffic = t[key]["dram_bytes_per_event"] * committed / args.steps
+        except Exception:
+            traffic = None
+
+    # end-to-end through the C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        n = cfgd["num_lps"] * cfgd["events_per_lp"]
+        pin_ev = G.PinnedArray(n, G.ITEM_DTYPE)
+        pin_ev.array[:] = G.initial_events(cfg)
+        pc = G.PinnedArray(cfgd["num_lps"], np.uint32)
+        ps = G.PinnedArray(cfgd["num_lps"], np.uint64)
+        po = G.PinnedArray(cfgd["num_lps"], np.uint64)
+        h.populate(pin_ev.array)
+        h.run()
+        h.result()
+        barrier()
+        t0 = time.perf_counter()
+        ecommitted = 0
+        for _ in range(args.steps):
+            h.populate(pin_ev.array)
+            h.run()
+            r = h.result()
+            h.lp_stats_into(pc.array, ps.array, po.array)
+            ecommitted += r["committed"]
+            if (r["digest"], r["committed"]) != ref_digest:
+                raise SystemExit("e2e run differs from the device-resident run")
+        barrier()
+        e_wall = max_over_ranks(time.perf_counter() - t0)
+        e2e = {"value": sum_over_ranks(ecommitted) / e_wall, "unit": UNIT,
+               "h2d_bytes_per_step": int(n * G.ITEM_DTYPE.itemsize),
+               "d2h_bytes_per_step": int(cfgd["num_lps"] * (4 + 8 + 8) + 64)}
+        for p in (pin_ev, pc, ps, po):
+            p.free()
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rr = cpu_reference_run(WORKLOAD, CPU_SAMPLE_END, threads)
+        cpu = {"value": rr["committed"] / rr["seconds"], "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"end_time {CPU_SAMPLE_END} of 1000 ({rr['committed']} events); window-synchronous per-LP "
+                         f"std::priority_queue port of the reference loop on {threads} threads"}
+
+    h.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD_NAME, "queue": args.queue, "loop": args.loop,
+                       "end_time": cfgd["end_time"], "events_per_run": committed / args.steps,
+                       "windows_per_run": windows / args.steps,
+                       "l2": "inputs larger than L2 (268 MB queue array)",
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": f"{peak_kind} hbm_gbs", "kernel": f"phold_laq_{args.loop}",
+                         "algorithmic_bytes_per_run": per_run_bytes},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(args.steps * info["launches_per_run"]),
+            "clocks": clocks,
+            "wall_s_timed": t_wall,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,385 @@
+"""gpupq_b200 -- B200-native rebuild of GPUPQ's priority-queue hot path.
+
+Python binding of libgpq.so (ctypes over the C ABI declared in include/gpq.h).  The
+compute path is the CUDA library; there is no Python or CPU fallback: importing the
+binding succeeds without a GPU, but every call that needs the device fails loudly if
+the library is missing or no GPU is present.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import build as _build
+
+__all__ = [
+    "GpqError", "ITEM_DTYPE", "PholdConfig", "PholdResult", "Phold", "lib", "presets",
+    "QUEUE_LAQ", "QUEUE_GAQ", "QUEUE_HQ", "QUEUE_LHQ", "QUEUE_LSQ", "LOOP_PLAIN", "LOOP_PERSISTENT",
+    "DEST_UNIFORM", "DEST_RING", "ring_threshold",
+]
+
+QUEUE_LAQ, QUEUE_GAQ, QUEUE_HQ, QUEUE_LHQ, QUEUE_LSQ = range(5)
+QUEUE_NAMES = {"laq": QUEUE_LAQ, "gaq": QUEUE_GAQ, "hq": QUEUE_HQ, "lhq": QUEUE_LHQ, "lsq": QUEUE_LSQ}
+LOOP_PLAIN, LOOP_PERSISTENT = 0, 1
+DEST_UNIFORM, DEST_RING = 0, 1
+
+STATUS = {
+    0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "queue full", 4: "insert buffer full",
+    5: "device wait timed out", 6: "out of device memory", 7: "unsupported", 8: "not ready",
+}
+
+ITEM_DTYPE = np.dtype([("ts", "<f4"), ("lp", "<u4"), ("id", "<u4"), ("aux", "<u4")])
+
+
+class GpqError(RuntimeError):
+    def __init__(self, status, where, detail=""):
+        self.status = status
+        super().__init__(f"{where}: {STATUS.get(status, status)} ({status}) {detail}".strip())
+
+
+class GpqItem(ctypes.Structure):
+    _fields_ = [("ts", ctypes.c_float), ("lp", ctypes.c_uint32), ("id", ctypes.c_uint32), ("aux", ctypes.c_uint32)]
+
+
+class PholdConfig(ctypes.Structure):
+    _fields_ = [
+        ("seed", ctypes.c_uint64),
+        ("num_lps", ctypes.c_uint32),
+        ("events_per_lp", ctypes.c_uint32),
+        ("lookahead", ctypes.c_float),
+        ("end_time", ctypes.c_float),
+        ("dest_mode", ctypes.c_uint32),
+        ("ring_width", ctypes.c_uint32),
+        ("ring_threshold", ctypes.c_uint32),
+        ("queue_kind", ctypes.c_uint32),
+        ("capacity", ctypes.c_uint32),
+        ("insert_capacity", ctypes.c_uint32),
+        ("loop_mode", ctypes.c_uint32),
+        ("block_threads", ctypes.c_uint32),
+        ("ctas_per_sm", ctypes.c_uint32),
+        ("max_steps", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 4),
+    ]
+
+
+class PholdResult(ctypes.Structure):
+    _fields_ = [
+        ("committed", ctypes.c_uint64),
+        ("steps", ctypes.c_uint64),
+        ("pending", ctypes.c_uint64),
+        ("pending_csum", ctypes.c_uint64),
+        ("digest", ctypes.c_uint64),
+        ("final_min", ctypes.c_float),
+        ("elapsed_ms", ctypes.c_float),
+        ("status", ctypes.c_int32),
+        ("reserved", ctypes.c_uint32 * 3),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+_LIB = None
+
+# Exported symbols and their ctypes signatures (kept in step with include/gpq.h).
+_VP = ctypes.c_void_p
+_SIGS = {
+    "gpq_status_string": ([ctypes.c_int], ctypes.c_char_p),
+    "gpq_version": ([], ctypes.c_char_p),
+    "gpq_last_error": ([], ctypes.c_char_p),
+    "gpq_set_spin_limit": ([ctypes.c_uint64], ctypes.c_int),
+    "gpq_phold_create": ([ctypes.POINTER(PholdConfig), ctypes.POINTER(_VP)], ctypes.c_int),
+    "gpq_phold_destroy": ([_VP], ctypes.c_int),
+    "gpq_phold_populate": ([_VP, _VP, ctypes.c_uint64, _VP], ctypes.c_int),
+    "gpq_phold_run": ([_VP, _VP], ctypes.c_int),
+    "gpq_phold_step": ([_VP, ctypes.c_uint32, ctypes.POINTER(ctypes.c_int), _VP], ctypes.c_int),
+    "gpq_phold_result_get": ([_VP, ctypes.POINTER(PholdResult), _VP], ctypes.c_int),
+    "gpq_phold_lp_stats": ([_VP, _VP, _VP, _VP, _VP], ctypes.c_int),
+    "gpq_phold_initial_events": ([ctypes.POINTER(PholdConfig), _VP, ctypes.c_uint64], ctypes.c_int),
+    "gpq_phold_children": ([ctypes.POINTER(PholdConfig), _VP, _VP, ctypes.c_uint64], ctypes.c_int),
+    "gpq_phold_launch_info": ([_VP, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32),
+                               ctypes.POINTER(ctypes.c_uint32)], ctypes.c_int),
+    "gpq_host_alloc": ([ctypes.c_uint64, ctypes.POINTER(_VP)], ctypes.c_int),
+    "gpq_host_free": ([_VP], ctypes.c_int),
+    "gpq_queue_create": ([ctypes.c_void_p, ctypes.POINTER(_VP)], ctypes.c_int),
+    "gpq_queue_destroy": ([_VP], ctypes.c_int),
+    "gpq_queue_insert": ([_VP, _VP, ctypes.c_uint64, ctypes.c_int, _VP], ctypes.c_int),
+    "gpq_queue_pre": ([_VP, _VP], ctypes.c_int),
+    "gpq_queue_post": ([_VP, _VP], ctypes.c_int),
+    "gpq_queue_post_init": ([_VP, _VP], ctypes.c_int),
+    "gpq_queue_get_min": ([_VP, ctypes.POINTER(ctypes.c_float), _VP], ctypes.c_int),
+    "gpq_queue_dequeue": ([_VP, ctypes.c_float, ctypes.c_uint32, _VP, ctypes.c_uint64,
+                           ctypes.POINTER(ctypes.c_uint64), _VP], ctypes.c_int),
+    "gpq_queue_length": ([_VP, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32), _VP], ctypes.c_int),
+    "gpq_queue_clear": ([_VP, ctypes.c_uint32, _VP], ctypes.c_int),
+    "gpq_queue_dump": ([_VP, ctypes.c_uint32, _VP, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64), _VP],
+                       ctypes.c_int),
+    "gpq_queue_counts": ([_VP, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64), _VP],
+                         ctypes.c_int),
+}
+
+
+def lib_path():
+    return _build.LIB
+
+
+def lib():
+    """Load libgpq.so (building it first if the sources are newer).  Raises if it cannot."""
+    global _LIB
+    if _LIB is None:
+        path = _build.LIB
+        if not _build.up_to_date():
+            try:
+                path = _build.build()
+            except Exception as e:  # no nvcc on this machine: use the shipped library if any
+                if not os.path.exists(path):
+                    raise RuntimeError(f"libgpq.so is missing and could not be built: {e}") from e
+        L = ctypes.CDLL(path)
+        for name, (argtypes, restype) in _SIGS.items():
+            f = getattr(L, name, None)
+            if f is not None:
+                f.argtypes = argtypes
+                f.restype = restype
+        _LIB = L
+    return _LIB
+
+
+def last_error():
+    return lib().gpq_last_error().decode(errors="replace")
+
+
+def check(status, where):
+    if status != 0:
+        raise GpqError(status, where, last_error())
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def ring_threshold(frac: float) -> int:
+    """Probability -> 32-bit threshold floor(frac * 2^32), computed in double."""
+    return min(int(frac * 4294967296.0), 0xFFFFFFFF)
+
+
+def presets():
+    """The named workloads (synthetic, seeded).
+
+    phold_plain: 1024 LPs x 16 events, lookahead 1.0, end 100, uniform destinations, seed 42.
+    phold_large: 65,536 LPs x 64 events, lookahead 0.1, end 1000, 90% ring +-16 / 10% uniform,
+                 per-LP capacity 256, seed 7.
+    """
+    return {
+        "phold_plain": dict(num_lps=1024, events_per_lp=16, lookahead=1.0, end_time=100.0, seed=42,
+                            dest_mode=DEST_UNIFORM, capacity=256, insert_capacity=64),
+        "phold_large": dict(num_lps=65536, events_per_lp=64, lookahead=0.1, end_time=1000.0, seed=7,
+                            dest_mode=DEST_RING, ring_width=16, ring_frac=0.9, capacity=256,
+                            insert_capacity=64),
+    }
+
+
+def make_phold_config(num_lps, events_per_lp, lookahead, end_time, seed, dest_mode=DEST_UNIFORM,
+                      ring_width=16, ring_frac=0.9, queue="laq", capacity=256, insert_capacity=64,
+                      loop="persistent", block_threads=0, ctas_per_sm=0, max_steps=0):
+    c = PholdConfig()
+    c.seed = seed
+    c.num_lps = num_lps
+    c.events_per_lp = events_per_lp
+    c.lookahead = lookahead
+    c.end_time = end_time
+    c.dest_mode = dest_mode
+    c.ring_width = ring_width if dest_mode == DEST_RING else 0
+    c.ring_threshold = ring_threshold(ring_frac) if dest_mode == DEST_RING else 0
+    c.queue_kind = QUEUE_NAMES[queue] if isinstance(queue, str) else int(queue)
+    c.capacity = capacity
+    c.insert_capacity = insert_capacity
+    c.loop_mode = {"plain": LOOP_PLAIN, "persistent": LOOP_PERSISTENT}[loop] if isinstance(loop, str) else int(loop)
+    c.block_threads = block_threads
+    c.ctas_per_sm = ctas_per_sm
+    c.max_steps = max_steps
+    return c
+
+
+class Phold:
+    """One PHOLD instance on the device (the reference's des_init/des_run/des_finish with
+    the PHOLD model, src/des.cu:74-221, src/phold.cu:124-192)."""
+
+    def __init__(self, cfg: PholdConfig):
+        self.cfg = cfg
+        self._h = ctypes.c_void_p()
+        check(lib().gpq_phold_create(ctypes.byref(cfg), ctypes.byref(self._h)), "gpq_phold_create")
+
+    def close(self):
+        if self._h:
+            lib().gpq_phold_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def populate(self, initial=None, stream=None):
+        if initial is not None:
+            initial = np.ascontiguousarray(initial, dtype=ITEM_DTYPE)
+            check(lib().gpq_phold_populate(self._h, _ptr(initial), len(initial), stream), "gpq_phold_populate")
+        else:
+            check(lib().gpq_phold_populate(self._h, None, 0, stream), "gpq_phold_populate")
+
+    def run(self, stream=None):
+        check(lib().gpq_phold_run(self._h, stream), "gpq_phold_run")
+
+    def step(self, n, stream=None):
+        done = ctypes.c_int(0)
+        check(lib().gpq_phold_step(self._h, n, ctypes.byref(done), stream), "gpq_phold_step")
+        return bool(done.value)
+
+    def result(self, stream=None):
+        r = PholdResult()
+        st = lib().gpq_phold_result_get(self._h, ctypes.byref(r), stream)
+        d = r.as_dict()
+        d["status_code"] = st
+        return d
+
+    def launch_info(self):
+        g, b, n = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        check(lib().gpq_phold_launch_info(self._h, ctypes.byref(g), ctypes.byref(b), ctypes.byref(n)),
+              "gpq_phold_launch_info")
+        return {"grid": g.value, "block": b.value, "launches_per_run": n.value}
+
+    def lp_stats_into(self, count, csum, ohash, stream=None):
+        check(lib().gpq_phold_lp_stats(self._h, _ptr(count), _ptr(csum), _ptr(ohash), stream), "gpq_phold_lp_stats")
+
+    def lp_stats(self, stream=None):
+        L = self.cfg.num_lps
+        count = np.zeros(L, np.uint32)
+        csum = np.zeros(L, np.uint64)
+        ohash = np.zeros(L, np.uint64)
+        check(lib().gpq_phold_lp_stats(self._h, _ptr(count), _ptr(csum), _ptr(ohash), stream), "gpq_phold_lp_stats")
+        return {"count": count, "csum": csum, "ohash": ohash}
+
+
+def initial_events(cfg: PholdConfig):
+    n = cfg.num_lps * cfg.events_per_lp
+    out = np.zeros(n, ITEM_DTYPE)
+    check(lib().gpq_phold_initial_events(ctypes.byref(cfg), _ptr(out), n), "gpq_phold_initial_events")
+    return out
+
+
+def children(cfg: PholdConfig, events):
+    events = np.ascontiguousarray(events, dtype=ITEM_DTYPE)
+    out = np.zeros(len(events), ITEM_DTYPE)
+    check(lib().gpq_phold_children(ctypes.byref(cfg), _ptr(events), _ptr(out), len(events)), "gpq_phold_children")
+    return out
+
+
+class QueueConfig(ctypes.Structure):
+    _fields_ = [
+        ("kind", ctypes.c_uint32),
+        ("num_lps", ctypes.c_uint32),
+        ("capacity", ctypes.c_uint32),
+        ("insert_capacity", ctypes.c_uint32),
+        ("node_size", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 3),
+    ]
+
+
+class Queue:
+    """A queue object (the reference's host queue API, src/queue.h:86-115)."""
+
+    def __init__(self, kind, num_lps, capacity=0, insert_capacity=0, node_size=0):
+        c = QueueConfig()
+        c.kind = QUEUE_NAMES[kind] if isinstance(kind, str) else int(kind)
+        c.num_lps = num_lps
+        c.capacity = capacity
+        c.insert_capacity = insert_capacity
+        c.node_size = node_size
+        self.num_lps = num_lps
+        self._h = ctypes.c_void_p()
+        check(lib().gpq_queue_create(ctypes.byref(c), ctypes.byref(self._h)), "gpq_queue_create")
+
+    def close(self):
+        if self._h:
+            lib().gpq_queue_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def insert(self, items):
+        items = np.ascontiguousarray(items, dtype=ITEM_DTYPE)
+        check(lib().gpq_queue_insert(self._h, _ptr(items), len(items), 0, None), "gpq_queue_insert")
+
+    def pre(self):
+        check(lib().gpq_queue_pre(self._h, None), "gpq_queue_pre")
+
+    def post(self):
+        check(lib().gpq_queue_post(self._h, None), "gpq_queue_post")
+
+    def post_init(self):
+        check(lib().gpq_queue_post_init(self._h, None), "gpq_queue_post_init")
+
+    def get_min(self):
+        v = ctypes.c_float()
+        check(lib().gpq_queue_get_min(self._h, ctypes.byref(v), None), "gpq_queue_get_min")
+        return v.value
+
+    def dequeue(self, bound, max_per_lp=0, capacity=None):
+        cap = capacity if capacity is not None else 1 << 20
+        out = np.zeros(cap, ITEM_DTYPE)
+        n = ctypes.c_uint64()
+        check(lib().gpq_queue_dequeue(self._h, bound, max_per_lp, _ptr(out), cap, ctypes.byref(n), None),
+              "gpq_queue_dequeue")
+        return out[: n.value].copy()
+
+    def length(self, lp):
+        v = ctypes.c_uint32()
+        check(lib().gpq_queue_length(self._h, lp, ctypes.byref(v), None), "gpq_queue_length")
+        return v.value
+
+    def clear(self, lp):
+        check(lib().gpq_queue_clear(self._h, lp, None), "gpq_queue_clear")
+
+    def dump(self, lp, capacity=1 << 20):
+        out = np.zeros(capacity, ITEM_DTYPE)
+        n = ctypes.c_uint64()
+        check(lib().gpq_queue_dump(self._h, lp, _ptr(out), capacity, ctypes.byref(n), None), "gpq_queue_dump")
+        return out[: n.value].copy()
+
+    def counts(self):
+        a, b = ctypes.c_uint64(), ctypes.c_uint64()
+        check(lib().gpq_queue_counts(self._h, ctypes.byref(a), ctypes.byref(b), None), "gpq_queue_counts")
+        return a.value, b.value
+
+
+class PinnedArray:
+    """A numpy array over page-locked host memory (gpq_host_alloc)."""
+
+    def __init__(self, n, dtype):
+        dtype = np.dtype(dtype)
+        self._p = ctypes.c_void_p()
+        check(lib().gpq_host_alloc(n * dtype.itemsize, ctypes.byref(self._p)), "gpq_host_alloc")
+        buf = (ctypes.c_char * (n * dtype.itemsize)).from_address(self._p.value)
+        self.array = np.frombuffer(buf, dtype=dtype, count=n)
+
+    def free(self):
+        if self._p:
+            self.array = None
+            lib().gpq_host_free(self._p)
+            self._p = ctypes.c_void_p()

@@ -1,0 +1,38 @@
+// Host-side helpers shared by the C-ABI implementation files.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+
+#include "gpq.h"
+
+namespace gpq {
+
+void set_last_error(const char* fmt, ...);
+uint64_t spin_limit();
+
+inline cudaStream_t as_stream(void* s, cudaStream_t fallback) {
+  return s ? reinterpret_cast<cudaStream_t>(s) : fallback;
+}
+
+}  // namespace gpq
+
+#define GPQ_CUDA_TRY(expr)                                                                      \
+  do {                                                                                          \
+    cudaError_t e_ = (expr);                                                                    \
+    if (e_ != cudaSuccess) {                                                                    \
+      gpq::set_last_error("%s:%d: %s -> %s", __FILE__, __LINE__, #expr, cudaGetErrorString(e_)); \
+      return (e_ == cudaErrorMemoryAllocation) ? GPQ_ERR_NOMEM : GPQ_ERR_CUDA;                 \
+    }                                                                                           \
+  } while (0)
+
+#define GPQ_CHECK_ARG(cond, msg)             \
+  do {                                       \
+    if (!(cond)) {                           \
+      gpq::set_last_error("invalid: %s", msg); \
+      return GPQ_ERR_INVALID;                \
+    }                                        \
+  } while (0)

@@ -1,0 +1,410 @@
+// PHOLD engine: C-ABI implementation (host side).
+//
+// Replaces the reference's DES driver and PHOLD model host code:
+//   des_init / des_run / des_finish  src/des.cu:74-221
+//   model_init / model_handle_next / model_get_events  src/phold.cu:124-192
+// The host owns every device buffer through the handle (the reference keeps them in
+// static __device__ globals, src/local_array_queue.cu:38-50).
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "host_common.h"
+#include "phold_kernels.cuh"
+
+namespace {
+
+constexpr uint32_t kDefaultBlock = 256;
+
+struct DevBuf {
+  void* p = nullptr;
+  ~DevBuf() { if (p) cudaFree(p); }
+};
+
+bool is_pow2(uint32_t x) { return x && !(x & (x - 1)); }
+uint32_t ilog2(uint32_t x) { uint32_t r = 0; while ((1u << r) < x) ++r; return r; }
+
+}  // namespace
+
+struct gpq_phold {
+  gpq_phold_config cfg{};
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t own = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  // device memory (one allocation per array)
+  gpq_item* ring = nullptr;
+  uint32_t* rd = nullptr;
+  uint32_t* wr = nullptr;
+  gpq_item* ibuf = nullptr;
+  uint32_t* icnt = nullptr;
+  uint32_t* count = nullptr;
+  unsigned long long* csum = nullptr;
+  unsigned long long* ohash = nullptr;
+  PholdCtrl* ctrl = nullptr;
+  PholdAcc* acc = nullptr;
+  gpq_item* staging = nullptr;  // host-provided initial events
+  uint64_t staging_n = 0;
+
+  // pinned host mirror of the control block (plain loop reads it every window)
+  PholdCtrl* h_ctrl = nullptr;
+
+  uint32_t cap_log2 = 0;
+  uint32_t block = kDefaultBlock;
+  uint32_t phase = 0;  // next window (host view; plain loop)
+  uint32_t last_grid = 0;  // CTAs of the last persistent launch
+  bool populated = false;
+  bool finalized = false;
+  float elapsed_ms = 0.f;
+
+  PholdDev dev() const {
+    PholdDev d;
+    d.p.seed = cfg.seed;
+    d.p.num_lps = cfg.num_lps;
+    d.p.dest_mode = cfg.dest_mode;
+    d.p.ring_width = cfg.ring_width;
+    d.p.ring_threshold = cfg.ring_threshold;
+    d.p.lookahead = cfg.lookahead;
+    d.p.end_time = cfg.end_time;
+    d.L = cfg.num_lps;
+    d.count = count;
+    d.csum = csum;
+    d.ohash = ohash;
+    d.ctrl = ctrl;
+    d.spin_limit = gpq::spin_limit();
+    return d;
+  }
+  LaqDev laq() const { return LaqDev{ring, rd, wr, cap_log2}; }
+  InsDev ins() const { return InsDev{ibuf, icnt, cfg.insert_capacity}; }
+  size_t window_smem() const { return (size_t)(block / 32) * laq_warp_smem_bytes(cfg.insert_capacity); }
+
+  ~gpq_phold() {
+    for (void* p : {(void*)ring, (void*)rd, (void*)wr, (void*)ibuf, (void*)icnt, (void*)count, (void*)csum,
+                    (void*)ohash, (void*)ctrl, (void*)acc, (void*)staging})
+      if (p) cudaFree(p);
+    if (h_ctrl) cudaFreeHost(h_ctrl);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (own) cudaStreamDestroy(own);
+  }
+};
+
+namespace {
+
+gpq_phold_params params_of(const gpq_phold_config& c) {
+  gpq_phold_params p;
+  p.seed = c.seed;
+  p.num_lps = c.num_lps;
+  p.dest_mode = c.dest_mode;
+  p.ring_width = c.ring_width;
+  p.ring_threshold = c.ring_threshold;
+  p.lookahead = c.lookahead;
+  p.end_time = c.end_time;
+  return p;
+}
+
+gpq_status validate(const gpq_phold_config* c) {
+  GPQ_CHECK_ARG(c, "config is NULL");
+  GPQ_CHECK_ARG(c->num_lps > 0 && c->num_lps <= (1u << 24), "num_lps must be in [1, 2^24]");
+  GPQ_CHECK_ARG(c->events_per_lp > 0, "events_per_lp must be > 0");
+  GPQ_CHECK_ARG((uint64_t)c->num_lps * c->events_per_lp <= 0xFFFFFFFFull, "num_lps * events_per_lp must fit 32-bit ids");
+  GPQ_CHECK_ARG(c->lookahead > 0.f && c->lookahead < 1e30f, "lookahead must be positive and finite");
+  GPQ_CHECK_ARG(c->end_time >= 0.f && c->end_time < 1e30f, "end_time must be finite and >= 0");
+  GPQ_CHECK_ARG(c->dest_mode == GPQ_DEST_UNIFORM || c->dest_mode == GPQ_DEST_RING, "dest_mode");
+  if (c->dest_mode == GPQ_DEST_RING)
+    GPQ_CHECK_ARG(c->ring_width >= 1 && 2ull * c->ring_width < c->num_lps, "ring_width must satisfy 1 <= 2w < num_lps");
+  GPQ_CHECK_ARG(c->loop_mode == GPQ_LOOP_PLAIN || c->loop_mode == GPQ_LOOP_PERSISTENT, "loop_mode");
+  GPQ_CHECK_ARG(c->queue_kind <= GPQ_QUEUE_LSQ, "queue_kind");
+  return GPQ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+gpq_status gpq_phold_create(const gpq_phold_config* cfg_in, gpq_phold** out) {
+  GPQ_CHECK_ARG(out, "out is NULL");
+  *out = nullptr;
+  gpq_status st = validate(cfg_in);
+  if (st != GPQ_OK) return st;
+  gpq_phold_config c = *cfg_in;
+  if (c.queue_kind != GPQ_QUEUE_LAQ) {
+    gpq::set_last_error("queue kind %u not available in the PHOLD engine", c.queue_kind);
+    return GPQ_ERR_UNSUPPORTED;
+  }
+  if (c.capacity == 0) c.capacity = 256;
+  if (c.insert_capacity == 0) c.insert_capacity = 64;
+  GPQ_CHECK_ARG(is_pow2(c.capacity) && c.capacity >= 32 && c.capacity <= (1u << 16),
+                "LAQ capacity must be a power of two in [32, 65536]");
+  GPQ_CHECK_ARG(c.insert_capacity >= 1 && c.insert_capacity <= 1024, "insert_capacity must be in [1, 1024]");
+  GPQ_CHECK_ARG(c.events_per_lp <= c.capacity, "events_per_lp must not exceed capacity");
+  GPQ_CHECK_ARG(c.events_per_lp <= 2048, "events_per_lp must be <= 2048");
+  if (c.block_threads == 0) c.block_threads = kDefaultBlock;
+  GPQ_CHECK_ARG(c.block_threads % 32 == 0 && c.block_threads >= 32 && c.block_threads <= 1024,
+                "block_threads must be a multiple of 32 in [32, 1024]");
+
+  gpq_phold* h = new (std::nothrow) gpq_phold();
+  if (!h) return GPQ_ERR_NOMEM;
+  h->cfg = c;
+  h->cap_log2 = ilog2(c.capacity);
+  h->block = c.block_threads;
+  auto fail = [&](gpq_status s) { delete h; return s; };
+#define TRY(expr)                                   \
+  do {                                              \
+    cudaError_t e_ = (expr);                        \
+    if (e_ != cudaSuccess) {                        \
+      gpq::set_last_error("%s -> %s", #expr, cudaGetErrorString(e_)); \
+      return fail(e_ == cudaErrorMemoryAllocation ? GPQ_ERR_NOMEM : GPQ_ERR_CUDA); \
+    }                                               \
+  } while (0)
+  TRY(cudaGetDevice(&h->device));
+  TRY(cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device));
+  TRY(cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking));
+  TRY(cudaEventCreate(&h->ev0));
+  TRY(cudaEventCreate(&h->ev1));
+  const size_t L = c.num_lps;
+  TRY(cudaMalloc(&h->ring, (L << h->cap_log2) * sizeof(gpq_item)));
+  TRY(cudaMalloc(&h->rd, L * sizeof(uint32_t)));
+  TRY(cudaMalloc(&h->wr, L * sizeof(uint32_t)));
+  TRY(cudaMalloc(&h->ibuf, 2 * L * c.insert_capacity * sizeof(gpq_item)));
+  TRY(cudaMalloc(&h->icnt, 2 * L * sizeof(uint32_t)));
+  TRY(cudaMalloc(&h->count, L * sizeof(uint32_t)));
+  TRY(cudaMalloc(&h->csum, L * sizeof(unsigned long long)));
+  TRY(cudaMalloc(&h->ohash, L * sizeof(unsigned long long)));
+  TRY(cudaMalloc(&h->ctrl, sizeof(PholdCtrl)));
+  TRY(cudaMalloc(&h->acc, sizeof(PholdAcc)));
+  TRY(cudaMallocHost(&h->h_ctrl, sizeof(PholdCtrl)));
+  const size_t smem = h->window_smem();
+  TRY(cudaFuncSetAttribute(phold_laq_window, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  TRY(cudaFuncSetAttribute(phold_laq_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+#undef TRY
+  *out = h;
+  return GPQ_OK;
+}
+
+gpq_status gpq_phold_destroy(gpq_phold* h) {
+  if (!h) return GPQ_ERR_INVALID;
+  cudaStreamSynchronize(h->own);
+  delete h;
+  return GPQ_OK;
+}
+
+gpq_status gpq_phold_populate(gpq_phold* h, const gpq_item* initial, uint64_t n, void* stream) {
+  GPQ_CHECK_ARG(h, "handle is NULL");
+  cudaStream_t st = gpq::as_stream(stream, h->own);
+  const gpq_phold_config& c = h->cfg;
+  const size_t L = c.num_lps;
+  const gpq_item* src = nullptr;
+  if (initial) {
+    GPQ_CHECK_ARG(n == (uint64_t)L * c.events_per_lp, "initial must hold num_lps * events_per_lp items");
+    if (h->staging_n < n) {
+      if (h->staging) cudaFree(h->staging);
+      h->staging = nullptr;
+      h->staging_n = 0;
+      GPQ_CUDA_TRY(cudaMalloc(&h->staging, n * sizeof(gpq_item)));
+      h->staging_n = n;
+    }
+    GPQ_CUDA_TRY(cudaMemcpyAsync(h->staging, initial, n * sizeof(gpq_item), cudaMemcpyHostToDevice, st));
+    src = h->staging;
+  }
+  PholdCtrl init{};
+  for (int i = 0; i < 3; ++i) { init.mins[i] = kInfBits; init.errs[i] = 0; }
+  *h->h_ctrl = init;
+  GPQ_CUDA_TRY(cudaMemcpyAsync(h->ctrl, h->h_ctrl, sizeof(PholdCtrl), cudaMemcpyHostToDevice, st));
+  GPQ_CUDA_TRY(cudaMemsetAsync(h->icnt, 0, 2 * L * sizeof(uint32_t), st));
+  const uint32_t wpb = 4;
+  const size_t smem = (size_t)wpb * c.events_per_lp * (sizeof(gpq_item) + sizeof(uint64_t));
+  GPQ_CUDA_TRY(cudaFuncSetAttribute(phold_laq_populate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const uint32_t grid = (uint32_t)((L + wpb - 1) / wpb);
+  phold_laq_populate<<<grid, wpb * 32, smem, st>>>(h->dev(), h->laq(), c.events_per_lp, src);
+  GPQ_CUDA_TRY(cudaGetLastError());
+  h->phase = 0;
+  h->populated = true;
+  h->finalized = false;
+  h->elapsed_ms = 0.f;
+  return GPQ_OK;
+}
+
+static gpq_status run_plain(gpq_phold* h, uint32_t nsteps, int* done, cudaStream_t st) {
+  const gpq_phold_config& c = h->cfg;
+  const uint32_t wpb = h->block / 32;
+  const uint32_t grid = (uint32_t)((c.num_lps + wpb - 1) / wpb);
+  const size_t smem = h->window_smem();
+  const PholdDev d = h->dev();
+  const LaqDev q = h->laq();
+  const InsDev ib = h->ins();
+  uint32_t executed = 0;
+  if (done) *done = 0;
+  // des_run loop: read the window minimum (D2H) -> run the window -> repeat.
+  for (;;) {
+    if (nsteps && executed >= nsteps) break;
+    if (c.max_steps && h->phase >= c.max_steps) { if (done) *done = 1; break; }
+    GPQ_CUDA_TRY(cudaMemcpyAsync(h->h_ctrl, h->ctrl, sizeof(PholdCtrl), cudaMemcpyDeviceToHost, st));
+    GPQ_CUDA_TRY(cudaStreamSynchronize(st));
+    const float m = gpq_u2f(h->h_ctrl->mins[h->phase % 3]);
+    if (h->h_ctrl->err != 0 || h->h_ctrl->errs[h->phase % 3] != 0 || !(m < c.end_time)) {
+      if (done) *done = 1;
+      break;
+    }
+    phold_laq_window<<<grid, h->block, smem, st>>>(d, q, ib, h->phase);
+    GPQ_CUDA_TRY(cudaGetLastError());
+    ++h->phase;
+    ++executed;
+  }
+  return GPQ_OK;
+}
+
+static gpq_status run_persistent(gpq_phold* h, cudaStream_t st) {
+  const gpq_phold_config& c = h->cfg;
+  const size_t smem = h->window_smem();
+  int per_sm = 0;
+  GPQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, phold_laq_persistent, (int)h->block, smem));
+  if (per_sm <= 0) {
+    gpq::set_last_error("persistent kernel does not fit on an SM (block %u, smem %zu)", h->block, smem);
+    return GPQ_ERR_INVALID;
+  }
+  if (c.ctas_per_sm) per_sm = std::min<int>(per_sm, (int)c.ctas_per_sm);
+  uint32_t grid = (uint32_t)(per_sm * h->num_sms);
+  const uint32_t wpb = h->block / 32;
+  const uint32_t need = (uint32_t)((c.num_lps + wpb - 1) / wpb);
+  grid = std::min(grid, std::max(need, 1u));
+  GPQ_CUDA_TRY(cudaMemsetAsync(&h->ctrl->bar, 0, sizeof(unsigned long long), st));
+  PholdDev d = h->dev();
+  LaqDev q = h->laq();
+  InsDev ib = h->ins();
+  uint32_t s0 = h->phase;
+  uint32_t maxs = c.max_steps ? (c.max_steps > s0 ? c.max_steps - s0 : 0) : 0;
+  if (c.max_steps && maxs == 0) return GPQ_OK;
+  void* args[] = {&d, &q, &ib, &s0, &maxs};
+  GPQ_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)phold_laq_persistent, dim3(grid), dim3(h->block), args, smem, st));
+  h->last_grid = grid;
+  return GPQ_OK;
+}
+
+// After a persistent launch: the device recorded the next window index in ctrl->phase.
+static gpq_status sync_phase(gpq_phold* h, cudaStream_t st) {
+  GPQ_CUDA_TRY(cudaMemcpyAsync(&h->h_ctrl->phase, &h->ctrl->phase, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  GPQ_CUDA_TRY(cudaStreamSynchronize(st));
+  h->phase = h->h_ctrl->phase;
+  return GPQ_OK;
+}
+
+gpq_status gpq_phold_run(gpq_phold* h, void* stream) {
+  GPQ_CHECK_ARG(h, "handle is NULL");
+  if (!h->populated) { gpq::set_last_error("gpq_phold_run before gpq_phold_populate"); return GPQ_ERR_NOT_READY; }
+  cudaStream_t st = gpq::as_stream(stream, h->own);
+  h->finalized = false;
+  GPQ_CUDA_TRY(cudaEventRecord(h->ev0, st));
+  gpq_status s = (h->cfg.loop_mode == GPQ_LOOP_PERSISTENT) ? run_persistent(h, st) : run_plain(h, 0, nullptr, st);
+  if (s != GPQ_OK) return s;
+  GPQ_CUDA_TRY(cudaEventRecord(h->ev1, st));
+  if (h->cfg.loop_mode == GPQ_LOOP_PERSISTENT) {
+    s = sync_phase(h, st);
+    if (s != GPQ_OK) return s;
+  }
+  GPQ_CUDA_TRY(cudaEventSynchronize(h->ev1));
+  float ms = 0.f;
+  GPQ_CUDA_TRY(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+  h->elapsed_ms = ms;
+  return GPQ_OK;
+}
+
+gpq_status gpq_phold_step(gpq_phold* h, uint32_t nsteps, int* done, void* stream) {
+  GPQ_CHECK_ARG(h, "handle is NULL");
+  if (!h->populated) return GPQ_ERR_NOT_READY;
+  h->finalized = false;
+  return run_plain(h, nsteps, done, gpq::as_stream(stream, h->own));
+}
+
+gpq_status gpq_phold_result_get(gpq_phold* h, gpq_phold_result* out, void* stream) {
+  GPQ_CHECK_ARG(h && out, "NULL argument");
+  if (!h->populated) return GPQ_ERR_NOT_READY;
+  cudaStream_t st = gpq::as_stream(stream, h->own);
+  PholdAcc a{};
+  a.pending_min = kInfBits;
+  GPQ_CUDA_TRY(cudaMemcpyAsync(h->acc, &a, sizeof(PholdAcc), cudaMemcpyHostToDevice, st));
+  const uint32_t wpb = 8;
+  const uint32_t grid = std::max(1u, std::min<uint32_t>((h->cfg.num_lps + wpb - 1) / wpb, 4096u));
+  phold_laq_finalize<<<grid, wpb * 32, 0, st>>>(h->dev(), h->laq(), h->ins(), h->acc);
+  GPQ_CUDA_TRY(cudaGetLastError());
+  GPQ_CUDA_TRY(cudaMemcpyAsync(&a, h->acc, sizeof(PholdAcc), cudaMemcpyDeviceToHost, st));
+  GPQ_CUDA_TRY(cudaMemcpyAsync(h->h_ctrl, h->ctrl, sizeof(PholdCtrl), cudaMemcpyDeviceToHost, st));
+  GPQ_CUDA_TRY(cudaStreamSynchronize(st));
+  std::memset(out, 0, sizeof(*out));
+  out->committed = a.committed;
+  out->steps = h->h_ctrl->steps;
+  out->pending = a.pending;
+  out->pending_csum = a.pending_csum;
+  out->digest = a.digest;
+  out->final_min = gpq_u2f(a.pending_min);
+  out->elapsed_ms = h->elapsed_ms;
+  out->status = (int32_t)h->h_ctrl->err;
+  h->finalized = true;
+  return (gpq_status)h->h_ctrl->err;
+}
+
+gpq_status gpq_phold_lp_stats(gpq_phold* h, uint32_t* count, uint64_t* csum, uint64_t* ohash, void* stream) {
+  GPQ_CHECK_ARG(h, "handle is NULL");
+  cudaStream_t st = gpq::as_stream(stream, h->own);
+  const size_t L = h->cfg.num_lps;
+  if (count) GPQ_CUDA_TRY(cudaMemcpyAsync(count, h->count, L * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  if (csum) GPQ_CUDA_TRY(cudaMemcpyAsync(csum, h->csum, L * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  if (ohash) GPQ_CUDA_TRY(cudaMemcpyAsync(ohash, h->ohash, L * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  GPQ_CUDA_TRY(cudaStreamSynchronize(st));
+  return GPQ_OK;
+}
+
+gpq_status gpq_phold_launch_info(gpq_phold* h, uint32_t* grid, uint32_t* block, uint32_t* launches_per_run) {
+  GPQ_CHECK_ARG(h, "handle is NULL");
+  if (grid) *grid = h->last_grid;
+  if (block) *block = h->block;
+  if (launches_per_run) *launches_per_run = (h->cfg.loop_mode == GPQ_LOOP_PERSISTENT) ? 1u : h->phase;
+  return GPQ_OK;
+}
+
+gpq_status gpq_host_alloc(uint64_t bytes, void** out) {
+  GPQ_CHECK_ARG(out, "out is NULL");
+  *out = nullptr;
+  GPQ_CUDA_TRY(cudaMallocHost(out, bytes ? bytes : 1));
+  return GPQ_OK;
+}
+
+gpq_status gpq_host_free(void* p) {
+  if (p) GPQ_CUDA_TRY(cudaFreeHost(p));
+  return GPQ_OK;
+}
+
+gpq_status gpq_phold_initial_events(const gpq_phold_config* cfg, gpq_item* out, uint64_t n) {
+  gpq_status st = validate(cfg);
+  if (st != GPQ_OK) return st;
+  GPQ_CHECK_ARG(out, "out is NULL");
+  GPQ_CHECK_ARG(n == (uint64_t)cfg->num_lps * cfg->events_per_lp, "n must be num_lps * events_per_lp");
+  const gpq_phold_params p = params_of(*cfg);
+  uint64_t i = 0;
+  for (uint32_t lp = 0; lp < cfg->num_lps; ++lp)
+    for (uint32_t k = 0; k < cfg->events_per_lp; ++k) out[i++] = gpq_phold_initial(p, lp, k, cfg->events_per_lp);
+  return GPQ_OK;
+}
+
+gpq_status gpq_phold_children(const gpq_phold_config* cfg, const gpq_item* events, gpq_item* children, uint64_t n) {
+  gpq_status st = validate(cfg);
+  if (st != GPQ_OK) return st;
+  GPQ_CHECK_ARG(events && children, "NULL array");
+  if (n == 0) return GPQ_OK;
+  gpq_item* d = nullptr;
+  GPQ_CUDA_TRY(cudaMalloc(&d, 2 * n * sizeof(gpq_item)));
+  cudaError_t e = cudaMemcpy(d, events, n * sizeof(gpq_item), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    const uint32_t grid = (uint32_t)std::min<uint64_t>((n + 255) / 256, 65535);
+    phold_children_kernel<<<grid, 256>>>(params_of(*cfg), d, d + n, n);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(children, d + n, n * sizeof(gpq_item), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  GPQ_CUDA_TRY(e);
+  return GPQ_OK;
+}
+
+}  // extern "C"

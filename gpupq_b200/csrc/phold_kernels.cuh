@@ -1,0 +1,186 @@
+// PHOLD engine kernels over the local array queue: population, one window per launch
+// (plain loop, like the reference's des_run), all windows in one persistent launch,
+// and the end-of-run reduction.
+#pragma once
+
+#include "laq.cuh"
+
+// Accumulators filled by the finalize kernel.
+struct PholdAcc {
+  unsigned long long committed;
+  unsigned long long pending;
+  unsigned long long pending_csum;
+  unsigned long long digest;
+  uint32_t pending_min;
+  uint32_t pad[3];
+};
+
+// ---------------------------------------------------------------------------------
+// Population (src/phold.cu:63-79,124-163): LP l receives events id = l*P + k.  One warp
+// per LP ranks its P events in shared memory and writes them sorted into the ring.
+// `src` = NULL generates the events from the seed; otherwise src holds them grouped by
+// LP (src[l*P + k]).  Also computes the first window minimum into mins[0].
+// ---------------------------------------------------------------------------------
+__global__ void phold_laq_populate(PholdDev d, LaqDev q, uint32_t per_lp, const gpq_item* __restrict__ src) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ uint32_t red[32];
+  const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint32_t wpb = blockDim.x >> 5;
+  gpq_item* s_it = reinterpret_cast<gpq_item*>(smem_raw) + (size_t)wib * per_lp;
+  uint64_t* s_key = reinterpret_cast<uint64_t*>(reinterpret_cast<gpq_item*>(smem_raw) + (size_t)wpb * per_lp) +
+                    (size_t)wib * per_lp;
+  const uint32_t lp = blockIdx.x * wpb + wib;
+  uint32_t mn = kInfBits;
+  if (lp < d.L) {
+    for (uint32_t j = lane; j < per_lp; j += 32) {
+      gpq_item e;
+      if (src) {
+        e = src[(size_t)lp * per_lp + j];
+        if (e.lp != lp) gpq_set_error(&d.ctrl->err, GPQ_ERR_INVALID);
+        e.lp = lp;
+      } else {
+        e = gpq_phold_initial(d.p, lp, j, per_lp);
+      }
+      s_it[j] = e;
+      s_key[j] = gpq_lp_key(e);
+      mn = min(mn, gpq_f2u(e.ts));
+    }
+    __syncwarp();
+    gpq_item* ring = q.ring + ((size_t)lp << q.cap_log2);
+    for (uint32_t j = lane; j < per_lp; j += 32) {
+      const uint64_t kj = s_key[j];
+      uint32_t r = 0;
+      for (uint32_t i = 0; i < per_lp; ++i) r += (s_key[i] < kj) ? 1u : 0u;
+      ring[r] = s_it[j];
+    }
+    if (lane == 0) {
+      q.rd[lp] = 0;
+      q.wr[lp] = per_lp;
+      d.count[lp] = 0;
+      d.csum[lp] = 0;
+      d.ohash[lp] = 0;
+    }
+  }
+  mn = block_min_u32(mn, red);
+  if (threadIdx.x == 0 && mn != kInfBits) atomicMin(&d.ctrl->mins[0], mn);
+}
+
+// Shared body of one window for all LPs owned by this block's warps
+// (LP = global warp index + k * total warps).  Returns nothing; folds the block's
+// minimum into mins[(s+1)%3].
+__device__ __forceinline__ void phold_laq_window_body(const PholdDev& d, const LaqDev& q, const InsDev& ib,
+                                                      uint32_t s, float m, unsigned char* smem_raw,
+                                                      uint32_t* red) {
+  const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint32_t wpb = blockDim.x >> 5;
+  const LaqWarpSmem sm = laq_warp_smem(smem_raw + (size_t)wib * laq_warp_smem_bytes(ib.ibc), ib.ibc);
+  const float bound = GPQ_FADD(m, d.p.lookahead);
+  uint32_t* err_slot = &d.ctrl->errs[(s + 1u) % 3u];
+  uint32_t mn = kInfBits;
+  const uint32_t nwarps = gridDim.x * wpb;
+  for (uint32_t lp = blockIdx.x * wpb + wib; lp < d.L; lp += nwarps) {
+    const LaqWindowOut o = laq_lp_window(d, q, ib, lp, s, bound, sm, lane, err_slot);
+    mn = min(mn, o.min_bits);
+  }
+  mn = block_min_u32(mn, red);
+  if (threadIdx.x == 0 && mn != kInfBits) atomicMin(&d.ctrl->mins[(s + 1u) % 3u], mn);
+}
+
+// Plain form: one launch per window; the kernel boundary is the barrier.
+__global__ void phold_laq_window(PholdDev d, LaqDev q, InsDev ib, uint32_t s) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ uint32_t red[32];
+  const uint32_t mb = d.ctrl->mins[s % 3u];
+  const float m = gpq_u2f(mb);
+  if (!(m < d.p.end_time)) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    d.ctrl->mins[(s + 2u) % 3u] = kInfBits;  // slot for window s+2 (last read in window s-1)
+    d.ctrl->errs[(s + 2u) % 3u] = 0u;
+    d.ctrl->steps += 1ull;
+    d.ctrl->phase = s + 1u;
+  }
+  phold_laq_window_body(d, q, ib, s, m, smem_raw, red);
+}
+
+// Persistent form: all windows in one cooperative launch; a bounded grid barrier
+// separates windows.  Every block takes the same exit decision from the same
+// (minimum, error) slot written before the barrier.
+__global__ void phold_laq_persistent(PholdDev d, LaqDev q, InsDev ib, uint32_t s0, uint32_t max_steps) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ uint32_t red[32];
+  unsigned long long target = 0;
+  uint32_t s = s0;
+  for (;; ++s) {
+    const uint32_t mb = ld_relaxed_u32(&d.ctrl->mins[s % 3u]);
+    const uint32_t eb = ld_relaxed_u32(&d.ctrl->errs[s % 3u]);
+    const float m = gpq_u2f(mb);
+    if (!(m < d.p.end_time) || eb != 0u || (max_steps != 0u && s - s0 >= max_steps)) break;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      d.ctrl->mins[(s + 2u) % 3u] = kInfBits;
+      d.ctrl->errs[(s + 2u) % 3u] = 0u;
+      d.ctrl->steps += 1ull;
+    }
+    phold_laq_window_body(d, q, ib, s, m, smem_raw, red);
+    target += gridDim.x;
+    if (!grid_barrier(&d.ctrl->bar, target, d.spin_limit, &d.ctrl->err)) {
+      s += 1u;
+      break;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) d.ctrl->phase = s;
+}
+
+// End of run: committed total, pending events (ring + the unmerged children of the last
+// window) and the order-sensitive digest over the per-LP outputs.  One warp per LP.
+__global__ void phold_laq_finalize(PholdDev d, LaqDev q, InsDev ib, PholdAcc* acc) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t wpb = blockDim.x >> 5;
+  const uint32_t nwarps = gridDim.x * wpb;
+  const uint32_t s = d.ctrl->phase;
+  const uint32_t prevb = (s + 1u) & 1u;
+  const uint32_t mask = (1u << q.cap_log2) - 1u;
+  uint64_t pend = 0, pcs = 0, dig = 0, com = 0;
+  uint32_t pmin = kInfBits;
+  for (uint32_t lp = blockIdx.x * wpb + (threadIdx.x >> 5); lp < d.L; lp += nwarps) {
+    const uint32_t rd = q.rd[lp], wr = q.wr[lp];
+    const gpq_item* ring = q.ring + ((size_t)lp << q.cap_log2);
+    for (uint32_t j = lane; j < wr - rd; j += 32) {
+      const gpq_item e = ring[(rd + j) & mask];
+      pcs += gpq_ev_hash(e.id, gpq_f2u(e.ts));
+      pend += 1;
+      pmin = min(pmin, gpq_f2u(e.ts));
+    }
+    const uint32_t k = min(ib.cnt[(size_t)prevb * d.L + lp], ib.ibc);
+    const gpq_item* src = ib.buf + ((size_t)prevb * d.L + lp) * ib.ibc;
+    for (uint32_t j = lane; j < k; j += 32) {
+      const gpq_item e = src[j];
+      pcs += gpq_ev_hash(e.id, gpq_f2u(e.ts));
+      pend += 1;
+      pmin = min(pmin, gpq_f2u(e.ts));
+    }
+    if (lane == 0) {
+      const uint32_t c = d.count[lp];
+      com += c;
+      const uint64_t lph = gpq_mix64(gpq_mix64(((uint64_t)lp << 32) | c) ^ d.csum[lp]) + d.ohash[lp];
+      dig += gpq_mix64(lph);
+    }
+  }
+  pend = warp_sum_u64(pend);
+  pcs = warp_sum_u64(pcs);
+  dig = warp_sum_u64(dig);
+  com = warp_sum_u64(com);
+  pmin = warp_min_u32(pmin);
+  if (lane == 0) {
+    atomicAdd(&acc->pending, (unsigned long long)pend);
+    atomicAdd(&acc->pending_csum, (unsigned long long)pcs);
+    atomicAdd(&acc->digest, (unsigned long long)dig);
+    atomicAdd(&acc->committed, (unsigned long long)com);
+    atomicMin(&acc->pending_min, pmin);
+  }
+}
+
+// Children of n events (the model's event function on the device).
+__global__ void phold_children_kernel(gpq_phold_params p, const gpq_item* __restrict__ ev, gpq_item* out, uint64_t n) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = gpq_phold_child(p, ev[i]);
+}

@@ -1,0 +1,213 @@
+/*
+ * gpq.h -- C ABI of gpupq_b200 (libgpq.so), a B200-native rebuild of GPUPQ's
+ * data-parallel priority-queue hot path.
+ *
+ * Plain C types only: pointers, sizes, and an opaque stream handle (`void*`,
+ * a cudaStream_t; NULL = the library's own stream).  Every function returns a
+ * gpq_status; nothing calls exit().  The reference's host functions abort the
+ * process on errors (src/util.cuh:36-39, src/des.cu:37-40,57-61).
+ *
+ * Three groups of entry points:
+ *   1. queue objects (gpq_queue_*): the reference's host queue API,
+ *      src/queue.h:86-115, for one of the five queue kinds;
+ *   2. the PHOLD engine (gpq_phold_*): the reference's DES driver + PHOLD model,
+ *      src/des.cu:74-214 and src/phold.cu:124-192, run as a plain host-driven step
+ *      loop (one launch per safe window, like des_run) or as one persistent launch;
+ *   3. utilities (gpq_status_string, gpq_version).
+ */
+#ifndef GPQ_H
+#define GPQ_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "gpq/model.h" /* gpq_item, gpq_phold_params */
+
+#if defined(__GNUC__)
+#define GPQ_API __attribute__((visibility("default")))
+#else
+#define GPQ_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum gpq_status {
+  GPQ_OK = 0,
+  GPQ_ERR_INVALID = 1,         /* bad argument or configuration */
+  GPQ_ERR_CUDA = 2,            /* a CUDA runtime call failed */
+  GPQ_ERR_QUEUE_FULL = 3,      /* a per-LP queue overflowed (reference: insert returns false,
+                                  src/local_array_queue.cu:492-498) */
+  GPQ_ERR_INSERT_FULL = 4,     /* a per-step insert buffer overflowed */
+  GPQ_ERR_TIMEOUT = 5,         /* a device-side wait gave up (bounded spin) */
+  GPQ_ERR_NOMEM = 6,           /* device allocation failed or budget exceeded */
+  GPQ_ERR_UNSUPPORTED = 7,     /* option not available for this queue kind */
+  GPQ_ERR_NOT_READY = 8        /* handle not populated / result not available */
+} gpq_status;
+
+/* The five queue kinds of the reference (src/config.h:8-13, src/queue.h:33-84). */
+typedef enum gpq_queue_kind {
+  GPQ_QUEUE_LAQ = 0, /* local array queue: per-LP sorted ring (src/local_array_queue.cu) */
+  GPQ_QUEUE_GAQ = 1, /* global array queue: one globally sorted array (src/global_array_queue.cu) */
+  GPQ_QUEUE_HQ = 2,  /* parallel heap of sorted r-item nodes (src/heap_queue.cu) */
+  GPQ_QUEUE_LHQ = 3, /* local heap queue: per-LP array heap (src/local_heap_queue.cu) */
+  GPQ_QUEUE_LSQ = 4  /* local splay queue: per-LP splay tree (src/local_splay_queue.cu) */
+} gpq_queue_kind;
+
+/* How the PHOLD engine drives its safe-window steps. */
+typedef enum gpq_loop_mode {
+  GPQ_LOOP_PLAIN = 0,      /* host loop: one launch per window + a D2H read of the minimum
+                              (the reference's des_run, src/des.cu:154-214) */
+  GPQ_LOOP_PERSISTENT = 1  /* one cooperative launch; windows separated by a bounded grid barrier */
+} gpq_loop_mode;
+
+/* ---------------------------------------------------------------------------------- */
+/* 1. Queue objects                                                                   */
+/* ---------------------------------------------------------------------------------- */
+
+typedef struct gpq_queue gpq_queue;
+
+typedef struct gpq_queue_config {
+  uint32_t kind;            /* gpq_queue_kind */
+  uint32_t num_lps;         /* number of logical processes (NUM_LPS, src/config.h:67) */
+  uint32_t capacity;        /* per-LP capacity (LAQ/LHQ/LSQ); total capacity / num_lps (GAQ, HQ) */
+  uint32_t insert_capacity; /* per-LP inserts accepted between two posts (LAQ/LHQ/LSQ);
+                               total per post = insert_capacity * num_lps (GAQ, HQ) */
+  uint32_t node_size;       /* HQ node size r (HQ_NODE_SIZE, src/config.h:88); 0 = default */
+  uint32_t reserved[3];
+} gpq_queue_config;
+
+/* queue_init (src/queue.h:86-87). */
+GPQ_API gpq_status gpq_queue_create(const gpq_queue_config* cfg, gpq_queue** out);
+GPQ_API gpq_status gpq_queue_destroy(gpq_queue* q);
+
+/* queue_insert for a batch of items (src/queue.cuh:46-47); items are HOST pointers
+ * unless `items_on_device` is non-zero.  Takes effect at the next gpq_queue_post. */
+GPQ_API gpq_status gpq_queue_insert(gpq_queue* q, const gpq_item* items, uint64_t n, int items_on_device, void* stream);
+
+/* queue_pre / queue_post / queue_post_init (src/queue.h:89-98). */
+GPQ_API gpq_status gpq_queue_pre(gpq_queue* q, void* stream);
+GPQ_API gpq_status gpq_queue_post(gpq_queue* q, void* stream);
+GPQ_API gpq_status gpq_queue_post_init(gpq_queue* q, void* stream);
+
+/* queue_get_min_ts (src/queue.h:100-103): smallest timestamp over all queued items
+ * (+inf when empty).  Blocks on the stream. */
+GPQ_API gpq_status gpq_queue_get_min(gpq_queue* q, float* min_ts, void* stream);
+
+/* queue_peek + queue_set_done for every LP at once (src/queue.cuh:49-54): removes, per
+ * LP, up to `max_per_lp` items with ts < bound, in key order (0 = no limit; the
+ * reference dequeues one per LP per step, src/phold.cu:84-94).  The removed items are
+ * written to `out` (host array of `out_capacity` items) grouped by LP in ascending LP
+ * order and key order inside an LP; `*n_out` receives their number. */
+GPQ_API gpq_status gpq_queue_dequeue(gpq_queue* q, float bound, uint32_t max_per_lp, gpq_item* out,
+                             uint64_t out_capacity, uint64_t* n_out, void* stream);
+
+/* queue_length / queue_is_empty / queue_clear (src/queue.cuh:62-69) for one LP. */
+GPQ_API gpq_status gpq_queue_length(gpq_queue* q, uint32_t lp, uint32_t* length, void* stream);
+GPQ_API gpq_status gpq_queue_clear(gpq_queue* q, uint32_t lp, void* stream);
+
+/* queue_print (src/queue.cuh:56-57) as data: the items of one LP in key order (for GAQ
+ * and HQ the items of that LP in the global structure).  `*n_out` = item count. */
+GPQ_API gpq_status gpq_queue_dump(gpq_queue* q, uint32_t lp, gpq_item* out, uint64_t out_capacity, uint64_t* n_out,
+                          void* stream);
+
+/* get_enqueue_count / get_dequeue_count (src/queue.h:110-113): items inserted and
+ * removed since creation. */
+GPQ_API gpq_status gpq_queue_counts(gpq_queue* q, uint64_t* enqueued, uint64_t* dequeued, void* stream);
+
+/* ---------------------------------------------------------------------------------- */
+/* 2. PHOLD engine                                                                    */
+/* ---------------------------------------------------------------------------------- */
+
+typedef struct gpq_phold gpq_phold;
+
+typedef struct gpq_phold_config {
+  uint64_t seed;
+  uint32_t num_lps;
+  uint32_t events_per_lp;   /* initial events per LP (ids lp*events_per_lp + k) */
+  float lookahead;          /* LOOKAHEAD (src/config.h:65) as float32 */
+  float end_time;           /* events with ts >= end_time are never committed */
+  uint32_t dest_mode;       /* GPQ_DEST_UNIFORM / GPQ_DEST_RING (gpq/model.h) */
+  uint32_t ring_width;      /* ring neighbourhood +-ring_width (self excluded) */
+  uint32_t ring_threshold;  /* ring with probability ring_threshold / 2^32 */
+  uint32_t queue_kind;      /* gpq_queue_kind */
+  uint32_t capacity;        /* per-LP queue capacity (power of two for LAQ) */
+  uint32_t insert_capacity; /* per-LP insert-buffer slots per window */
+  uint32_t loop_mode;       /* gpq_loop_mode */
+  uint32_t block_threads;   /* CTA size (multiple of 32); 0 = tuned default */
+  uint32_t ctas_per_sm;     /* persistent grid: CTAs per SM; 0 = occupancy maximum */
+  uint32_t max_steps;       /* safety cap on windows; 0 = none */
+  uint32_t reserved[4];
+} gpq_phold_config;
+
+typedef struct gpq_phold_result {
+  uint64_t committed;     /* events committed (ts < end_time) */
+  uint64_t steps;         /* safe windows executed */
+  uint64_t pending;       /* events left queued at the end (all with ts >= end_time) */
+  uint64_t pending_csum;  /* sum of ev_hash over the pending events */
+  uint64_t digest;        /* order-sensitive digest over (lp, count, csum, ohash) */
+  float final_min;        /* smallest pending timestamp at the end */
+  float elapsed_ms;       /* device time of the last gpq_phold_run (CUDA events) */
+  int32_t status;         /* device error word (gpq_status) */
+  uint32_t reserved[3];
+} gpq_phold_result;
+
+GPQ_API gpq_status gpq_phold_create(const gpq_phold_config* cfg, gpq_phold** out);
+GPQ_API gpq_status gpq_phold_destroy(gpq_phold* h);
+
+/* model_init (src/phold.cu:124-163): resets all state and inserts the initial events.
+ * `initial` = NULL generates them on the device from the seed; otherwise it is a HOST
+ * array of n = num_lps * events_per_lp items (e.g. from gpq_phold_initial_events). */
+GPQ_API gpq_status gpq_phold_populate(gpq_phold* h, const gpq_item* initial, uint64_t n, void* stream);
+
+/* des_run (src/des.cu:134-221): run safe windows until the minimum reaches end_time.
+ * Stream-ordered; the device time between start and end is recorded with CUDA events
+ * on `stream` and reported in gpq_phold_result.elapsed_ms. */
+GPQ_API gpq_status gpq_phold_run(gpq_phold* h, void* stream);
+
+/* Run at most `nsteps` further windows (plain loop); *done = 1 once finished. */
+GPQ_API gpq_status gpq_phold_step(gpq_phold* h, uint32_t nsteps, int* done, void* stream);
+
+/* des_finish (src/des.cu:89-132) as data.  Blocks on the stream. */
+GPQ_API gpq_status gpq_phold_result_get(gpq_phold* h, gpq_phold_result* out, void* stream);
+
+/* model_get_events (src/phold.cu:169-182) per LP: committed count, order-insensitive
+ * checksum and order-sensitive hash (HOST arrays of num_lps entries; any may be NULL). */
+GPQ_API gpq_status gpq_phold_lp_stats(gpq_phold* h, uint32_t* count, uint64_t* csum, uint64_t* ohash, void* stream);
+
+/* The initial events the engine would generate, written to a HOST array of
+ * num_lps * events_per_lp items (host computation, bit-identical to the device). */
+GPQ_API gpq_status gpq_phold_initial_events(const gpq_phold_config* cfg, gpq_item* out, uint64_t n);
+
+/* Children of `n` events under `cfg` (the model's event function), computed on the
+ * device; `events` and `children` are HOST arrays. */
+GPQ_API gpq_status gpq_phold_children(const gpq_phold_config* cfg, const gpq_item* events, gpq_item* children,
+                              uint64_t n);
+
+/* Launch geometry of the last gpq_phold_run: persistent grid (CTAs), CTA size, and the
+ * number of kernel launches the run made (1 for the persistent loop, one per window
+ * for the plain loop). */
+GPQ_API gpq_status gpq_phold_launch_info(gpq_phold* h, uint32_t* grid, uint32_t* block, uint32_t* launches_per_run);
+
+/* Page-locked host memory for the end-to-end path (host <-> device copies). */
+GPQ_API gpq_status gpq_host_alloc(uint64_t bytes, void** out);
+GPQ_API gpq_status gpq_host_free(void* p);
+
+/* Device-side timeout of bounded waits (grid barrier spins), in spin iterations. */
+GPQ_API gpq_status gpq_set_spin_limit(uint64_t iterations);
+
+/* ---------------------------------------------------------------------------------- */
+/* 3. Utilities                                                                       */
+/* ---------------------------------------------------------------------------------- */
+
+GPQ_API const char* gpq_status_string(gpq_status s);
+GPQ_API const char* gpq_version(void);
+/* Human-readable text of the last error seen on this thread (static storage). */
+GPQ_API const char* gpq_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPQ_H */

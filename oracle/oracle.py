@@ -1,0 +1,125 @@
+"""ctypes wrapper of the CPU oracle (test infrastructure only).
+
+Loaded by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg; never by the
+gpupq_b200 product.  See oracle/phold_oracle.cpp for what is restated from the reference.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import build as _build
+
+_LIB = None
+
+
+class OraclePholdCfg(ctypes.Structure):
+    _fields_ = [
+        ("seed", ctypes.c_uint64),
+        ("num_lps", ctypes.c_uint32),
+        ("events_per_lp", ctypes.c_uint32),
+        ("dest_mode", ctypes.c_uint32),
+        ("ring_width", ctypes.c_uint32),
+        ("ring_threshold", ctypes.c_uint32),
+        ("lookahead", ctypes.c_float),
+        ("end_time", ctypes.c_float),
+    ]
+
+
+class OraclePholdSummary(ctypes.Structure):
+    _fields_ = [
+        ("committed", ctypes.c_uint64),
+        ("steps", ctypes.c_uint64),
+        ("pending", ctypes.c_uint64),
+        ("pending_csum", ctypes.c_uint64),
+        ("seconds", ctypes.c_double),
+    ]
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = _build.LIB
+        if not os.path.exists(path):
+            path = _build.build()
+        _LIB = ctypes.CDLL(path)
+        u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+        u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
+        f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+        i64p = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
+        _LIB.oracle_phold_seq.argtypes = [ctypes.POINTER(OraclePholdCfg), u32p, u64p, u64p,
+                                          ctypes.POINTER(OraclePholdSummary)]
+        _LIB.oracle_phold_window.argtypes = [ctypes.POINTER(OraclePholdCfg), ctypes.c_int, u32p, u64p,
+                                             u64p, ctypes.POINTER(OraclePholdSummary)]
+        _LIB.oracle_phold_child.argtypes = [ctypes.POINTER(OraclePholdCfg), f32p, u32p, u32p,
+                                            ctypes.c_uint64, f32p, u32p]
+        _LIB.oracle_phold_initial.argtypes = [ctypes.POINTER(OraclePholdCfg), f32p, u32p, u32p]
+        _LIB.oracle_logf.argtypes = [ctypes.c_float]
+        _LIB.oracle_logf.restype = ctypes.c_float
+        _LIB.oracle_ring_search.argtypes = [i64p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int64]
+        _LIB.oracle_ring_search.restype = ctypes.c_int
+        _LIB.oracle_ring_insert_sorted.argtypes = [i64p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                   ctypes.c_int64]
+        _LIB.oracle_ring_quicksort.argtypes = [i64p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    return _LIB
+
+
+def ring_threshold(frac: float) -> int:
+    """Probability -> 32-bit threshold (floor(frac * 2^32)), computed in double."""
+    return min(int(frac * 4294967296.0), 0xFFFFFFFF)
+
+
+def make_cfg(num_lps, events_per_lp, lookahead, end_time, seed, dest_mode=0, ring_width=16, ring_frac=0.9):
+    c = OraclePholdCfg()
+    c.seed = seed
+    c.num_lps = num_lps
+    c.events_per_lp = events_per_lp
+    c.dest_mode = dest_mode
+    c.ring_width = ring_width
+    c.ring_threshold = ring_threshold(ring_frac) if dest_mode == 1 else 0
+    c.lookahead = lookahead
+    c.end_time = end_time
+    return c
+
+
+def phold(cfg, threads=0):
+    """Run the oracle. threads=0: sequential global priority queue; >=1: windowed per-LP driver."""
+    L = cfg.num_lps
+    count = np.zeros(L, np.uint32)
+    csum = np.zeros(L, np.uint64)
+    ohash = np.zeros(L, np.uint64)
+    s = OraclePholdSummary()
+    if threads == 0:
+        rc = lib().oracle_phold_seq(ctypes.byref(cfg), count, csum, ohash, ctypes.byref(s))
+    else:
+        rc = lib().oracle_phold_window(ctypes.byref(cfg), threads, count, csum, ohash, ctypes.byref(s))
+    if rc != 0:
+        raise RuntimeError("oracle failed")
+    return {
+        "count": count, "csum": csum, "ohash": ohash,
+        "committed": int(s.committed), "steps": int(s.steps), "pending": int(s.pending),
+        "pending_csum": int(s.pending_csum), "seconds": float(s.seconds),
+    }
+
+
+def child(cfg, ts, lp, ids):
+    ts = np.ascontiguousarray(ts, np.float32)
+    lp = np.ascontiguousarray(lp, np.uint32)
+    ids = np.ascontiguousarray(ids, np.uint32)
+    out_ts = np.zeros_like(ts)
+    out_lp = np.zeros_like(lp)
+    lib().oracle_phold_child(ctypes.byref(cfg), ts, lp, ids, len(ts), out_ts, out_lp)
+    return out_ts, out_lp
+
+
+def initial(cfg):
+    n = cfg.num_lps * cfg.events_per_lp
+    ts = np.zeros(n, np.float32)
+    lp = np.zeros(n, np.uint32)
+    ids = np.zeros(n, np.uint32)
+    lib().oracle_phold_initial(ctypes.byref(cfg), ts, lp, ids)
+    return ts, lp, ids
+
+
+def logf(x):
+    return lib().oracle_logf(float(x))

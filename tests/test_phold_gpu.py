@@ -1,0 +1,121 @@
+"""GPU parity of the PHOLD engine against the CPU oracle (bit-exact: integer counts,
+64-bit checksums and float32 timestamps compared as bits)."""
+import numpy as np
+import pytest
+
+import gpupq_b200 as G
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+C1 = dict(num_lps=1024, events_per_lp=16, lookahead=1.0, end_time=100.0, seed=42, dest_mode=0)
+
+
+def _oracle(cfgd, threads=0):
+    keys = ("num_lps", "events_per_lp", "lookahead", "end_time", "seed", "dest_mode", "ring_width")
+    return O.phold(O.make_cfg(**{k: v for k, v in cfgd.items() if k in keys}), threads)
+
+
+def _run(cfgd, **kw):
+    cfg = G.make_phold_config(**cfgd, **kw)
+    with G.Phold(cfg) as h:
+        h.populate()
+        h.run()
+        r = h.result()
+        s = h.lp_stats()
+    return r, s
+
+
+def _assert_same(r, s, o, check_steps=True):
+    assert r["status_code"] == 0, r
+    assert np.array_equal(s["count"], o["count"])
+    assert np.array_equal(s["csum"], o["csum"])
+    assert np.array_equal(s["ohash"], o["ohash"])
+    assert r["committed"] == o["committed"]
+    assert r["pending"] == o["pending"]
+    assert r["pending_csum"] == o["pending_csum"]
+    if check_steps:
+        assert r["steps"] == o["steps"]
+
+
+def test_children_match_oracle(gpu_lib):
+    cfgd = dict(num_lps=5000, events_per_lp=3, lookahead=0.1, end_time=10.0, seed=7, dest_mode=1, ring_width=16)
+    cfg = G.make_phold_config(**cfgd)
+    ev = G.initial_events(cfg)
+    rng = np.random.default_rng(0)
+    ev["ts"] = (rng.random(len(ev)) * 1000).astype(np.float32)
+    ch = G.children(cfg, ev)
+    ots, olp = O.child(O.make_cfg(**cfgd), ev["ts"], ev["lp"], ev["id"])
+    assert np.array_equal(ch["ts"].view(np.uint32), ots.view(np.uint32))
+    assert np.array_equal(ch["lp"], olp)
+    assert np.array_equal(ch["id"], ev["id"])
+
+
+@pytest.mark.parametrize("loop", ["plain", "persistent"])
+def test_phold_plain_workload_bit_exact(gpu_lib, loop):
+    """1024 LPs x 16 events, lookahead 1.0, end 100, uniform destinations, seed 42."""
+    o = _oracle(C1)
+    r, s = _run(C1, loop=loop)
+    _assert_same(r, s, o)
+    assert r["committed"] == 820705
+
+
+@pytest.mark.parametrize("loop", ["plain", "persistent"])
+def test_phold_large_reduced_bit_exact(gpu_lib, loop):
+    """The 65,536-LP ring workload cut to end time 3 (checked by the threaded oracle)."""
+    cfgd = dict(num_lps=65536, events_per_lp=64, lookahead=0.1, end_time=3.0, seed=7, dest_mode=1, ring_width=16)
+    o = _oracle(cfgd, threads=8)
+    r, s = _run(cfgd, loop=loop, capacity=256, insert_capacity=64)
+    _assert_same(r, s, o)
+
+
+@pytest.mark.parametrize("cfgd,kw", [
+    (dict(num_lps=1, events_per_lp=1, lookahead=0.5, end_time=30.0, seed=1, dest_mode=0), {}),
+    (dict(num_lps=7, events_per_lp=5, lookahead=0.25, end_time=40.0, seed=9, dest_mode=0), dict(block_threads=32)),
+    (dict(num_lps=100, events_per_lp=33, lookahead=0.05, end_time=8.0, seed=11, dest_mode=1, ring_width=2),
+     dict(capacity=128, insert_capacity=128)),
+    (dict(num_lps=333, events_per_lp=200, lookahead=0.02, end_time=2.0, seed=13, dest_mode=1, ring_width=1),
+     dict(capacity=512, insert_capacity=256)),
+    (dict(num_lps=64, events_per_lp=4, lookahead=1.0, end_time=0.0, seed=2, dest_mode=0), {}),
+])
+@pytest.mark.parametrize("loop", ["plain", "persistent"])
+def test_phold_edge_shapes(gpu_lib, cfgd, kw, loop):
+    o = _oracle(cfgd)
+    r, s = _run(cfgd, loop=loop, **kw)
+    _assert_same(r, s, o)
+
+
+def test_host_initial_events_path(gpu_lib):
+    cfg = G.make_phold_config(**C1)
+    ev = G.initial_events(cfg)
+    with G.Phold(cfg) as h:
+        h.populate(ev)
+        h.run()
+        r1 = h.result()
+        h.populate()
+        h.run()
+        r2 = h.result()
+    assert r1["digest"] == r2["digest"] and r1["committed"] == r2["committed"] == 820705
+
+
+def test_step_api_resumes(gpu_lib):
+    cfg = G.make_phold_config(**C1, loop="plain")
+    o = _oracle(C1)
+    with G.Phold(cfg) as h:
+        h.populate()
+        done = False
+        n = 0
+        while not done:
+            done = h.step(7)
+            n += 1
+        r = h.result()
+        s = h.lp_stats()
+    _assert_same(r, s, o)
+    assert n > 10
+
+
+def test_queue_overflow_reported(gpu_lib):
+    # per-LP capacity 32 with 32 initial events: the first child overflows the queue
+    cfgd = dict(num_lps=16, events_per_lp=32, lookahead=0.01, end_time=50.0, seed=3, dest_mode=0)
+    r, _ = _run(cfgd, capacity=32, insert_capacity=64)
+    assert r["status_code"] in (3, 4)
