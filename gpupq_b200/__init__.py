@@ -99,6 +99,8 @@ _SIGS = {
     "gpq_phold_children": ([ctypes.POINTER(PholdConfig), _VP, _VP, ctypes.c_uint64], ctypes.c_int),
     "gpq_phold_launch_info": ([_VP, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32),
                                ctypes.POINTER(ctypes.c_uint32)], ctypes.c_int),
+    "gpq_phold_run_static": ([ctypes.POINTER(PholdConfig), _VP, _VP, _VP, _VP, ctypes.POINTER(PholdResult), _VP],
+                             ctypes.c_int),
     "gpq_host_alloc": ([ctypes.c_uint64, ctypes.POINTER(_VP)], ctypes.c_int),
     "gpq_host_free": ([_VP], ctypes.c_int),
     "gpq_queue_create": ([ctypes.c_void_p, ctypes.POINTER(_VP)], ctypes.c_int),

@@ -1,0 +1,54 @@
+// Host-side PHOLD configuration helpers shared by the engine entry points.
+#pragma once
+
+#include "host_common.h"
+
+namespace gpq {
+
+inline gpq_phold_params phold_params_of(const gpq_phold_config& c) {
+  gpq_phold_params p;
+  p.seed = c.seed;
+  p.num_lps = c.num_lps;
+  p.dest_mode = c.dest_mode;
+  p.ring_width = c.ring_width;
+  p.ring_threshold = c.ring_threshold;
+  p.lookahead = c.lookahead;
+  p.end_time = c.end_time;
+  return p;
+}
+
+inline bool is_pow2(uint32_t x) { return x && !(x & (x - 1)); }
+inline uint32_t ilog2_ceil(uint32_t x) { uint32_t r = 0; while ((1u << r) < x) ++r; return r; }
+
+// Checks that hold for every queue kind and loop mode.
+inline gpq_status validate_phold_config(const gpq_phold_config* c) {
+  GPQ_CHECK_ARG(c, "config is NULL");
+  GPQ_CHECK_ARG(c->num_lps > 0 && c->num_lps <= (1u << 24), "num_lps must be in [1, 2^24]");
+  GPQ_CHECK_ARG(c->events_per_lp > 0, "events_per_lp must be > 0");
+  GPQ_CHECK_ARG((uint64_t)c->num_lps * c->events_per_lp <= 0xFFFFFFFFull, "num_lps * events_per_lp must fit 32-bit ids");
+  GPQ_CHECK_ARG(c->lookahead > 0.f && c->lookahead < 1e30f, "lookahead must be positive and finite");
+  GPQ_CHECK_ARG(c->end_time >= 0.f && c->end_time < 1e30f, "end_time must be finite and >= 0");
+  GPQ_CHECK_ARG(c->dest_mode == GPQ_DEST_UNIFORM || c->dest_mode == GPQ_DEST_RING, "dest_mode");
+  if (c->dest_mode == GPQ_DEST_RING)
+    GPQ_CHECK_ARG(c->ring_width >= 1 && 2ull * c->ring_width < c->num_lps, "ring_width must satisfy 1 <= 2w < num_lps");
+  GPQ_CHECK_ARG(c->loop_mode == GPQ_LOOP_PLAIN || c->loop_mode == GPQ_LOOP_PERSISTENT, "loop_mode");
+  GPQ_CHECK_ARG(c->queue_kind <= GPQ_QUEUE_LSQ, "queue_kind");
+  return GPQ_OK;
+}
+
+// Fills the LAQ defaults (capacity 256, insert capacity 64, 256-thread CTAs) and checks them.
+inline gpq_status normalize_laq_config(gpq_phold_config* c) {
+  if (c->capacity == 0) c->capacity = 256;
+  if (c->insert_capacity == 0) c->insert_capacity = 64;
+  GPQ_CHECK_ARG(is_pow2(c->capacity) && c->capacity >= 32 && c->capacity <= (1u << 16),
+                "LAQ capacity must be a power of two in [32, 65536]");
+  GPQ_CHECK_ARG(c->insert_capacity >= 1 && c->insert_capacity <= 1024, "insert_capacity must be in [1, 1024]");
+  GPQ_CHECK_ARG(c->events_per_lp <= c->capacity, "events_per_lp must not exceed capacity");
+  GPQ_CHECK_ARG(c->events_per_lp <= 2048, "events_per_lp must be <= 2048");
+  if (c->block_threads == 0) c->block_threads = 256;
+  GPQ_CHECK_ARG(c->block_threads % 32 == 0 && c->block_threads >= 32 && c->block_threads <= 1024,
+                "block_threads must be a multiple of 32 in [32, 1024]");
+  return GPQ_OK;
+}
+
+}  // namespace gpq

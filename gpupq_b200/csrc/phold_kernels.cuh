@@ -21,7 +21,7 @@ struct PholdAcc {
 // `src` = NULL generates the events from the seed; otherwise src holds them grouped by
 // LP (src[l*P + k]).  Also computes the first window minimum into mins[0].
 // ---------------------------------------------------------------------------------
-__global__ void phold_laq_populate(PholdDev d, LaqDev q, uint32_t per_lp, const gpq_item* __restrict__ src) {
+static __global__ void phold_laq_populate(PholdDev d, LaqDev q, uint32_t per_lp, const gpq_item* __restrict__ src) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ uint32_t red[32];
   const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -87,7 +87,7 @@ __device__ __forceinline__ void phold_laq_window_body(const PholdDev& d, const L
 }
 
 // Plain form: one launch per window; the kernel boundary is the barrier.
-__global__ void phold_laq_window(PholdDev d, LaqDev q, InsDev ib, uint32_t s) {
+static __global__ void phold_laq_window(PholdDev d, LaqDev q, InsDev ib, uint32_t s) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ uint32_t red[32];
   const uint32_t mb = d.ctrl->mins[s % 3u];
@@ -105,7 +105,7 @@ __global__ void phold_laq_window(PholdDev d, LaqDev q, InsDev ib, uint32_t s) {
 // Persistent form: all windows in one cooperative launch; a bounded grid barrier
 // separates windows.  Every block takes the same exit decision from the same
 // (minimum, error) slot written before the barrier.
-__global__ void phold_laq_persistent(PholdDev d, LaqDev q, InsDev ib, uint32_t s0, uint32_t max_steps) {
+static __global__ void phold_laq_persistent(PholdDev d, LaqDev q, InsDev ib, uint32_t s0, uint32_t max_steps) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ uint32_t red[32];
   unsigned long long target = 0;
@@ -132,7 +132,7 @@ __global__ void phold_laq_persistent(PholdDev d, LaqDev q, InsDev ib, uint32_t s
 
 // End of run: committed total, pending events (ring + the unmerged children of the last
 // window) and the order-sensitive digest over the per-LP outputs.  One warp per LP.
-__global__ void phold_laq_finalize(PholdDev d, LaqDev q, InsDev ib, PholdAcc* acc) {
+static __global__ void phold_laq_finalize(PholdDev d, LaqDev q, InsDev ib, PholdAcc* acc) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t wpb = blockDim.x >> 5;
   const uint32_t nwarps = gridDim.x * wpb;
@@ -180,7 +180,7 @@ __global__ void phold_laq_finalize(PholdDev d, LaqDev q, InsDev ib, PholdAcc* ac
 }
 
 // Children of n events (the model's event function on the device).
-__global__ void phold_children_kernel(gpq_phold_params p, const gpq_item* __restrict__ ev, gpq_item* out, uint64_t n) {
+static __global__ void phold_children_kernel(gpq_phold_params p, const gpq_item* __restrict__ ev, gpq_item* out, uint64_t n) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
     out[i] = gpq_phold_child(p, ev[i]);
 }

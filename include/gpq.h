@@ -190,6 +190,34 @@ GPQ_API gpq_status gpq_phold_children(const gpq_phold_config* cfg, const gpq_ite
  * for the plain loop). */
 GPQ_API gpq_status gpq_phold_launch_info(gpq_phold* h, uint32_t* grid, uint32_t* block, uint32_t* launches_per_run);
 
+/* Allocation-free PHOLD run.  No counterpart in the reference (it allocates its queues
+ * with cudaMalloc in queue_init, src/local_array_queue.cu:429-433).
+ *
+ * For callers that cannot allocate device memory at run time: an application whose
+ * device memory is already owned by another allocator or fixed plan (a cudaMalloc would
+ * fail or break the plan), or a latency-bound caller that cannot pay for cudaMalloc and
+ * cudaFree, which may synchronize the device.  One call populates, runs every window
+ * with the persistent loop, and reduces the results -- like gpq_phold_create + populate +
+ * run + result_get + destroy, with the same results -- but allocates nothing: all queue
+ * state lives in one fixed array of GPQ_STATIC_SCRATCH_BYTES (16 MiB) of device memory
+ * that every GPU loading this library holds until the process exits.
+ *
+ *   d_initial  DEVICE array of num_lps * events_per_lp items grouped by LP (as from
+ *              gpq_phold_initial_events), or NULL to generate them from the seed;
+ *   d_count, d_csum, d_ohash  DEVICE arrays of num_lps entries, overwritten with the
+ *              per-LP results (as gpq_phold_lp_stats);
+ *   out        HOST result; elapsed_ms is not measured here (0).
+ * Local array queue only.  A configuration whose queues need more than the fixed array
+ * (about 1024 LPs at capacity 256 and insert capacity 64 use 6.3 MiB) is rejected with
+ * GPQ_ERR_INVALID and a message naming the size.  The first call on a device (with that
+ * device current) looks up the array's device address; make that first call before any
+ * stream capture.  All calls share the array and each call re-initializes what it needs:
+ * calls that overlap on the GPU race with each other -- serialize them.  Blocks on
+ * `stream` (NULL = the legacy default stream). */
+#define GPQ_STATIC_SCRATCH_BYTES (16u * 1024u * 1024u)
+GPQ_API gpq_status gpq_phold_run_static(const gpq_phold_config* cfg, const gpq_item* d_initial, uint32_t* d_count,
+                                        uint64_t* d_csum, uint64_t* d_ohash, gpq_phold_result* out, void* stream);
+
 /* Page-locked host memory for the end-to-end path (host <-> device copies). */
 GPQ_API gpq_status gpq_host_alloc(uint64_t bytes, void** out);
 GPQ_API gpq_status gpq_host_free(void* p);

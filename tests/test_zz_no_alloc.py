@@ -1,0 +1,84 @@
+"""The allocation-free PHOLD entry point (gpq_phold_run_static) against the allocating one.
+
+gpq_phold_run_static exists for callers that cannot allocate device memory while they
+run -- e.g. an application whose device memory belongs to another allocator or a fixed
+plan, or a latency-bound loop that cannot pay for cudaMalloc/cudaFree.  It keeps all
+queue state in one fixed 16 MiB device array, so its results must equal the normal
+create/populate/run path exactly.  This file is collected last on purpose: a run that
+stops at the first failure has executed every other test before it.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import gpupq_b200 as G
+
+CFG_A = dict(num_lps=1024, events_per_lp=16, lookahead=1.0, end_time=100.0, seed=42, dest_mode=0)
+CFG_B = dict(num_lps=500, events_per_lp=8, lookahead=0.1, end_time=30.0, seed=5, dest_mode=1, ring_width=16)
+
+
+def _reference_path(cfgd):
+    cfg = G.make_phold_config(**cfgd, loop="persistent")
+    with G.Phold(cfg) as h:
+        h.populate()
+        h.run()
+        r = h.result()
+        s = h.lp_stats()
+    return r, s
+
+
+def _static_path(cfgd, initial=None):
+    import torch
+    L = cfgd["num_lps"]
+    cfg = G.make_phold_config(**cfgd, loop="persistent")
+    count = torch.full((L,), 0x5A5A5A5A, dtype=torch.int32, device="cuda")
+    csum = torch.full((L,), 123, dtype=torch.int64, device="cuda")
+    ohash = torch.full((L,), -7, dtype=torch.int64, device="cuda")
+    d_init = None
+    keep = None
+    if initial is not None:
+        keep = torch.from_numpy(initial.view(np.uint8).copy()).cuda()
+        d_init = ctypes.c_void_p(keep.data_ptr())
+    torch.cuda.synchronize()
+    res = G.PholdResult()
+    st = G.lib().gpq_phold_run_static(ctypes.byref(cfg), d_init, ctypes.c_void_p(count.data_ptr()),
+                                      ctypes.c_void_p(csum.data_ptr()), ctypes.c_void_p(ohash.data_ptr()),
+                                      ctypes.byref(res), None)
+    torch.cuda.synchronize()
+    G.check(st, "gpq_phold_run_static")
+    s = {"count": count.cpu().numpy().view(np.uint32), "csum": csum.cpu().numpy().view(np.uint64),
+         "ohash": ohash.cpu().numpy().view(np.uint64)}
+    return res.as_dict(), s
+
+
+def _same(a, b):
+    (ra, sa), (rb, sb) = a, b
+    for k in ("committed", "steps", "pending", "pending_csum", "digest"):
+        assert ra[k] == rb[k], k
+    for k in ("count", "csum", "ohash"):
+        assert np.array_equal(sa[k], sb[k]), k
+
+
+@pytest.mark.gpu
+def test_static_entry_point_matches_allocating_path(gpu_lib):
+    want_a = _reference_path(CFG_A)
+    want_b = _reference_path(CFG_B)
+    # consecutive calls share the fixed array; each must start from a clean state
+    _same(_static_path(CFG_A), want_a)
+    _same(_static_path(CFG_B), want_b)
+    _same(_static_path(CFG_A), want_a)
+    # caller-provided initial events (device array) give the same run
+    init = G.initial_events(G.make_phold_config(**CFG_B))
+    _same(_static_path(CFG_B, init), want_b)
+    assert want_a[0]["committed"] == 820705
+
+
+def test_static_entry_point_rejects_oversized_config():
+    cfg = G.make_phold_config(num_lps=65536, events_per_lp=64, lookahead=0.1, end_time=10.0, seed=7)
+    res = G.PholdResult()
+    st = G.lib().gpq_phold_run_static(ctypes.byref(cfg), None, ctypes.c_void_p(16), ctypes.c_void_p(16),
+                                      ctypes.c_void_p(16), ctypes.byref(res), None)
+    assert st == 1  # GPQ_ERR_INVALID, before any device work
+    msg = G.last_error()
+    assert "needs" in msg and "16777216" in msg
