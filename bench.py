@@ -162,6 +162,9 @@ def main():
     ap.add_argument("--end-time", type=float, default=None, help="override the workload end time (debug)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (library defaults)")
+    ap.add_argument("--retune", action="store_true", help="ignore the autotuner cache")
+    ap.add_argument("--tune-windows", type=int, default=200)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -185,7 +188,13 @@ def main():
     if args.end_time is not None:
         cfgd["end_time"] = args.end_time
     cfgd["seed"] = WORKLOAD["seed"] + rank
-    cfg = G.make_phold_config(**cfgd, queue=args.queue, capacity=256, insert_capacity=64, loop=args.loop)
+    shape = {}
+    if not args.no_tune:
+        from gpupq_b200 import autotune
+        shape = autotune.tune_phold(dict(cfgd, capacity=256), queue=args.queue, loop=args.loop,
+                                    windows=args.tune_windows, force=args.retune)
+    cfg = G.make_phold_config(**cfgd, queue=args.queue, capacity=256, loop=args.loop,
+                              **dict({"insert_capacity": 64}, **shape))
     h = G.Phold(cfg)
 
     def barrier():
@@ -310,7 +319,8 @@ def main():
                        "end_time": cfgd["end_time"], "events_per_run": committed / args.steps,
                        "windows_per_run": windows / args.steps,
                        "l2": "inputs larger than L2 (268 MB queue array)",
-                       "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU"},
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU",
+                       "launch_shape": dict(shape, block_threads=info["block"], grid=info["grid"])},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": f"{peak_kind} hbm_gbs", "kernel": f"phold_laq_{args.loop}",

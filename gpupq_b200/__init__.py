@@ -58,7 +58,8 @@ class PholdConfig(ctypes.Structure):
         ("block_threads", ctypes.c_uint32),
         ("ctas_per_sm", ctypes.c_uint32),
         ("max_steps", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 4),
+        ("lanes_per_lp", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 3),
     ]
 
 
@@ -182,7 +183,7 @@ def presets():
 
 def make_phold_config(num_lps, events_per_lp, lookahead, end_time, seed, dest_mode=DEST_UNIFORM,
                       ring_width=16, ring_frac=0.9, queue="laq", capacity=256, insert_capacity=64,
-                      loop="persistent", block_threads=0, ctas_per_sm=0, max_steps=0):
+                      loop="persistent", block_threads=0, ctas_per_sm=0, max_steps=0, lanes_per_lp=0):
     c = PholdConfig()
     c.seed = seed
     c.num_lps = num_lps
@@ -199,6 +200,7 @@ def make_phold_config(num_lps, events_per_lp, lookahead, end_time, seed, dest_mo
     c.block_threads = block_threads
     c.ctas_per_sm = ctas_per_sm
     c.max_steps = max_steps
+    c.lanes_per_lp = lanes_per_lp
     return c
 
 

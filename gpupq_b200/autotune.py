@@ -1,0 +1,110 @@
+"""Autotuner for the PHOLD engine's launch shape.
+
+For a workload class it times candidate (lanes_per_lp, block_threads, ctas_per_sm,
+insert_capacity) settings on the first `windows` safe windows of the real workload
+(same seed, same queues), rejects candidates that overflow or disagree with the others
+(every candidate runs the same windows, so committed count and digest must match), and
+keeps the fastest.  Results are cached in a JSON file keyed by GPU name and workload
+class, so later runs pick the tuned shape without re-timing.
+"""
+import itertools
+import json
+import os
+import time
+
+from . import GpqError, Phold, make_phold_config
+
+DEFAULT_CACHE = os.environ.get("GPQ_TUNE_CACHE", os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib",
+                                                              "tune_cache.json"))
+
+DEFAULT_SPACE = {
+    "lanes_per_lp": [4, 8, 16, 32],
+    "block_threads": [128, 256, 512],
+    "ctas_per_sm": [0],
+    "insert_capacity": [64],
+}
+
+
+def _gpu_name():
+    try:
+        import torch
+        if torch.cuda.is_available():
+            return torch.cuda.get_device_name(0)
+    except Exception:
+        pass
+    return "unknown-gpu"
+
+
+def workload_key(cfgd, queue, loop):
+    keys = ("num_lps", "events_per_lp", "lookahead", "dest_mode", "capacity")
+    parts = [f"{k}={cfgd.get(k)}" for k in keys]
+    return f"{_gpu_name()}|{queue}|{loop}|" + "|".join(parts)
+
+
+def _load(cache):
+    try:
+        with open(cache) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def _save(cache, data):
+    try:
+        os.makedirs(os.path.dirname(cache), exist_ok=True)
+        tmp = cache + ".tmp"
+        with open(tmp, "w") as f:
+            json.dump(data, f, indent=1, sort_keys=True)
+        os.replace(tmp, cache)
+    except OSError:
+        pass
+
+
+def tune_phold(cfgd, queue="laq", loop="persistent", windows=200, space=None, cache=DEFAULT_CACHE,
+               force=False, verbose=False):
+    """Return the fastest launch-shape settings (a dict of make_phold_config keyword
+    arguments) for this workload class, timing candidates if not cached."""
+    key = workload_key(cfgd, queue, loop)
+    data = _load(cache)
+    if not force and key in data:
+        return dict(data[key]["best"])
+    space = dict(DEFAULT_SPACE, **(space or {}))
+    names = list(space.keys())
+    results = []
+    ref = None
+    for values in itertools.product(*[space[n] for n in names]):
+        shape = dict(zip(names, values))
+        if shape["block_threads"] < shape["lanes_per_lp"]:
+            continue
+        try:
+            cfg = make_phold_config(**cfgd, queue=queue, loop=loop, max_steps=windows, **shape)
+            with Phold(cfg) as h:
+                h.populate()
+                h.run()  # warm-up (module load, first-touch)
+                h.populate()
+                h.run()
+                r = h.result()
+        except GpqError as e:
+            if verbose:
+                print("autotune: reject", shape, e)
+            continue
+        if r["status_code"] != 0:
+            continue
+        sig = (r["committed"], r["digest"], r["steps"])
+        if ref is None:
+            ref = sig
+        elif sig != ref:
+            raise RuntimeError(f"autotune: candidate {shape} disagrees with the others: {sig} vs {ref}")
+        per_window = r["elapsed_ms"] / max(1, r["steps"])
+        results.append((per_window, shape))
+        if verbose:
+            print(f"autotune: {shape} {per_window * 1e3:.1f} us/window")
+    if not results:
+        raise RuntimeError("autotune: no candidate ran")
+    results.sort(key=lambda x: x[0])
+    best = results[0][1]
+    data[key] = {"best": best, "us_per_window": results[0][0] * 1e3, "when": time.strftime("%Y-%m-%dT%H:%M:%S"),
+                 "windows": windows,
+                 "all": [{"shape": s, "us_per_window": t * 1e3} for t, s in results]}
+    _save(cache, data)
+    return dict(best)

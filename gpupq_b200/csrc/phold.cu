@@ -78,7 +78,8 @@ struct gpq_phold {
   }
   LaqDev laq() const { return LaqDev{ring, rd, wr, cap_log2}; }
   InsDev ins() const { return InsDev{ibuf, icnt, cfg.insert_capacity}; }
-  size_t window_smem() const { return (size_t)(block / 32) * laq_warp_smem_bytes(cfg.insert_capacity); }
+  LaqKernelSet ks{};
+  size_t window_smem() const { return (size_t)(block / ks.group) * laq_group_smem_bytes(cfg.insert_capacity); }
 
   ~gpq_phold() {
     for (void* p : {(void*)ring, (void*)rd, (void*)wr, (void*)ibuf, (void*)icnt, (void*)count, (void*)csum,
@@ -145,9 +146,15 @@ gpq_status gpq_phold_create(const gpq_phold_config* cfg_in, gpq_phold** out) {
   TRY(cudaMalloc(&h->ctrl, sizeof(PholdCtrl)));
   TRY(cudaMalloc(&h->acc, sizeof(PholdAcc)));
   TRY(cudaMallocHost(&h->h_ctrl, sizeof(PholdCtrl)));
+  if (!laq_kernel_set(c.lanes_per_lp, &h->ks)) return fail(GPQ_ERR_INVALID);
+  if (!gpq::fit_block_to_smem(&h->block, h->ks.group, laq_group_smem_bytes(c.insert_capacity), 200 * 1024)) {
+    gpq::set_last_error("insert_capacity %u needs too much shared memory per lane group", c.insert_capacity);
+    return fail(GPQ_ERR_INVALID);
+  }
+  h->cfg.block_threads = h->block;
   const size_t smem = h->window_smem();
-  TRY(cudaFuncSetAttribute(phold_laq_window, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  TRY(cudaFuncSetAttribute(phold_laq_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  TRY(cudaFuncSetAttribute(h->ks.window, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  TRY(cudaFuncSetAttribute(h->ks.persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 #undef TRY
   *out = h;
   return GPQ_OK;
@@ -198,12 +205,12 @@ gpq_status gpq_phold_populate(gpq_phold* h, const gpq_item* initial, uint64_t n,
 
 static gpq_status run_plain(gpq_phold* h, uint32_t nsteps, int* done, cudaStream_t st) {
   const gpq_phold_config& c = h->cfg;
-  const uint32_t wpb = h->block / 32;
-  const uint32_t grid = (uint32_t)((c.num_lps + wpb - 1) / wpb);
+  const uint32_t gpb = h->block / h->ks.group;
+  const uint32_t grid = (uint32_t)((c.num_lps + gpb - 1) / gpb);
   const size_t smem = h->window_smem();
-  const PholdDev d = h->dev();
-  const LaqDev q = h->laq();
-  const InsDev ib = h->ins();
+  PholdDev d = h->dev();
+  LaqDev q = h->laq();
+  InsDev ib = h->ins();
   uint32_t executed = 0;
   if (done) *done = 0;
   // des_run loop: read the window minimum (D2H) -> run the window -> repeat.
@@ -217,8 +224,9 @@ static gpq_status run_plain(gpq_phold* h, uint32_t nsteps, int* done, cudaStream
       if (done) *done = 1;
       break;
     }
-    phold_laq_window<<<grid, h->block, smem, st>>>(d, q, ib, h->phase);
-    GPQ_CUDA_TRY(cudaGetLastError());
+    uint32_t phase = h->phase;
+    void* args[] = {&d, &q, &ib, &phase};
+    GPQ_CUDA_TRY(cudaLaunchKernel(h->ks.window, dim3(grid), dim3(h->block), args, smem, st));
     ++h->phase;
     ++executed;
   }
@@ -229,15 +237,15 @@ static gpq_status run_persistent(gpq_phold* h, cudaStream_t st) {
   const gpq_phold_config& c = h->cfg;
   const size_t smem = h->window_smem();
   int per_sm = 0;
-  GPQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, phold_laq_persistent, (int)h->block, smem));
+  GPQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, h->ks.persistent, (int)h->block, smem));
   if (per_sm <= 0) {
     gpq::set_last_error("persistent kernel does not fit on an SM (block %u, smem %zu)", h->block, smem);
     return GPQ_ERR_INVALID;
   }
   if (c.ctas_per_sm) per_sm = std::min<int>(per_sm, (int)c.ctas_per_sm);
   uint32_t grid = (uint32_t)(per_sm * h->num_sms);
-  const uint32_t wpb = h->block / 32;
-  const uint32_t need = (uint32_t)((c.num_lps + wpb - 1) / wpb);
+  const uint32_t gpb = h->block / h->ks.group;
+  const uint32_t need = (uint32_t)((c.num_lps + gpb - 1) / gpb);
   grid = std::min(grid, std::max(need, 1u));
   GPQ_CUDA_TRY(cudaMemsetAsync(&h->ctrl->bar, 0, sizeof(unsigned long long), st));
   PholdDev d = h->dev();
@@ -247,7 +255,7 @@ static gpq_status run_persistent(gpq_phold* h, cudaStream_t st) {
   uint32_t maxs = c.max_steps ? (c.max_steps > s0 ? c.max_steps - s0 : 0) : 0;
   if (c.max_steps && maxs == 0) return GPQ_OK;
   void* args[] = {&d, &q, &ib, &s0, &maxs};
-  GPQ_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)phold_laq_persistent, dim3(grid), dim3(h->block), args, smem, st));
+  GPQ_CUDA_TRY(cudaLaunchCooperativeKernel(h->ks.persistent, dim3(grid), dim3(h->block), args, smem, st));
   h->last_grid = grid;
   return GPQ_OK;
 }

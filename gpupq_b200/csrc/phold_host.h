@@ -46,9 +46,20 @@ inline gpq_status normalize_laq_config(gpq_phold_config* c) {
   GPQ_CHECK_ARG(c->events_per_lp <= c->capacity, "events_per_lp must not exceed capacity");
   GPQ_CHECK_ARG(c->events_per_lp <= 2048, "events_per_lp must be <= 2048");
   if (c->block_threads == 0) c->block_threads = 256;
+  if (c->lanes_per_lp == 0) c->lanes_per_lp = 8;
+  GPQ_CHECK_ARG(c->lanes_per_lp == 4 || c->lanes_per_lp == 8 || c->lanes_per_lp == 16 || c->lanes_per_lp == 32,
+                "lanes_per_lp must be 4, 8, 16 or 32");
   GPQ_CHECK_ARG(c->block_threads % 32 == 0 && c->block_threads >= 32 && c->block_threads <= 1024,
                 "block_threads must be a multiple of 32 in [32, 1024]");
   return GPQ_OK;
+}
+
+// Halves the CTA size until the per-CTA merge scratch (one slice per lane group) fits
+// `limit` bytes of shared memory.  Returns false if even one warp does not fit.
+inline bool fit_block_to_smem(uint32_t* block, uint32_t group, size_t group_bytes, size_t limit) {
+  while ((size_t)(*block / group) * group_bytes > limit && *block > 32) *block /= 2;
+  if (*block < 32) *block = 32;
+  return (size_t)(*block / group) * group_bytes <= limit;
 }
 
 }  // namespace gpq

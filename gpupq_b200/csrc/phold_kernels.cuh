@@ -65,21 +65,23 @@ static __global__ void phold_laq_populate(PholdDev d, LaqDev q, uint32_t per_lp,
   if (threadIdx.x == 0 && mn != kInfBits) atomicMin(&d.ctrl->mins[0], mn);
 }
 
-// Shared body of one window for all LPs owned by this block's warps
-// (LP = global warp index + k * total warps).  Returns nothing; folds the block's
-// minimum into mins[(s+1)%3].
+// Shared body of one window for all LPs owned by this block's lane groups
+// (LP = global group index + k * total groups).  Folds the block's minimum into
+// mins[(s+1)%3].
+template <int G>
 __device__ __forceinline__ void phold_laq_window_body(const PholdDev& d, const LaqDev& q, const InsDev& ib,
                                                       uint32_t s, float m, unsigned char* smem_raw,
                                                       uint32_t* red) {
-  const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const uint32_t wpb = blockDim.x >> 5;
-  const LaqWarpSmem sm = laq_warp_smem(smem_raw + (size_t)wib * laq_warp_smem_bytes(ib.ibc), ib.ibc);
+  const LaneGroup<G> g;
+  const uint32_t gib = threadIdx.x / G;  // group in block
+  const uint32_t gpb = blockDim.x / G;
+  const LaqGroupSmem sm = laq_group_smem(smem_raw + (size_t)gib * laq_group_smem_bytes(ib.ibc), ib.ibc);
   const float bound = GPQ_FADD(m, d.p.lookahead);
   uint32_t* err_slot = &d.ctrl->errs[(s + 1u) % 3u];
   uint32_t mn = kInfBits;
-  const uint32_t nwarps = gridDim.x * wpb;
-  for (uint32_t lp = blockIdx.x * wpb + wib; lp < d.L; lp += nwarps) {
-    const LaqWindowOut o = laq_lp_window(d, q, ib, lp, s, bound, sm, lane, err_slot);
+  const uint32_t ngroups = gridDim.x * gpb;
+  for (uint32_t lp = blockIdx.x * gpb + gib; lp < d.L; lp += ngroups) {
+    const LaqWindowOut o = laq_lp_window<G>(d, q, ib, lp, s, bound, sm, g, err_slot);
     mn = min(mn, o.min_bits);
   }
   mn = block_min_u32(mn, red);
@@ -87,6 +89,7 @@ __device__ __forceinline__ void phold_laq_window_body(const PholdDev& d, const L
 }
 
 // Plain form: one launch per window; the kernel boundary is the barrier.
+template <int G>
 static __global__ void phold_laq_window(PholdDev d, LaqDev q, InsDev ib, uint32_t s) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ uint32_t red[32];
@@ -99,12 +102,13 @@ static __global__ void phold_laq_window(PholdDev d, LaqDev q, InsDev ib, uint32_
     d.ctrl->steps += 1ull;
     d.ctrl->phase = s + 1u;
   }
-  phold_laq_window_body(d, q, ib, s, m, smem_raw, red);
+  phold_laq_window_body<G>(d, q, ib, s, m, smem_raw, red);
 }
 
 // Persistent form: all windows in one cooperative launch; a bounded grid barrier
 // separates windows.  Every block takes the same exit decision from the same
 // (minimum, error) slot written before the barrier.
+template <int G>
 static __global__ void phold_laq_persistent(PholdDev d, LaqDev q, InsDev ib, uint32_t s0, uint32_t max_steps) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ uint32_t red[32];
@@ -120,7 +124,7 @@ static __global__ void phold_laq_persistent(PholdDev d, LaqDev q, InsDev ib, uin
       d.ctrl->errs[(s + 2u) % 3u] = 0u;
       d.ctrl->steps += 1ull;
     }
-    phold_laq_window_body(d, q, ib, s, m, smem_raw, red);
+    phold_laq_window_body<G>(d, q, ib, s, m, smem_raw, red);
     target += gridDim.x;
     if (!grid_barrier(&d.ctrl->bar, target, d.spin_limit, &d.ctrl->err)) {
       s += 1u;
@@ -128,6 +132,23 @@ static __global__ void phold_laq_persistent(PholdDev d, LaqDev q, InsDev ib, uin
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) d.ctrl->phase = s;
+}
+
+// Kernel pointers of one lane-group size (host-side dispatch).
+struct LaqKernelSet {
+  const void* window;
+  const void* persistent;
+  uint32_t group;
+};
+
+inline bool laq_kernel_set(uint32_t group, LaqKernelSet* out) {
+  switch (group) {
+    case 4: *out = {(const void*)phold_laq_window<4>, (const void*)phold_laq_persistent<4>, 4}; return true;
+    case 8: *out = {(const void*)phold_laq_window<8>, (const void*)phold_laq_persistent<8>, 8}; return true;
+    case 16: *out = {(const void*)phold_laq_window<16>, (const void*)phold_laq_persistent<16>, 16}; return true;
+    case 32: *out = {(const void*)phold_laq_window<32>, (const void*)phold_laq_persistent<32>, 32}; return true;
+  }
+  return false;
 }
 
 // End of run: committed total, pending events (ring + the unmerged children of the last

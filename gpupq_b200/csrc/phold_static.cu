@@ -72,7 +72,11 @@ gpq_status scratch_for_current_device(unsigned char** out) {
       gpq::set_last_error("cudaGetSymbolAddress(scratch) -> %s", cudaGetErrorString(e));
       return GPQ_ERR_CUDA;
     }
-    GPQ_CUDA_TRY(cudaFuncSetAttribute(phold_laq_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+    for (uint32_t grp : {4u, 8u, 16u, 32u}) {
+      LaqKernelSet ks;
+      laq_kernel_set(grp, &ks);
+      GPQ_CUDA_TRY(cudaFuncSetAttribute(ks.persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+    }
     GPQ_CUDA_TRY(cudaFuncSetAttribute(phold_laq_populate, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     g_scratch_dev[dev] = static_cast<unsigned char*>(p);
   }
@@ -117,7 +121,10 @@ extern "C" gpq_status gpq_phold_run_static(const gpq_phold_config* cfg_in, const
     return GPQ_ERR_INVALID;
   }
   const size_t pop_smem = (size_t)4 * c.events_per_lp * (sizeof(gpq_item) + sizeof(uint64_t));
-  const size_t win_smem = (size_t)(c.block_threads / 32) * laq_warp_smem_bytes(c.insert_capacity);
+  LaqKernelSet ks;
+  if (!laq_kernel_set(c.lanes_per_lp, &ks)) return GPQ_ERR_INVALID;
+  gpq::fit_block_to_smem(&c.block_threads, c.lanes_per_lp, laq_group_smem_bytes(c.insert_capacity), 96 * 1024);
+  const size_t win_smem = (size_t)(c.block_threads / c.lanes_per_lp) * laq_group_smem_bytes(c.insert_capacity);
   if (pop_smem > 200 * 1024 || win_smem > 96 * 1024) {
     gpq::set_last_error("gpq_phold_run_static: events_per_lp or insert_capacity too large for shared memory");
     return GPQ_ERR_INVALID;
@@ -153,17 +160,17 @@ extern "C" gpq_status gpq_phold_run_static(const gpq_phold_config* cfg_in, const
   GPQ_CUDA_TRY(cudaGetLastError());
 
   int per_sm = 0;
-  GPQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, phold_laq_persistent, (int)c.block_threads, win_smem));
+  GPQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ks.persistent, (int)c.block_threads, win_smem));
   if (per_sm <= 0) {
     gpq::set_last_error("gpq_phold_run_static: window kernel does not fit on an SM");
     return GPQ_ERR_INVALID;
   }
   if (c.ctas_per_sm) per_sm = std::min<int>(per_sm, (int)c.ctas_per_sm);
-  const uint32_t wpb = c.block_threads / 32;
-  uint32_t grid = std::min<uint32_t>((uint32_t)(per_sm * sms), std::max(1u, (c.num_lps + wpb - 1) / wpb));
+  const uint32_t gpb = c.block_threads / c.lanes_per_lp;
+  uint32_t grid = std::min<uint32_t>((uint32_t)(per_sm * sms), std::max(1u, (c.num_lps + gpb - 1) / gpb));
   uint32_t s0 = 0, maxs = c.max_steps;
   void* args[] = {&d, &q, &ib, &s0, &maxs};
-  GPQ_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)phold_laq_persistent, dim3(grid), dim3(c.block_threads), args,
+  GPQ_CUDA_TRY(cudaLaunchCooperativeKernel(ks.persistent, dim3(grid), dim3(c.block_threads), args,
                                            win_smem, s));
   const uint32_t fwpb = 8;
   phold_laq_finalize<<<std::max(1u, std::min<uint32_t>((c.num_lps + fwpb - 1) / fwpb, 4096u)), fwpb * 32, 0, s>>>(

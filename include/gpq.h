@@ -138,7 +138,8 @@ typedef struct gpq_phold_config {
   uint32_t block_threads;   /* CTA size (multiple of 32); 0 = tuned default */
   uint32_t ctas_per_sm;     /* persistent grid: CTAs per SM; 0 = occupancy maximum */
   uint32_t max_steps;       /* safety cap on windows; 0 = none */
-  uint32_t reserved[4];
+  uint32_t lanes_per_lp;    /* LAQ: lanes that work on one LP (4, 8, 16 or 32); 0 = tuned default */
+  uint32_t reserved[3];
 } gpq_phold_config;
 
 typedef struct gpq_phold_result {

@@ -16,6 +16,16 @@ def _oracle(cfgd, threads=0):
     return O.phold(O.make_cfg(**{k: v for k, v in cfgd.items() if k in keys}), threads)
 
 
+_ORACLE_CACHE = {}
+
+
+def _oracle_cached(cfgd):
+    key = tuple(sorted(cfgd.items()))
+    if key not in _ORACLE_CACHE:
+        _ORACLE_CACHE[key] = _oracle(cfgd, threads=8)
+    return _ORACLE_CACHE[key]
+
+
 def _run(cfgd, **kw):
     cfg = G.make_phold_config(**cfgd, **kw)
     with G.Phold(cfg) as h:
@@ -52,20 +62,22 @@ def test_children_match_oracle(gpu_lib):
 
 
 @pytest.mark.parametrize("loop", ["plain", "persistent"])
-def test_phold_plain_workload_bit_exact(gpu_lib, loop):
+@pytest.mark.parametrize("lanes", [4, 8, 16, 32])
+def test_phold_plain_workload_bit_exact(gpu_lib, loop, lanes):
     """1024 LPs x 16 events, lookahead 1.0, end 100, uniform destinations, seed 42."""
     o = _oracle(C1)
-    r, s = _run(C1, loop=loop)
+    r, s = _run(C1, loop=loop, lanes_per_lp=lanes)
     _assert_same(r, s, o)
     assert r["committed"] == 820705
 
 
-@pytest.mark.parametrize("loop", ["plain", "persistent"])
-def test_phold_large_reduced_bit_exact(gpu_lib, loop):
+@pytest.mark.parametrize("loop,lanes,block", [("plain", 8, 256), ("persistent", 4, 128), ("persistent", 8, 256),
+                                               ("persistent", 16, 512), ("persistent", 32, 256)])
+def test_phold_large_reduced_bit_exact(gpu_lib, loop, lanes, block):
     """The 65,536-LP ring workload cut to end time 3 (checked by the threaded oracle)."""
     cfgd = dict(num_lps=65536, events_per_lp=64, lookahead=0.1, end_time=3.0, seed=7, dest_mode=1, ring_width=16)
-    o = _oracle(cfgd, threads=8)
-    r, s = _run(cfgd, loop=loop, capacity=256, insert_capacity=64)
+    o = _oracle_cached(cfgd)
+    r, s = _run(cfgd, loop=loop, capacity=256, insert_capacity=64, lanes_per_lp=lanes, block_threads=block)
     _assert_same(r, s, o)
 
 
@@ -78,10 +90,10 @@ def test_phold_large_reduced_bit_exact(gpu_lib, loop):
      dict(capacity=512, insert_capacity=256)),
     (dict(num_lps=64, events_per_lp=4, lookahead=1.0, end_time=0.0, seed=2, dest_mode=0), {}),
 ])
-@pytest.mark.parametrize("loop", ["plain", "persistent"])
-def test_phold_edge_shapes(gpu_lib, cfgd, kw, loop):
+@pytest.mark.parametrize("loop,lanes", [("plain", 32), ("persistent", 4), ("persistent", 8), ("persistent", 32)])
+def test_phold_edge_shapes(gpu_lib, cfgd, kw, loop, lanes):
     o = _oracle(cfgd)
-    r, s = _run(cfgd, loop=loop, **kw)
+    r, s = _run(cfgd, loop=loop, lanes_per_lp=lanes, **kw)
     _assert_same(r, s, o)
 
 
