@@ -18,10 +18,10 @@ DEFAULT_CACHE = os.environ.get("GPQ_TUNE_CACHE", os.path.join(os.path.dirname(os
                                                               "tune_cache.json"))
 
 DEFAULT_SPACE = {
-    "lanes_per_lp": [4, 8, 16, 32],
-    "block_threads": [128, 256, 512],
+    "lanes_per_lp": [8, 16, 32],
+    "block_threads": [64, 128, 256],
     "ctas_per_sm": [0],
-    "insert_capacity": [64],
+    "insert_capacity": [32, 64],
 }
 
 

@@ -15,9 +15,11 @@
 //     sorted ring backwards in chunks of 4G items with 16-byte loads, moves every old
 //     item up by the number of new items below it (binary search in the sorted new keys)
 //     and drops the new items into the gaps -- one pass over the part of the ring that
-//     moves, instead of one pass per inserted item;
-//   * the drain reads the head G items at a time; a ballot finds the safe prefix and each
-//     lane handles one event (hashes, child, insert) in parallel.
+//     moves, instead of one pass per inserted item; the merged head is kept in shared
+//     memory for the drain;
+//   * the drain finds the safe prefix with a ballot and stages those events in shared
+//     memory; the whole CTA then processes the staged events one per thread (hashes,
+//     child, insert), so the event arithmetic runs on full warps.
 #pragma once
 
 #include "common.cuh"
@@ -83,34 +85,34 @@ struct LaneGroup {
   __device__ __forceinline__ uint32_t umin(uint32_t v) const { return __reduce_min_sync(mask, v); }
 };
 
-// Per-group shared memory used by the merge.
+// Per-group shared memory: the merge's new-key arrays and a copy of the merged head.
 struct LaqGroupSmem {
+  gpq_item* head;  // [G] first G items of the merged run (valid when the merge saw them all)
   uint64_t* ku;    // [ibc] new keys, arrival order
   uint64_t* ks;    // [ibc] new keys, sorted
   uint32_t* rk;    // [ibc] rank of the j-th new item
   uint32_t* hist;  // [ibc + 1] number of moved old items per shift
 };
 
-__host__ __device__ inline size_t laq_group_smem_bytes(uint32_t ibc) {
-  size_t b = (size_t)ibc * 8 * 2 + (size_t)ibc * 4 + (size_t)(ibc + 1) * 4;
+__host__ __device__ inline size_t laq_group_smem_bytes(uint32_t ibc, uint32_t group) {
+  size_t b = (size_t)group * 16 + (size_t)ibc * 8 * 2 + (size_t)ibc * 4 + (size_t)(ibc + 1) * 4;
   return (b + 15) & ~(size_t)15;
 }
 
-__device__ __forceinline__ LaqGroupSmem laq_group_smem(unsigned char* base, uint32_t ibc) {
+__device__ __forceinline__ LaqGroupSmem laq_group_smem(unsigned char* base, uint32_t ibc, uint32_t group) {
   LaqGroupSmem s;
-  s.ku = reinterpret_cast<uint64_t*>(base);
+  s.head = reinterpret_cast<gpq_item*>(base);
+  s.ku = reinterpret_cast<uint64_t*>(base + (size_t)group * 16);
   s.ks = s.ku + ibc;
   s.rk = reinterpret_cast<uint32_t*>(s.ks + ibc);
   s.hist = s.rk + ibc;
   return s;
 }
 
-// Merge the k unsorted items at `src` into the sorted ring run [rd, rd + n).
-// The caller guarantees n + k <= capacity.  All lanes of the group, convergent.
+// Ranks the k new items (keys -> smem ks in order, rk[j] = rank of item j); clears hist.
 template <int G>
-__device__ __forceinline__ void laq_merge(gpq_item* ring, uint32_t mask, uint32_t rd, uint32_t n,
-                                          const gpq_item* __restrict__ src, uint32_t k, const LaqGroupSmem& sm,
-                                          const LaneGroup<G>& g) {
+__device__ __forceinline__ void laq_rank_new(const gpq_item* __restrict__ src, uint32_t k, const LaqGroupSmem& sm,
+                                             const LaneGroup<G>& g) {
   for (uint32_t j = g.gl; j < k; j += G) sm.ku[j] = gpq_lp_key(src[j]);
   g.sync();
   for (uint32_t j = g.gl; j < k; j += G) {
@@ -122,40 +124,72 @@ __device__ __forceinline__ void laq_merge(gpq_item* ring, uint32_t mask, uint32_
   }
   for (uint32_t h = g.gl; h <= k; h += G) sm.hist[h] = 0;
   g.sync();
+}
 
-  constexpr int U = 4;  // items per lane per chunk
+__device__ __forceinline__ uint32_t laq_count_below(const uint64_t* ks, uint32_t k, uint64_t key) {
+  uint32_t a = 0, b = k;
+  while (a < b) {
+    const uint32_t mid = (a + b) >> 1;
+    if (ks[mid] < key) a = mid + 1; else b = mid;
+  }
+  return a;
+}
+
+// Merge the k unsorted items at `src` into the sorted ring run [rd, rd + n) (n + k <=
+// capacity).  Old items are visited backwards in chunks of 4G (lane-strided); an item
+// moves up by the number of new items below it (binary search in the sorted new keys),
+// and the new items then drop into the gaps.  Items whose merged position is below G are also copied to
+// sm.head.  Returns true when sm.head holds the complete merged head (every item that
+// ends below position G was visited).  All lanes of the group, convergent.
+template <int G>
+__device__ __forceinline__ bool laq_merge(gpq_item* ring, uint32_t mask, uint32_t rd, uint32_t n,
+                                          const gpq_item* __restrict__ src, uint32_t k, const LaqGroupSmem& sm,
+                                          const LaneGroup<G>& g) {
+  constexpr int U = 4;  // consecutive items per lane per chunk
   int32_t hi = (int32_t)n;
+  int32_t lo = hi > U * G ? hi - U * G : 0;
+  gpq_item o[U];
+  // The first (topmost) chunk is loaded before the new items are ranked so that both
+  // loads are in flight together.
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const int32_t i = lo + u * G + (int32_t)g.gl;
+    if (i < hi) o[u] = ring[(rd + (uint32_t)i) & mask];
+  }
+  laq_rank_new<G>(src, k, sm, g);
+  bool complete = true;
   while (hi > 0) {
-    const int32_t lo = hi > U * G ? hi - U * G : 0;
-    gpq_item o[U];
     uint32_t sh[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int32_t i = lo + u * G + (int32_t)g.gl;
-      sh[u] = 0;
-      if (i < hi) {
-        o[u] = ring[(rd + (uint32_t)i) & mask];
-        const uint64_t key = gpq_lp_key(o[u]);
-        uint32_t a = 0, b = k;
-        while (a < b) {
-          const uint32_t mid = (a + b) >> 1;
-          if (sm.ks[mid] < key) a = mid + 1; else b = mid;
-        }
-        sh[u] = a;  // number of new items below this old item
-      }
+      sh[u] = (i < hi) ? laq_count_below(sm.ks, k, gpq_lp_key(o[u])) : 0u;
     }
     const uint32_t sh_lo = g.shfl(sh[0], 0);  // shift of item `lo`, the chunk's smallest
     g.sync();                                 // every load of the chunk precedes every store
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int32_t i = lo + u * G + (int32_t)g.gl;
-      if (i < hi && sh[u] > 0) {
-        ring[(rd + (uint32_t)i + sh[u]) & mask] = o[u];
-        atomicAdd(&sm.hist[sh[u]], 1u);
+      if (i < hi) {
+        const uint32_t pos = (uint32_t)i + sh[u];
+        if (sh[u] > 0) {
+          ring[(rd + pos) & mask] = o[u];
+          atomicAdd(&sm.hist[sh[u]], 1u);
+        }
+        if (pos < (uint32_t)G) sm.head[pos] = o[u];
       }
     }
-    if (sh_lo == 0) break;  // shifts are non-decreasing: nothing below `lo` moves
+    if (sh_lo == 0) {  // shifts are non-decreasing: nothing below `lo` moves
+      complete = (lo == 0);  // unvisited items [0, lo) keep positions below lo
+      break;
+    }
     hi = lo;
+    lo = hi > U * G ? hi - U * G : 0;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int32_t i = lo + u * G + (int32_t)g.gl;
+      if (i < hi) o[u] = ring[(rd + (uint32_t)i) & mask];
+    }
   }
   g.sync();
   // New item of rank r lands after the n - (#old items with shift > r) old items below it.
@@ -163,36 +197,90 @@ __device__ __forceinline__ void laq_merge(gpq_item* ring, uint32_t mask, uint32_
     const uint32_t r = sm.rk[j];
     uint32_t gt = 0;
     for (uint32_t h = r + 1; h <= k; ++h) gt += sm.hist[h];
-    ring[(rd + r + n - gt) & mask] = src[j];
+    const uint32_t pos = r + n - gt;
+    const gpq_item it = src[j];
+    ring[(rd + pos) & mask] = it;
+    if (pos < (uint32_t)G) sm.head[pos] = it;
   }
   g.sync();
+  return complete;
 }
 
-// Result of one LP's window.
-struct LaqWindowOut {
-  uint32_t committed;
-  uint32_t min_bits;  // min over the LP's new head and the children's timestamps
+// Per-LP state read at the start of its window (prefetched one LP ahead).
+struct LaqMeta {
+  uint32_t k, rd, wr, count;
+  unsigned long long csum, ohash;
 };
 
-// One LP, one window s: merge the children of window s-1, then drain every event with
-// ts < bound (= m_s + lookahead) and ts < end_time, in key order, inserting the children
-// into the window-s insert buffers.  All lanes of the group, convergent.
+__device__ __forceinline__ LaqMeta laq_load_meta(const PholdDev& d, const LaqDev& q, const InsDev& ib, uint32_t lp,
+                                                 uint32_t prevb) {
+  LaqMeta m;
+  m.k = ib.cnt[(size_t)prevb * d.L + lp];
+  m.rd = q.rd[lp];
+  m.wr = q.wr[lp];
+  m.count = d.count[lp];
+  m.csum = d.csum[lp];
+  m.ohash = d.ohash[lp];
+  return m;
+}
+
+static constexpr uint32_t kStageHole = 0xffffffffu;  // aux of a reserved but unused staging slot
+
+// Per-CTA shared staging of one super-round: the safe events found by the lane groups
+// (aux = slot << 16 | index in the LP's safe prefix) and per-LP-slot accumulators.
+struct LaqStage {
+  gpq_item* ev;              // [cap] staged events
+  uint32_t* cnt;             // number of staged events
+  uint32_t* seq0;            // [slots] LP's committed count before this window
+  unsigned long long* csum;  // [slots] LP checksum (value before the window + this window's events)
+  unsigned long long* ohash; // [slots]
+  uint32_t* lp;              // [slots] LP of the slot (~0u = unused)
+  uint32_t cap;
+};
+
+// Process one safe event: per-LP hashes into the slot accumulators, the child into the
+// window's insert buffers.  Returns the child's timestamp bits.
+__device__ __forceinline__ uint32_t laq_process_event(const PholdDev& d, const InsDev& ib, const LaqStage& st,
+                                                      const gpq_item e, uint32_t curb, uint32_t* err_slot) {
+  const uint32_t slot = e.aux >> 16;
+  const uint32_t idx = e.aux & 0xffffu;
+  const uint32_t tb = gpq_f2u(e.ts);
+  const uint64_t h = gpq_ev_hash(e.id, tb);
+  atomicAdd(&st.csum[slot], (unsigned long long)h);
+  atomicAdd(&st.ohash[slot], (unsigned long long)gpq_seq_hash(h, (uint64_t)st.seq0[slot] + idx));
+  gpq_item pe = e;
+  pe.aux = e.lp;
+  const gpq_item ch = gpq_phold_child(d.p, pe);
+  const uint32_t pos = atomicAdd(&ib.cnt[(size_t)curb * d.L + ch.lp], 1u);
+  if (pos < ib.ibc) {
+    ib.buf[((size_t)curb * d.L + ch.lp) * ib.ibc + pos] = ch;
+  } else {
+    gpq_set_error(&d.ctrl->err, GPQ_ERR_INSERT_FULL);
+    atomicOr(err_slot, 1u);
+  }
+  return gpq_f2u(ch.ts);
+}
+
+// One LP, one window s, first pass: merge the children of window s-1, then find the
+// safe prefix (ts < bound = m_s + lookahead and ts < end_time) and stage it for the
+// CTA-wide event pass; advance fel_read past it.  If the staging area is full the
+// group processes its events itself.  Returns the new head's timestamp bits, min'ed
+// with any child processed here.  All lanes of the group, convergent.
 template <int G>
-__device__ __forceinline__ LaqWindowOut laq_lp_window(const PholdDev& d, const LaqDev& q, const InsDev& ib,
-                                                      uint32_t lp, uint32_t s, float bound, const LaqGroupSmem& sm,
-                                                      const LaneGroup<G>& g, uint32_t* err_slot) {
+__device__ __forceinline__ uint32_t laq_lp_stage(const PholdDev& d, const LaqDev& q, const InsDev& ib,
+                                                 uint32_t lp, uint32_t slot, uint32_t s, float bound,
+                                                 const LaqGroupSmem& sm, const LaqStage& st, const LaneGroup<G>& g,
+                                                 uint32_t* err_slot, const LaqMeta& mt) {
   const uint32_t L = d.L;
   const uint32_t prevb = (s + 1u) & 1u, curb = s & 1u;
   const uint32_t cap = 1u << q.cap_log2, mask = cap - 1u;
   gpq_item* ring = q.ring + ((size_t)lp << q.cap_log2);
   const float T = d.p.end_time;
 
-  uint32_t k = ib.cnt[(size_t)prevb * L + lp];
-  const uint32_t rd = q.rd[lp];
-  uint32_t wr = q.wr[lp];
-  const uint32_t seq0 = d.count[lp];
-  uint32_t n = wr - rd;
-
+  uint32_t k = mt.k;
+  const uint32_t rd = mt.rd;
+  uint32_t n = mt.wr - rd;
+  bool head_in_smem = false;
   if (k > 0) {
     if (k > ib.ibc) k = ib.ibc;  // overflow was flagged by the inserter
     if (n + k > cap) {
@@ -200,44 +288,49 @@ __device__ __forceinline__ LaqWindowOut laq_lp_window(const PholdDev& d, const L
       k = cap - n;
     }
     const gpq_item* src = ib.buf + ((size_t)prevb * L + lp) * ib.ibc;
-    laq_merge<G>(ring, mask, rd, n, src, k, sm, g);
+    head_in_smem = laq_merge<G>(ring, mask, rd, n, src, k, sm, g);
     n += k;
-    wr += k;
     if (g.gl == 0) {
-      q.wr[lp] = wr;
+      q.wr[lp] = mt.wr + k;
       ib.cnt[(size_t)prevb * L + lp] = 0;
     }
   }
 
-  // Drain the safe prefix.
-  uint32_t done = 0;
-  uint64_t acc_cs = 0, acc_oh = 0;
-  uint32_t cmin = kInfBits, head = kInfBits;
-  gpq_item* const ins_base = ib.buf + (size_t)curb * L * ib.ibc;
-  uint32_t* const ins_cnt = ib.cnt + (size_t)curb * L;
+  if (g.gl == 0) {  // slot accumulators start from the LP's values before this window
+    st.seq0[slot] = mt.count;
+    st.csum[slot] = mt.csum;
+    st.ohash[slot] = mt.ohash;
+  }
+  g.sync();
+  uint32_t done = 0, head = kInfBits, cmin = kInfBits;
   while (done < n) {
     const uint32_t i = done + g.gl;
     gpq_item e;
     bool safe = false;
     if (i < n) {
-      e = ring[(rd + i) & mask];
+      e = (head_in_smem && i < (uint32_t)G) ? sm.head[i] : ring[(rd + i) & mask];
       safe = (e.ts < bound) && (e.ts < T);
     }
-    const uint32_t c = __popc(g.ballot(safe));  // ring is sorted: the safe items form a prefix
-    if (safe) {
-      const uint32_t tb = gpq_f2u(e.ts);
-      const uint64_t h = gpq_ev_hash(e.id, tb);
-      acc_cs += h;
-      acc_oh += gpq_seq_hash(h, (uint64_t)seq0 + i);
-      const gpq_item ch = gpq_phold_child(d.p, e);
-      const uint32_t slot = atomicAdd(&ins_cnt[ch.lp], 1u);
-      if (slot < ib.ibc) {
-        ins_base[(size_t)ch.lp * ib.ibc + slot] = ch;
-      } else {
-        gpq_set_error(&d.ctrl->err, GPQ_ERR_INSERT_FULL);
-        atomicOr(err_slot, 1u);
+    const uint32_t c = __popc(g.ballot(safe));  // the run is sorted: safe items form a prefix
+    if (c > 0) {
+      uint32_t base = 0;
+      if (g.gl == 0) base = atomicAdd(st.cnt, c);
+      base = g.shfl(base, 0);
+      if (safe) {
+        e.aux = (slot << 16) | i;
+        if (base + c <= st.cap) {
+          st.ev[base + g.gl] = e;
+        } else {
+          // Staging full: handle the event here, and mark the reserved slot that lies
+          // inside the area as empty so that the event pass skips it.
+          if (base + g.gl < st.cap) {
+            gpq_item hole = e;
+            hole.aux = kStageHole;
+            st.ev[base + g.gl] = hole;
+          }
+          cmin = min(cmin, laq_process_event(d, ib, st, e, curb, err_slot));
+        }
       }
-      cmin = min(cmin, gpq_f2u(ch.ts));
     }
     if (c < (uint32_t)G) {
       head = g.shfl((i < n) ? gpq_f2u(e.ts) : kInfBits, c);
@@ -246,17 +339,12 @@ __device__ __forceinline__ LaqWindowOut laq_lp_window(const PholdDev& d, const L
     }
     done += G;
   }
-  acc_cs = g.sum(acc_cs);
-  acc_oh = g.sum(acc_oh);
-  cmin = g.umin(cmin);
-  if (g.gl == 0 && done > 0) {
-    d.count[lp] = seq0 + done;
-    d.csum[lp] += acc_cs;
-    d.ohash[lp] += acc_oh;
-    q.rd[lp] = rd + done;
+  if (g.gl == 0) {
+    st.lp[slot] = done > 0 ? lp : ~0u;  // the event pass writes the checksums back
+    if (done > 0) {
+      d.count[lp] = mt.count + done;
+      q.rd[lp] = rd + done;
+    }
   }
-  LaqWindowOut out;
-  out.committed = done;
-  out.min_bits = min(cmin, head);
-  return out;
+  return min(head, g.umin(cmin));
 }

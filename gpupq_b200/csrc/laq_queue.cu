@@ -15,7 +15,7 @@ __global__ void laq_post_kernel(LaqDev q, gpq_item* ibuf, uint32_t* icnt, uint32
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const LaneGroup<32> g;
   const uint32_t wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  const LaqGroupSmem sm = laq_group_smem(smem_raw + (size_t)wib * laq_group_smem_bytes(ibc), ibc);
+  const LaqGroupSmem sm = laq_group_smem(smem_raw + (size_t)wib * laq_group_smem_bytes(ibc, 32), ibc, 32);
   const uint32_t cap = 1u << q.cap_log2, mask = cap - 1u;
   for (uint32_t lp = blockIdx.x * wpb + wib; lp < L; lp += gridDim.x * wpb) {
     uint32_t k = min(icnt[lp], ibc);
@@ -101,7 +101,7 @@ class LaqQueue final : public LocalQueueBase {
     GPQ_CUDA_TRY(cudaMalloc(&wr_, (size_t)L_ * sizeof(uint32_t)));
     GPQ_CUDA_TRY(cudaMemsetAsync(rd_, 0, (size_t)L_ * sizeof(uint32_t), own_));
     GPQ_CUDA_TRY(cudaMemsetAsync(wr_, 0, (size_t)L_ * sizeof(uint32_t), own_));
-    const size_t smem = 8 * laq_group_smem_bytes(ibc_);
+    const size_t smem = 8 * laq_group_smem_bytes(ibc_, 32);
     GPQ_CUDA_TRY(cudaFuncSetAttribute(laq_post_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     GPQ_CUDA_TRY(cudaStreamSynchronize(own_));
     return GPQ_OK;
@@ -109,7 +109,7 @@ class LaqQueue final : public LocalQueueBase {
 
   gpq_status post(cudaStream_t st) override {
     const uint32_t grid = std::max(1u, std::min<uint32_t>((L_ + 7) / 8, 8192));
-    laq_post_kernel<<<grid, 256, 8 * laq_group_smem_bytes(ibc_), st>>>(dev(), ibuf_, icnt_, ibc_, L_, ctr_);
+    laq_post_kernel<<<grid, 256, 8 * laq_group_smem_bytes(ibc_, 32), st>>>(dev(), ibuf_, icnt_, ibc_, L_, ctr_);
     GPQ_CUDA_TRY(cudaGetLastError());
     return take_error(st);
   }

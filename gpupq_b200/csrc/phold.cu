@@ -79,7 +79,7 @@ struct gpq_phold {
   LaqDev laq() const { return LaqDev{ring, rd, wr, cap_log2}; }
   InsDev ins() const { return InsDev{ibuf, icnt, cfg.insert_capacity}; }
   LaqKernelSet ks{};
-  size_t window_smem() const { return (size_t)(block / ks.group) * laq_group_smem_bytes(cfg.insert_capacity); }
+  size_t window_smem() const { return phold_window_smem_bytes(block, ks.group, cfg.insert_capacity); }
 
   ~gpq_phold() {
     for (void* p : {(void*)ring, (void*)rd, (void*)wr, (void*)ibuf, (void*)icnt, (void*)count, (void*)csum,
@@ -147,7 +147,10 @@ gpq_status gpq_phold_create(const gpq_phold_config* cfg_in, gpq_phold** out) {
   TRY(cudaMalloc(&h->acc, sizeof(PholdAcc)));
   TRY(cudaMallocHost(&h->h_ctrl, sizeof(PholdCtrl)));
   if (!laq_kernel_set(c.lanes_per_lp, &h->ks)) return fail(GPQ_ERR_INVALID);
-  if (!gpq::fit_block_to_smem(&h->block, h->ks.group, laq_group_smem_bytes(c.insert_capacity), 200 * 1024)) {
+  if (!gpq::fit_block_to_smem(&h->block, h->ks.group,
+                              laq_group_smem_bytes(c.insert_capacity, h->ks.group) +
+                                  24 * kStageRounds,
+                              200 * 1024 - 4096 * 16 - 16)) {
     gpq::set_last_error("insert_capacity %u needs too much shared memory per lane group", c.insert_capacity);
     return fail(GPQ_ERR_INVALID);
   }

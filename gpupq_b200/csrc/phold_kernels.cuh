@@ -65,9 +65,31 @@ static __global__ void phold_laq_populate(PholdDev d, LaqDev q, uint32_t per_lp,
   if (threadIdx.x == 0 && mn != kInfBits) atomicMin(&d.ctrl->mins[0], mn);
 }
 
-// Shared body of one window for all LPs owned by this block's lane groups
-// (LP = global group index + k * total groups).  Folds the block's minimum into
-// mins[(s+1)%3].
+// Per-CTA staging of one super-round (shared memory): room for 8 safe events per LP on
+// average; a lane group that finds the area full handles its events itself.
+static constexpr uint32_t kStageRounds = 4;  // rounds (LPs per lane group) per super-round
+
+__host__ __device__ inline uint32_t phold_stage_cap(uint32_t block, uint32_t group) {
+  const uint32_t c = kStageRounds * (block / group) * 8u;
+  return c < 512u ? 512u : (c > 4096u ? 4096u : c);
+}
+
+__host__ __device__ inline size_t phold_stage_smem_bytes(uint32_t block, uint32_t group) {
+  const size_t slots = (size_t)kStageRounds * (block / group);
+  return (size_t)phold_stage_cap(block, group) * 16 + slots * (8 + 8 + 4 + 4) + 16;
+}
+
+__host__ __device__ inline size_t phold_window_smem_bytes(uint32_t block, uint32_t group, uint32_t ibc) {
+  return (size_t)(block / group) * laq_group_smem_bytes(ibc, group) + phold_stage_smem_bytes(block, group);
+}
+
+// Shared body of one window for all LPs owned by this CTA.  The CTA's LPs are
+// lp = blockIdx.x * gpb + gib + r * ngroups for rounds r = 0, 1, ...; they are handled
+// in super-rounds of kStageRounds rounds, each in three passes:
+//   A  every lane group merges and stages its LP of each round (lane-group parallel);
+//   B  every thread of the CTA processes staged events (one event per thread);
+//   C  per-LP checksums go back to global memory.
+// Folds the CTA's minimum into mins[(s+1)%3].
 template <int G>
 __device__ __forceinline__ void phold_laq_window_body(const PholdDev& d, const LaqDev& q, const InsDev& ib,
                                                       uint32_t s, float m, unsigned char* smem_raw,
@@ -75,14 +97,56 @@ __device__ __forceinline__ void phold_laq_window_body(const PholdDev& d, const L
   const LaneGroup<G> g;
   const uint32_t gib = threadIdx.x / G;  // group in block
   const uint32_t gpb = blockDim.x / G;
-  const LaqGroupSmem sm = laq_group_smem(smem_raw + (size_t)gib * laq_group_smem_bytes(ib.ibc), ib.ibc);
+  const size_t gbytes = laq_group_smem_bytes(ib.ibc, G);
+  const LaqGroupSmem sm = laq_group_smem(smem_raw + (size_t)gib * gbytes, ib.ibc, G);
+  unsigned char* sbase = smem_raw + (size_t)gpb * gbytes;
+  const uint32_t nslots = kStageRounds * gpb;
+  const uint32_t stage_cap = phold_stage_cap(blockDim.x, G);
+  LaqStage st;
+  st.ev = reinterpret_cast<gpq_item*>(sbase);
+  st.csum = reinterpret_cast<unsigned long long*>(sbase + (size_t)stage_cap * 16);
+  st.ohash = st.csum + nslots;
+  st.seq0 = reinterpret_cast<uint32_t*>(st.ohash + nslots);
+  st.lp = st.seq0 + nslots;
+  st.cnt = st.lp + nslots;
+  st.cap = stage_cap;
+
   const float bound = GPQ_FADD(m, d.p.lookahead);
   uint32_t* err_slot = &d.ctrl->errs[(s + 1u) % 3u];
-  uint32_t mn = kInfBits;
+  const uint32_t prevb = (s + 1u) & 1u, curb = s & 1u;
   const uint32_t ngroups = gridDim.x * gpb;
-  for (uint32_t lp = blockIdx.x * gpb + gib; lp < d.L; lp += ngroups) {
-    const LaqWindowOut o = laq_lp_window<G>(d, q, ib, lp, s, bound, sm, g, err_slot);
-    mn = min(mn, o.min_bits);
+  const uint32_t first = blockIdx.x * gpb;
+  uint32_t mn = kInfBits;
+  for (uint32_t r0 = 0; first + r0 * ngroups < d.L; r0 += kStageRounds) {
+    if (threadIdx.x == 0) *st.cnt = 0;
+    for (uint32_t t = threadIdx.x; t < nslots; t += blockDim.x) st.lp[t] = ~0u;
+    __syncthreads();
+    // A: merge + stage, one LP per lane group per round (metadata prefetched one round ahead)
+    uint32_t lp = first + gib + r0 * ngroups;
+    LaqMeta next;
+    if (lp < d.L) next = laq_load_meta(d, q, ib, lp, prevb);
+    for (uint32_t r = 0; r < kStageRounds && lp < d.L; ++r, lp += ngroups) {
+      const LaqMeta cur = next;
+      if (r + 1 < kStageRounds && lp + ngroups < d.L) next = laq_load_meta(d, q, ib, lp + ngroups, prevb);
+      mn = min(mn, laq_lp_stage<G>(d, q, ib, lp, r * gpb + gib, s, bound, sm, st, g, err_slot, cur));
+    }
+    __syncthreads();
+    // B: one staged event per thread
+    const uint32_t ns = min(*st.cnt, st.cap);
+    for (uint32_t t = threadIdx.x; t < ns; t += blockDim.x) {
+      const gpq_item e = st.ev[t];
+      if (e.aux != kStageHole) mn = min(mn, laq_process_event(d, ib, st, e, curb, err_slot));
+    }
+    __syncthreads();
+    // C: checksums back to the LPs that committed events
+    for (uint32_t t = threadIdx.x; t < nslots; t += blockDim.x) {
+      const uint32_t l = st.lp[t];
+      if (l != ~0u) {
+        d.csum[l] = st.csum[t];
+        d.ohash[l] = st.ohash[t];
+      }
+    }
+    __syncthreads();
   }
   mn = block_min_u32(mn, red);
   if (threadIdx.x == 0 && mn != kInfBits) atomicMin(&d.ctrl->mins[(s + 1u) % 3u], mn);

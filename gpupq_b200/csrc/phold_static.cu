@@ -123,8 +123,11 @@ extern "C" gpq_status gpq_phold_run_static(const gpq_phold_config* cfg_in, const
   const size_t pop_smem = (size_t)4 * c.events_per_lp * (sizeof(gpq_item) + sizeof(uint64_t));
   LaqKernelSet ks;
   if (!laq_kernel_set(c.lanes_per_lp, &ks)) return GPQ_ERR_INVALID;
-  gpq::fit_block_to_smem(&c.block_threads, c.lanes_per_lp, laq_group_smem_bytes(c.insert_capacity), 96 * 1024);
-  const size_t win_smem = (size_t)(c.block_threads / c.lanes_per_lp) * laq_group_smem_bytes(c.insert_capacity);
+  gpq::fit_block_to_smem(&c.block_threads, c.lanes_per_lp,
+                         laq_group_smem_bytes(c.insert_capacity, c.lanes_per_lp) +
+                             24 * kStageRounds,
+                         96 * 1024 - 4096 * 16 - 16);
+  const size_t win_smem = phold_window_smem_bytes(c.block_threads, c.lanes_per_lp, c.insert_capacity);
   if (pop_smem > 200 * 1024 || win_smem > 96 * 1024) {
     gpq::set_last_error("gpq_phold_run_static: events_per_lp or insert_capacity too large for shared memory");
     return GPQ_ERR_INVALID;

@@ -89,6 +89,10 @@ def test_phold_large_reduced_bit_exact(gpu_lib, loop, lanes, block):
     (dict(num_lps=333, events_per_lp=200, lookahead=0.02, end_time=2.0, seed=13, dest_mode=1, ring_width=1),
      dict(capacity=512, insert_capacity=256)),
     (dict(num_lps=64, events_per_lp=4, lookahead=1.0, end_time=0.0, seed=2, dest_mode=0), {}),
+    # lookahead far above the spread: nearly every queued event is safe in every window,
+    # which overflows the per-warp staging area and exercises the in-group fallback
+    (dict(num_lps=3000, events_per_lp=60, lookahead=20.0, end_time=60.0, seed=17, dest_mode=1, ring_width=4),
+     dict(capacity=256, insert_capacity=256)),
 ])
 @pytest.mark.parametrize("loop,lanes", [("plain", 32), ("persistent", 4), ("persistent", 8), ("persistent", 32)])
 def test_phold_edge_shapes(gpu_lib, cfgd, kw, loop, lanes):
