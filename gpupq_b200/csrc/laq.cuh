@@ -22,67 +22,13 @@
 //     child, insert), so the event arithmetic runs on full warps.
 #pragma once
 
-#include "common.cuh"
-#include "gpq/model.h"
+#include "phold_common.cuh"
 
 struct LaqDev {
   gpq_item* ring;  // num_lps << cap_log2 items
   uint32_t* rd;    // per-LP read counter (fel_read); slot = counter & (cap - 1)
   uint32_t* wr;    // per-LP write counter (fel_write)
   uint32_t cap_log2;
-};
-
-struct InsDev {
-  gpq_item* buf;  // [2][num_lps][ibc]
-  uint32_t* cnt;  // [2][num_lps]
-  uint32_t ibc;
-};
-
-// Control words of one PHOLD instance (device memory).
-struct PholdCtrl {
-  uint32_t mins[3];  // window minimum slots (float bits), rotating by window index
-  uint32_t errs[3];  // per-window error slots, rotating like mins
-  uint32_t err;      // sticky error word reported to the host
-  uint32_t phase;    // index of the next window to run
-  unsigned long long bar;    // grid-barrier arrival counter (persistent launch)
-  unsigned long long steps;  // windows executed
-};
-
-struct PholdDev {
-  gpq_phold_params p;
-  uint32_t L;
-  uint32_t* count;
-  unsigned long long* csum;
-  unsigned long long* ohash;
-  PholdCtrl* ctrl;
-  uint64_t spin_limit;
-};
-
-// A group of G consecutive lanes of one warp working on one LP.
-template <int G>
-struct LaneGroup {
-  static_assert(G == 4 || G == 8 || G == 16 || G == 32, "group size");
-  uint32_t gl;    // lane within the group
-  uint32_t base;  // first lane of the group
-  uint32_t mask;  // the group's lanes
-  __device__ __forceinline__ LaneGroup() {
-    const uint32_t lane = threadIdx.x & 31u;
-    gl = lane & (G - 1);
-    base = lane & ~(uint32_t)(G - 1);
-    mask = (G == 32) ? GPQ_FULL_MASK : (((1u << G) - 1u) << base);
-  }
-  __device__ __forceinline__ void sync() const { __syncwarp(mask); }
-  __device__ __forceinline__ uint32_t ballot(bool p) const {
-    const uint32_t b = __ballot_sync(mask, p);
-    return (G == 32) ? b : ((b >> base) & ((1u << G) - 1u));
-  }
-  __device__ __forceinline__ uint32_t shfl(uint32_t v, uint32_t src) const { return __shfl_sync(mask, v, src, G); }
-  __device__ __forceinline__ uint64_t sum(uint64_t v) const {
-#pragma unroll
-    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, G);
-    return v;
-  }
-  __device__ __forceinline__ uint32_t umin(uint32_t v) const { return __reduce_min_sync(mask, v); }
 };
 
 // Per-group shared memory: the merge's new-key arrays and a copy of the merged head.
@@ -224,52 +170,14 @@ __device__ __forceinline__ LaqMeta laq_load_meta(const PholdDev& d, const LaqDev
   return m;
 }
 
-static constexpr uint32_t kStageHole = 0xffffffffu;  // aux of a reserved but unused staging slot
-
-// Per-CTA shared staging of one super-round: the safe events found by the lane groups
-// (aux = slot << 16 | index in the LP's safe prefix) and per-LP-slot accumulators.
-struct LaqStage {
-  gpq_item* ev;              // [cap] staged events
-  uint32_t* cnt;             // number of staged events
-  uint32_t* seq0;            // [slots] LP's committed count before this window
-  unsigned long long* csum;  // [slots] LP checksum (value before the window + this window's events)
-  unsigned long long* ohash; // [slots]
-  uint32_t* lp;              // [slots] LP of the slot (~0u = unused)
-  uint32_t cap;
-};
-
-// Process one safe event: per-LP hashes into the slot accumulators, the child into the
-// window's insert buffers.  Returns the child's timestamp bits.
-__device__ __forceinline__ uint32_t laq_process_event(const PholdDev& d, const InsDev& ib, const LaqStage& st,
-                                                      const gpq_item e, uint32_t curb, uint32_t* err_slot) {
-  const uint32_t slot = e.aux >> 16;
-  const uint32_t idx = e.aux & 0xffffu;
-  const uint32_t tb = gpq_f2u(e.ts);
-  const uint64_t h = gpq_ev_hash(e.id, tb);
-  atomicAdd(&st.csum[slot], (unsigned long long)h);
-  atomicAdd(&st.ohash[slot], (unsigned long long)gpq_seq_hash(h, (uint64_t)st.seq0[slot] + idx));
-  gpq_item pe = e;
-  pe.aux = e.lp;
-  const gpq_item ch = gpq_phold_child(d.p, pe);
-  const uint32_t pos = atomicAdd(&ib.cnt[(size_t)curb * d.L + ch.lp], 1u);
-  if (pos < ib.ibc) {
-    ib.buf[((size_t)curb * d.L + ch.lp) * ib.ibc + pos] = ch;
-  } else {
-    gpq_set_error(&d.ctrl->err, GPQ_ERR_INSERT_FULL);
-    atomicOr(err_slot, 1u);
-  }
-  return gpq_f2u(ch.ts);
-}
-
 // One LP, one window s, first pass: merge the children of window s-1, then find the
 // safe prefix (ts < bound = m_s + lookahead and ts < end_time) and stage it for the
-// CTA-wide event pass; advance fel_read past it.  If the staging area is full the
-// group processes its events itself.  Returns the new head's timestamp bits, min'ed
-// with any child processed here.  All lanes of the group, convergent.
+// CTA-wide event pass; advance fel_read past it.  Returns the new head's timestamp
+// bits, min'ed with any child processed here.  All lanes of the group, convergent.
 template <int G>
 __device__ __forceinline__ uint32_t laq_lp_stage(const PholdDev& d, const LaqDev& q, const InsDev& ib,
                                                  uint32_t lp, uint32_t slot, uint32_t s, float bound,
-                                                 const LaqGroupSmem& sm, const LaqStage& st, const LaneGroup<G>& g,
+                                                 const LaqGroupSmem& sm, const PholdStage& st, const LaneGroup<G>& g,
                                                  uint32_t* err_slot, const LaqMeta& mt) {
   const uint32_t L = d.L;
   const uint32_t prevb = (s + 1u) & 1u, curb = s & 1u;
@@ -296,11 +204,7 @@ __device__ __forceinline__ uint32_t laq_lp_stage(const PholdDev& d, const LaqDev
     }
   }
 
-  if (g.gl == 0) {  // slot accumulators start from the LP's values before this window
-    st.seq0[slot] = mt.count;
-    st.csum[slot] = mt.csum;
-    st.ohash[slot] = mt.ohash;
-  }
+  if (g.gl == 0) phold_stage_slot_init(st, slot, mt.count, mt.csum, mt.ohash);
   g.sync();
   uint32_t done = 0, head = kInfBits, cmin = kInfBits;
   while (done < n) {
@@ -312,26 +216,7 @@ __device__ __forceinline__ uint32_t laq_lp_stage(const PholdDev& d, const LaqDev
       safe = (e.ts < bound) && (e.ts < T);
     }
     const uint32_t c = __popc(g.ballot(safe));  // the run is sorted: safe items form a prefix
-    if (c > 0) {
-      uint32_t base = 0;
-      if (g.gl == 0) base = atomicAdd(st.cnt, c);
-      base = g.shfl(base, 0);
-      if (safe) {
-        e.aux = (slot << 16) | i;
-        if (base + c <= st.cap) {
-          st.ev[base + g.gl] = e;
-        } else {
-          // Staging full: handle the event here, and mark the reserved slot that lies
-          // inside the area as empty so that the event pass skips it.
-          if (base + g.gl < st.cap) {
-            gpq_item hole = e;
-            hole.aux = kStageHole;
-            st.ev[base + g.gl] = hole;
-          }
-          cmin = min(cmin, laq_process_event(d, ib, st, e, curb, err_slot));
-        }
-      }
-    }
+    cmin = min(cmin, phold_stage_batch<G>(d, ib, st, g, e, safe, i, c, slot, curb, err_slot));
     if (c < (uint32_t)G) {
       head = g.shfl((i < n) ? gpq_f2u(e.ts) : kInfBits, c);
       done += c;
@@ -348,3 +233,22 @@ __device__ __forceinline__ uint32_t laq_lp_stage(const PholdDev& d, const LaqDev
   }
   return min(head, g.umin(cmin));
 }
+
+// Local array queue as a PHOLD engine policy.
+template <int G_>
+struct LaqPolicy {
+  static constexpr int G = G_;
+  using Dev = LaqDev;
+  using Meta = LaqMeta;
+  using Smem = LaqGroupSmem;
+  __host__ __device__ static size_t group_smem_bytes(uint32_t ibc) { return laq_group_smem_bytes(ibc, G); }
+  __device__ static Smem smem(unsigned char* base, uint32_t ibc) { return laq_group_smem(base, ibc, G); }
+  __device__ static Meta load_meta(const PholdDev& d, const Dev& q, const InsDev& ib, uint32_t lp, uint32_t prevb) {
+    return laq_load_meta(d, q, ib, lp, prevb);
+  }
+  __device__ static uint32_t stage_lp(const PholdDev& d, const Dev& q, const InsDev& ib, uint32_t lp, uint32_t slot,
+                                      uint32_t s, float bound, const Smem& sm, const PholdStage& st,
+                                      const LaneGroup<G>& g, uint32_t* err_slot, const Meta& mt) {
+    return laq_lp_stage<G>(d, q, ib, lp, slot, s, bound, sm, st, g, err_slot, mt);
+  }
+};

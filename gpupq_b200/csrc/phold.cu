@@ -35,9 +35,12 @@ struct gpq_phold {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
   // device memory (one allocation per array)
-  gpq_item* ring = nullptr;
-  uint32_t* rd = nullptr;
-  uint32_t* wr = nullptr;
+  gpq_item* items = nullptr;  // per-LP queue items (ring / heap / node pool)
+  uint32_t* qa = nullptr;     // per-LP queue words (see LpQueueDev)
+  uint32_t* qb = nullptr;
+  uint32_t* qc = nullptr;
+  uint32_t* links = nullptr;  // splay links
+  uint16_t* freestk = nullptr;
   gpq_item* ibuf = nullptr;
   uint32_t* icnt = nullptr;
   uint32_t* count = nullptr;
@@ -76,14 +79,25 @@ struct gpq_phold {
     d.spin_limit = gpq::spin_limit();
     return d;
   }
-  LaqDev laq() const { return LaqDev{ring, rd, wr, cap_log2}; }
+  LpQueueDev lq() const {
+    LpQueueDev l;
+    l.kind = cfg.queue_kind;
+    l.cap_log2 = cap_log2;
+    l.items = items;
+    l.a = qa;
+    l.b = qb;
+    l.c = qc;
+    l.links = links;
+    l.freestk = freestk;
+    return l;
+  }
   InsDev ins() const { return InsDev{ibuf, icnt, cfg.insert_capacity}; }
-  LaqKernelSet ks{};
-  size_t window_smem() const { return phold_window_smem_bytes(block, ks.group, cfg.insert_capacity); }
+  PholdKernelSet ks{};
+  size_t window_smem() const { return phold_window_smem_bytes(block, ks.group, ks.group_smem); }
 
   ~gpq_phold() {
-    for (void* p : {(void*)ring, (void*)rd, (void*)wr, (void*)ibuf, (void*)icnt, (void*)count, (void*)csum,
-                    (void*)ohash, (void*)ctrl, (void*)acc, (void*)staging})
+    for (void* p : {(void*)items, (void*)qa, (void*)qb, (void*)qc, (void*)links, (void*)freestk, (void*)ibuf,
+                    (void*)icnt, (void*)count, (void*)csum, (void*)ohash, (void*)ctrl, (void*)acc, (void*)staging})
       if (p) cudaFree(p);
     if (h_ctrl) cudaFreeHost(h_ctrl);
     if (ev0) cudaEventDestroy(ev0);
@@ -108,11 +122,11 @@ gpq_status gpq_phold_create(const gpq_phold_config* cfg_in, gpq_phold** out) {
   gpq_status st = validate(cfg_in);
   if (st != GPQ_OK) return st;
   gpq_phold_config c = *cfg_in;
-  if (c.queue_kind != GPQ_QUEUE_LAQ) {
+  if (c.queue_kind != GPQ_QUEUE_LAQ && c.queue_kind != GPQ_QUEUE_LHQ && c.queue_kind != GPQ_QUEUE_LSQ) {
     gpq::set_last_error("queue kind %u not available in the PHOLD engine", c.queue_kind);
     return GPQ_ERR_UNSUPPORTED;
   }
-  st = gpq::normalize_laq_config(&c);
+  st = gpq::normalize_queue_config(&c);
   if (st != GPQ_OK) return st;
 
   gpq_phold* h = new (std::nothrow) gpq_phold();
@@ -135,9 +149,14 @@ gpq_status gpq_phold_create(const gpq_phold_config* cfg_in, gpq_phold** out) {
   TRY(cudaEventCreate(&h->ev0));
   TRY(cudaEventCreate(&h->ev1));
   const size_t L = c.num_lps;
-  TRY(cudaMalloc(&h->ring, (L << h->cap_log2) * sizeof(gpq_item)));
-  TRY(cudaMalloc(&h->rd, L * sizeof(uint32_t)));
-  TRY(cudaMalloc(&h->wr, L * sizeof(uint32_t)));
+  TRY(cudaMalloc(&h->items, (L << h->cap_log2) * sizeof(gpq_item)));
+  TRY(cudaMalloc(&h->qa, L * sizeof(uint32_t)));
+  TRY(cudaMalloc(&h->qb, L * sizeof(uint32_t)));
+  TRY(cudaMalloc(&h->qc, L * sizeof(uint32_t)));
+  if (c.queue_kind == GPQ_QUEUE_LSQ) {
+    TRY(cudaMalloc(&h->links, (L << h->cap_log2) * sizeof(uint32_t)));
+    TRY(cudaMalloc(&h->freestk, (L << h->cap_log2) * sizeof(uint16_t)));
+  }
   TRY(cudaMalloc(&h->ibuf, 2 * L * c.insert_capacity * sizeof(gpq_item)));
   TRY(cudaMalloc(&h->icnt, 2 * L * sizeof(uint32_t)));
   TRY(cudaMalloc(&h->count, L * sizeof(uint32_t)));
@@ -146,11 +165,9 @@ gpq_status gpq_phold_create(const gpq_phold_config* cfg_in, gpq_phold** out) {
   TRY(cudaMalloc(&h->ctrl, sizeof(PholdCtrl)));
   TRY(cudaMalloc(&h->acc, sizeof(PholdAcc)));
   TRY(cudaMallocHost(&h->h_ctrl, sizeof(PholdCtrl)));
-  if (!laq_kernel_set(c.lanes_per_lp, &h->ks)) return fail(GPQ_ERR_INVALID);
-  if (!gpq::fit_block_to_smem(&h->block, h->ks.group,
-                              laq_group_smem_bytes(c.insert_capacity, h->ks.group) +
-                                  24 * kStageRounds,
-                              200 * 1024 - 4096 * 16 - 16)) {
+  if (!phold_kernel_set(c.queue_kind, c.lanes_per_lp, c.insert_capacity, &h->ks)) return fail(GPQ_ERR_INVALID);
+  if (!gpq::fit_block_to_smem(&h->block, h->ks.group, h->ks.group_smem + 24 * kStageRounds,
+                              200 * 1024 - 2048 * 16 - 16)) {
     gpq::set_last_error("insert_capacity %u needs too much shared memory per lane group", c.insert_capacity);
     return fail(GPQ_ERR_INVALID);
   }
@@ -195,9 +212,9 @@ gpq_status gpq_phold_populate(gpq_phold* h, const gpq_item* initial, uint64_t n,
   GPQ_CUDA_TRY(cudaMemsetAsync(h->icnt, 0, 2 * L * sizeof(uint32_t), st));
   const uint32_t wpb = 4;
   const size_t smem = (size_t)wpb * c.events_per_lp * (sizeof(gpq_item) + sizeof(uint64_t));
-  GPQ_CUDA_TRY(cudaFuncSetAttribute(phold_laq_populate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  GPQ_CUDA_TRY(cudaFuncSetAttribute(phold_populate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const uint32_t grid = (uint32_t)((L + wpb - 1) / wpb);
-  phold_laq_populate<<<grid, wpb * 32, smem, st>>>(h->dev(), h->laq(), c.events_per_lp, src);
+  phold_populate_kernel<<<grid, wpb * 32, smem, st>>>(h->dev(), h->lq(), c.events_per_lp, src);
   GPQ_CUDA_TRY(cudaGetLastError());
   h->phase = 0;
   h->populated = true;
@@ -212,7 +229,7 @@ static gpq_status run_plain(gpq_phold* h, uint32_t nsteps, int* done, cudaStream
   const uint32_t grid = (uint32_t)((c.num_lps + gpb - 1) / gpb);
   const size_t smem = h->window_smem();
   PholdDev d = h->dev();
-  LaqDev q = h->laq();
+  LpQueueDev q = h->lq();
   InsDev ib = h->ins();
   uint32_t executed = 0;
   if (done) *done = 0;
@@ -252,7 +269,7 @@ static gpq_status run_persistent(gpq_phold* h, cudaStream_t st) {
   grid = std::min(grid, std::max(need, 1u));
   GPQ_CUDA_TRY(cudaMemsetAsync(&h->ctrl->bar, 0, sizeof(unsigned long long), st));
   PholdDev d = h->dev();
-  LaqDev q = h->laq();
+  LpQueueDev q = h->lq();
   InsDev ib = h->ins();
   uint32_t s0 = h->phase;
   uint32_t maxs = c.max_steps ? (c.max_steps > s0 ? c.max_steps - s0 : 0) : 0;
@@ -307,7 +324,7 @@ gpq_status gpq_phold_result_get(gpq_phold* h, gpq_phold_result* out, void* strea
   GPQ_CUDA_TRY(cudaMemcpyAsync(h->acc, &a, sizeof(PholdAcc), cudaMemcpyHostToDevice, st));
   const uint32_t wpb = 8;
   const uint32_t grid = std::max(1u, std::min<uint32_t>((h->cfg.num_lps + wpb - 1) / wpb, 4096u));
-  phold_laq_finalize<<<grid, wpb * 32, 0, st>>>(h->dev(), h->laq(), h->ins(), h->acc);
+  phold_finalize_kernel<<<grid, wpb * 32, 0, st>>>(h->dev(), h->lq(), h->ins(), h->acc);
   GPQ_CUDA_TRY(cudaGetLastError());
   GPQ_CUDA_TRY(cudaMemcpyAsync(&a, h->acc, sizeof(PholdAcc), cudaMemcpyDeviceToHost, st));
   GPQ_CUDA_TRY(cudaMemcpyAsync(h->h_ctrl, h->ctrl, sizeof(PholdCtrl), cudaMemcpyDeviceToHost, st));

@@ -36,23 +36,35 @@ inline gpq_status validate_phold_config(const gpq_phold_config* c) {
   return GPQ_OK;
 }
 
-// Fills the LAQ defaults (capacity 256, insert capacity 64, 256-thread CTAs) and checks them.
-inline gpq_status normalize_laq_config(gpq_phold_config* c) {
+// Fills the per-kind defaults (capacity 256, insert capacity 64, 256-thread CTAs,
+// 8 lanes per LP; one lane for the splay queue) and checks them.
+inline gpq_status normalize_queue_config(gpq_phold_config* c) {
   if (c->capacity == 0) c->capacity = 256;
   if (c->insert_capacity == 0) c->insert_capacity = 64;
   GPQ_CHECK_ARG(is_pow2(c->capacity) && c->capacity >= 32 && c->capacity <= (1u << 16),
-                "LAQ capacity must be a power of two in [32, 65536]");
+                "capacity must be a power of two in [32, 65536]");
+  if (c->queue_kind == GPQ_QUEUE_LSQ)
+    GPQ_CHECK_ARG(c->capacity <= 32768, "splay queue capacity must be <= 32768");
   GPQ_CHECK_ARG(c->insert_capacity >= 1 && c->insert_capacity <= 1024, "insert_capacity must be in [1, 1024]");
   GPQ_CHECK_ARG(c->events_per_lp <= c->capacity, "events_per_lp must not exceed capacity");
   GPQ_CHECK_ARG(c->events_per_lp <= 2048, "events_per_lp must be <= 2048");
   if (c->block_threads == 0) c->block_threads = 256;
-  if (c->lanes_per_lp == 0) c->lanes_per_lp = 8;
-  GPQ_CHECK_ARG(c->lanes_per_lp == 4 || c->lanes_per_lp == 8 || c->lanes_per_lp == 16 || c->lanes_per_lp == 32,
-                "lanes_per_lp must be 4, 8, 16 or 32");
   GPQ_CHECK_ARG(c->block_threads % 32 == 0 && c->block_threads >= 32 && c->block_threads <= 1024,
                 "block_threads must be a multiple of 32 in [32, 1024]");
+  if (c->queue_kind == GPQ_QUEUE_LSQ) c->lanes_per_lp = 1;
+  if (c->lanes_per_lp == 0) c->lanes_per_lp = 8;
+  if (c->queue_kind == GPQ_QUEUE_LAQ)
+    GPQ_CHECK_ARG(c->lanes_per_lp == 4 || c->lanes_per_lp == 8 || c->lanes_per_lp == 16 || c->lanes_per_lp == 32,
+                  "lanes_per_lp must be 4, 8, 16 or 32 for the local array queue");
+  if (c->queue_kind == GPQ_QUEUE_LHQ)
+    GPQ_CHECK_ARG(c->lanes_per_lp == 1 || c->lanes_per_lp == 4 || c->lanes_per_lp == 8 || c->lanes_per_lp == 16 ||
+                      c->lanes_per_lp == 32,
+                  "lanes_per_lp must be 1, 4, 8, 16 or 32 for the local heap queue");
   return GPQ_OK;
 }
+
+// The LAQ entry points call this name.
+inline gpq_status normalize_laq_config(gpq_phold_config* c) { return normalize_queue_config(c); }
 
 // Halves the CTA size until the per-CTA merge scratch (one slice per lane group) fits
 // `limit` bytes of shared memory.  Returns false if even one warp does not fit.

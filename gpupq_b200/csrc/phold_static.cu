@@ -73,11 +73,11 @@ gpq_status scratch_for_current_device(unsigned char** out) {
       return GPQ_ERR_CUDA;
     }
     for (uint32_t grp : {4u, 8u, 16u, 32u}) {
-      LaqKernelSet ks;
-      laq_kernel_set(grp, &ks);
+      PholdKernelSet ks;
+      phold_kernel_set(GPQ_QUEUE_LAQ, grp, 64, &ks);
       GPQ_CUDA_TRY(cudaFuncSetAttribute(ks.persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
     }
-    GPQ_CUDA_TRY(cudaFuncSetAttribute(phold_laq_populate, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    GPQ_CUDA_TRY(cudaFuncSetAttribute(phold_populate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     g_scratch_dev[dev] = static_cast<unsigned char*>(p);
   }
   *out = g_scratch_dev[dev];
@@ -121,13 +121,11 @@ extern "C" gpq_status gpq_phold_run_static(const gpq_phold_config* cfg_in, const
     return GPQ_ERR_INVALID;
   }
   const size_t pop_smem = (size_t)4 * c.events_per_lp * (sizeof(gpq_item) + sizeof(uint64_t));
-  LaqKernelSet ks;
-  if (!laq_kernel_set(c.lanes_per_lp, &ks)) return GPQ_ERR_INVALID;
-  gpq::fit_block_to_smem(&c.block_threads, c.lanes_per_lp,
-                         laq_group_smem_bytes(c.insert_capacity, c.lanes_per_lp) +
-                             24 * kStageRounds,
-                         96 * 1024 - 4096 * 16 - 16);
-  const size_t win_smem = phold_window_smem_bytes(c.block_threads, c.lanes_per_lp, c.insert_capacity);
+  PholdKernelSet ks;
+  if (!phold_kernel_set(GPQ_QUEUE_LAQ, c.lanes_per_lp, c.insert_capacity, &ks)) return GPQ_ERR_INVALID;
+  gpq::fit_block_to_smem(&c.block_threads, c.lanes_per_lp, ks.group_smem + 24 * kStageRounds,
+                         96 * 1024 - 2048 * 16 - 16);
+  const size_t win_smem = phold_window_smem_bytes(c.block_threads, c.lanes_per_lp, ks.group_smem);
   if (pop_smem > 200 * 1024 || win_smem > 96 * 1024) {
     gpq::set_last_error("gpq_phold_run_static: events_per_lp or insert_capacity too large for shared memory");
     return GPQ_ERR_INVALID;
@@ -149,8 +147,12 @@ extern "C" gpq_status gpq_phold_run_static(const gpq_phold_config* cfg_in, const
   d.ohash = reinterpret_cast<unsigned long long*>(d_ohash);
   d.ctrl = reinterpret_cast<PholdCtrl*>(base + lay.ctrl);
   d.spin_limit = gpq::spin_limit();
-  LaqDev q{reinterpret_cast<gpq_item*>(base + lay.ring), reinterpret_cast<uint32_t*>(base + lay.rd),
-           reinterpret_cast<uint32_t*>(base + lay.wr), gpq::ilog2_ceil(c.capacity)};
+  LpQueueDev q{};
+  q.kind = GPQ_QUEUE_LAQ;
+  q.cap_log2 = gpq::ilog2_ceil(c.capacity);
+  q.items = reinterpret_cast<gpq_item*>(base + lay.ring);
+  q.a = reinterpret_cast<uint32_t*>(base + lay.rd);
+  q.b = reinterpret_cast<uint32_t*>(base + lay.wr);
   InsDev ib{reinterpret_cast<gpq_item*>(base + lay.ibuf), reinterpret_cast<uint32_t*>(base + lay.icnt),
             c.insert_capacity};
   PholdAcc* acc = reinterpret_cast<PholdAcc*>(base + lay.acc);
@@ -159,7 +161,7 @@ extern "C" gpq_status gpq_phold_run_static(const gpq_phold_config* cfg_in, const
   static_reset_kernel<<<(unsigned)std::min<size_t>((n_icnt + 255) / 256, 1024), 256, 0, s>>>(d.ctrl, acc, ib.cnt, n_icnt);
   GPQ_CUDA_TRY(cudaGetLastError());
   const uint32_t pwpb = 4;
-  phold_laq_populate<<<(c.num_lps + pwpb - 1) / pwpb, pwpb * 32, pop_smem, s>>>(d, q, c.events_per_lp, d_initial);
+  phold_populate_kernel<<<(c.num_lps + pwpb - 1) / pwpb, pwpb * 32, pop_smem, s>>>(d, q, c.events_per_lp, d_initial);
   GPQ_CUDA_TRY(cudaGetLastError());
 
   int per_sm = 0;
@@ -176,7 +178,7 @@ extern "C" gpq_status gpq_phold_run_static(const gpq_phold_config* cfg_in, const
   GPQ_CUDA_TRY(cudaLaunchCooperativeKernel(ks.persistent, dim3(grid), dim3(c.block_threads), args,
                                            win_smem, s));
   const uint32_t fwpb = 8;
-  phold_laq_finalize<<<std::max(1u, std::min<uint32_t>((c.num_lps + fwpb - 1) / fwpb, 4096u)), fwpb * 32, 0, s>>>(
+  phold_finalize_kernel<<<std::max(1u, std::min<uint32_t>((c.num_lps + fwpb - 1) / fwpb, 4096u)), fwpb * 32, 0, s>>>(
       d, q, ib, acc);
   GPQ_CUDA_TRY(cudaGetLastError());
 

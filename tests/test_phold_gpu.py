@@ -61,23 +61,29 @@ def test_children_match_oracle(gpu_lib):
     assert np.array_equal(ch["id"], ev["id"])
 
 
+QUEUE_SHAPES = [("laq", 4), ("laq", 8), ("laq", 16), ("laq", 32), ("lhq", 1), ("lhq", 8), ("lhq", 32), ("lsq", 1)]
+
+
 @pytest.mark.parametrize("loop", ["plain", "persistent"])
-@pytest.mark.parametrize("lanes", [4, 8, 16, 32])
-def test_phold_plain_workload_bit_exact(gpu_lib, loop, lanes):
+@pytest.mark.parametrize("queue,lanes", QUEUE_SHAPES)
+def test_phold_plain_workload_bit_exact(gpu_lib, loop, queue, lanes):
     """1024 LPs x 16 events, lookahead 1.0, end 100, uniform destinations, seed 42."""
     o = _oracle(C1)
-    r, s = _run(C1, loop=loop, lanes_per_lp=lanes)
+    r, s = _run(C1, loop=loop, queue=queue, lanes_per_lp=lanes)
     _assert_same(r, s, o)
     assert r["committed"] == 820705
 
 
-@pytest.mark.parametrize("loop,lanes,block", [("plain", 8, 256), ("persistent", 4, 128), ("persistent", 8, 256),
-                                               ("persistent", 16, 512), ("persistent", 32, 256)])
-def test_phold_large_reduced_bit_exact(gpu_lib, loop, lanes, block):
+@pytest.mark.parametrize("queue,loop,lanes,block", [
+    ("laq", "plain", 8, 256), ("laq", "persistent", 4, 128), ("laq", "persistent", 8, 256),
+    ("laq", "persistent", 16, 512), ("laq", "persistent", 32, 256),
+    ("lhq", "persistent", 8, 128), ("lhq", "plain", 4, 256), ("lsq", "persistent", 1, 128), ("lsq", "plain", 1, 256)])
+def test_phold_large_reduced_bit_exact(gpu_lib, queue, loop, lanes, block):
     """The 65,536-LP ring workload cut to end time 3 (checked by the threaded oracle)."""
     cfgd = dict(num_lps=65536, events_per_lp=64, lookahead=0.1, end_time=3.0, seed=7, dest_mode=1, ring_width=16)
     o = _oracle_cached(cfgd)
-    r, s = _run(cfgd, loop=loop, capacity=256, insert_capacity=64, lanes_per_lp=lanes, block_threads=block)
+    r, s = _run(cfgd, queue=queue, loop=loop, capacity=256, insert_capacity=64, lanes_per_lp=lanes,
+                block_threads=block)
     _assert_same(r, s, o)
 
 
@@ -94,10 +100,12 @@ def test_phold_large_reduced_bit_exact(gpu_lib, loop, lanes, block):
     (dict(num_lps=3000, events_per_lp=60, lookahead=20.0, end_time=60.0, seed=17, dest_mode=1, ring_width=4),
      dict(capacity=256, insert_capacity=256)),
 ])
-@pytest.mark.parametrize("loop,lanes", [("plain", 32), ("persistent", 4), ("persistent", 8), ("persistent", 32)])
-def test_phold_edge_shapes(gpu_lib, cfgd, kw, loop, lanes):
+@pytest.mark.parametrize("queue,loop,lanes", [("laq", "plain", 32), ("laq", "persistent", 4), ("laq", "persistent", 8),
+                                              ("laq", "persistent", 32), ("lhq", "persistent", 8), ("lhq", "plain", 1),
+                                              ("lsq", "persistent", 1), ("lsq", "plain", 1)])
+def test_phold_edge_shapes(gpu_lib, cfgd, kw, queue, loop, lanes):
     o = _oracle(cfgd)
-    r, s = _run(cfgd, loop=loop, lanes_per_lp=lanes, **kw)
+    r, s = _run(cfgd, queue=queue, loop=loop, lanes_per_lp=lanes, **kw)
     _assert_same(r, s, o)
 
 
@@ -130,8 +138,9 @@ def test_step_api_resumes(gpu_lib):
     assert n > 10
 
 
-def test_queue_overflow_reported(gpu_lib):
+@pytest.mark.parametrize("queue", ["laq", "lhq", "lsq"])
+def test_queue_overflow_reported(gpu_lib, queue):
     # per-LP capacity 32 with 32 initial events: the first child overflows the queue
     cfgd = dict(num_lps=16, events_per_lp=32, lookahead=0.01, end_time=50.0, seed=3, dest_mode=0)
-    r, _ = _run(cfgd, capacity=32, insert_capacity=64)
+    r, _ = _run(cfgd, queue=queue, capacity=32, insert_capacity=64)
     assert r["status_code"] in (3, 4)
