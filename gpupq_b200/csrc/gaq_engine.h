@@ -1,0 +1,37 @@
+// Host side of the global array queue: the sorted-array maintenance shared by the PHOLD
+// engine (kind GPQ_QUEUE_GAQ) and the GAQ queue object.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "gpq.h"
+
+struct PholdDev;
+
+namespace gpq {
+
+// Stable sort of n items by timestamp bits with the project's LSD radix sort.
+// Keys must lie in [kmin, kmax]; only ceil(log2(kmax - kmin + 1) / 8) passes run.  The
+// items start in `a`; `b` is a second buffer of n items; `hist` holds
+// 256 * ceil(n / 4096) words.  *sorted receives a or b, whichever holds the result.
+gpq_status radix_sort_by_ts(gpq_item* a, gpq_item* b, uint32_t n, uint32_t kmin, uint32_t kmax, uint32_t* hist,
+                            gpq_item** sorted, cudaStream_t st);
+size_t radix_hist_words(uint32_t n);
+
+// Merge two arrays sorted by timestamp bits into `out` (A first on equal timestamps).
+gpq_status merge_by_ts(const gpq_item* A, uint32_t na, const gpq_item* B, uint32_t nb, gpq_item* out,
+                       cudaStream_t st);
+
+struct GaqEngine;
+gpq_status gaq_engine_create(const gpq_phold_config& c, GaqEngine** out);
+void gaq_engine_destroy(GaqEngine* g);
+gpq_status gaq_engine_populate(GaqEngine* g, const PholdDev& d, const gpq_item* dev_src, cudaStream_t st);
+// Runs up to nsteps windows (0 = until done); *done = 1 when the minimum reached the end
+// time; *windows += windows executed.  Returns the device error, if any.
+gpq_status gaq_engine_run(GaqEngine* g, const PholdDev& d, uint32_t nsteps, int* done, uint64_t* windows,
+                          cudaStream_t st);
+// committed, pending, pending_csum, digest, pending_min (as float bits)
+gpq_status gaq_engine_finalize(GaqEngine* g, const PholdDev& d, uint64_t out[4], uint32_t* pmin, cudaStream_t st);
+uint32_t gaq_engine_launches_per_window();
+
+}  // namespace gpq

@@ -127,6 +127,9 @@ gpq_status LocalQueueBase::scan_counts(const uint32_t* cnt, uint64_t* total, cud
 gpq_status make_queue(const gpq_queue_config& cfg, std::unique_ptr<QueueImpl>& out) {
   switch (cfg.kind) {
     case GPQ_QUEUE_LAQ: return make_laq_queue(cfg, out);
+    case GPQ_QUEUE_LHQ:
+    case GPQ_QUEUE_LSQ: return make_lpq_queue(cfg, out);
+    case GPQ_QUEUE_GAQ: return make_gaq_queue(cfg, out);
     default:
       set_last_error("queue kind %u is not available", cfg.kind);
       return GPQ_ERR_UNSUPPORTED;

@@ -12,6 +12,7 @@
 
 #include "host_common.h"
 #include "phold_host.h"
+#include "gaq_engine.h"
 #include "phold_kernels.cuh"
 
 namespace {
@@ -93,6 +94,8 @@ struct gpq_phold {
   }
   InsDev ins() const { return InsDev{ibuf, icnt, cfg.insert_capacity}; }
   PholdKernelSet ks{};
+  gpq::GaqEngine* gaq = nullptr;  // global array queue state (queue_kind == GPQ_QUEUE_GAQ)
+  uint64_t gaq_windows = 0;
   size_t window_smem() const { return phold_window_smem_bytes(block, ks.group, ks.group_smem); }
 
   ~gpq_phold() {
@@ -100,6 +103,7 @@ struct gpq_phold {
                     (void*)icnt, (void*)count, (void*)csum, (void*)ohash, (void*)ctrl, (void*)acc, (void*)staging})
       if (p) cudaFree(p);
     if (h_ctrl) cudaFreeHost(h_ctrl);
+    if (gaq) gpq::gaq_engine_destroy(gaq);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (own) cudaStreamDestroy(own);
@@ -122,7 +126,7 @@ gpq_status gpq_phold_create(const gpq_phold_config* cfg_in, gpq_phold** out) {
   gpq_status st = validate(cfg_in);
   if (st != GPQ_OK) return st;
   gpq_phold_config c = *cfg_in;
-  if (c.queue_kind != GPQ_QUEUE_LAQ && c.queue_kind != GPQ_QUEUE_LHQ && c.queue_kind != GPQ_QUEUE_LSQ) {
+  if (c.queue_kind == GPQ_QUEUE_HQ) {
     gpq::set_last_error("queue kind %u not available in the PHOLD engine", c.queue_kind);
     return GPQ_ERR_UNSUPPORTED;
   }
@@ -149,10 +153,12 @@ gpq_status gpq_phold_create(const gpq_phold_config* cfg_in, gpq_phold** out) {
   TRY(cudaEventCreate(&h->ev0));
   TRY(cudaEventCreate(&h->ev1));
   const size_t L = c.num_lps;
-  TRY(cudaMalloc(&h->items, (L << h->cap_log2) * sizeof(gpq_item)));
-  TRY(cudaMalloc(&h->qa, L * sizeof(uint32_t)));
-  TRY(cudaMalloc(&h->qb, L * sizeof(uint32_t)));
-  TRY(cudaMalloc(&h->qc, L * sizeof(uint32_t)));
+  if (c.queue_kind != GPQ_QUEUE_GAQ) {
+    TRY(cudaMalloc(&h->items, (L << h->cap_log2) * sizeof(gpq_item)));
+    TRY(cudaMalloc(&h->qa, L * sizeof(uint32_t)));
+    TRY(cudaMalloc(&h->qb, L * sizeof(uint32_t)));
+    TRY(cudaMalloc(&h->qc, L * sizeof(uint32_t)));
+  }
   if (c.queue_kind == GPQ_QUEUE_LSQ) {
     TRY(cudaMalloc(&h->links, (L << h->cap_log2) * sizeof(uint32_t)));
     TRY(cudaMalloc(&h->freestk, (L << h->cap_log2) * sizeof(uint16_t)));
@@ -165,6 +171,12 @@ gpq_status gpq_phold_create(const gpq_phold_config* cfg_in, gpq_phold** out) {
   TRY(cudaMalloc(&h->ctrl, sizeof(PholdCtrl)));
   TRY(cudaMalloc(&h->acc, sizeof(PholdAcc)));
   TRY(cudaMallocHost(&h->h_ctrl, sizeof(PholdCtrl)));
+  if (c.queue_kind == GPQ_QUEUE_GAQ) {
+    gpq_status gs = gpq::gaq_engine_create(c, &h->gaq);
+    if (gs != GPQ_OK) return fail(gs);
+    *out = h;
+    return GPQ_OK;
+  }
   if (!phold_kernel_set(c.queue_kind, c.lanes_per_lp, c.insert_capacity, &h->ks)) return fail(GPQ_ERR_INVALID);
   if (!gpq::fit_block_to_smem(&h->block, h->ks.group, h->ks.group_smem + 24 * kStageRounds,
                               200 * 1024 - 2048 * 16 - 16)) {
@@ -210,6 +222,16 @@ gpq_status gpq_phold_populate(gpq_phold* h, const gpq_item* initial, uint64_t n,
   *h->h_ctrl = init;
   GPQ_CUDA_TRY(cudaMemcpyAsync(h->ctrl, h->h_ctrl, sizeof(PholdCtrl), cudaMemcpyHostToDevice, st));
   GPQ_CUDA_TRY(cudaMemsetAsync(h->icnt, 0, 2 * L * sizeof(uint32_t), st));
+  h->phase = 0;
+  h->gaq_windows = 0;
+  if (h->gaq) {
+    gpq_status gs = gpq::gaq_engine_populate(h->gaq, h->dev(), src, st);
+    if (gs != GPQ_OK) return gs;
+    h->populated = true;
+    h->finalized = false;
+    h->elapsed_ms = 0.f;
+    return GPQ_OK;
+  }
   const uint32_t wpb = 4;
   const size_t smem = (size_t)wpb * c.events_per_lp * (sizeof(gpq_item) + sizeof(uint64_t));
   GPQ_CUDA_TRY(cudaFuncSetAttribute(phold_populate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -294,10 +316,12 @@ gpq_status gpq_phold_run(gpq_phold* h, void* stream) {
   cudaStream_t st = gpq::as_stream(stream, h->own);
   h->finalized = false;
   GPQ_CUDA_TRY(cudaEventRecord(h->ev0, st));
-  gpq_status s = (h->cfg.loop_mode == GPQ_LOOP_PERSISTENT) ? run_persistent(h, st) : run_plain(h, 0, nullptr, st);
+  gpq_status s;
+  if (h->gaq) s = gpq::gaq_engine_run(h->gaq, h->dev(), 0, nullptr, &h->gaq_windows, st);
+  else s = (h->cfg.loop_mode == GPQ_LOOP_PERSISTENT) ? run_persistent(h, st) : run_plain(h, 0, nullptr, st);
   if (s != GPQ_OK) return s;
   GPQ_CUDA_TRY(cudaEventRecord(h->ev1, st));
-  if (h->cfg.loop_mode == GPQ_LOOP_PERSISTENT) {
+  if (!h->gaq && h->cfg.loop_mode == GPQ_LOOP_PERSISTENT) {
     s = sync_phase(h, st);
     if (s != GPQ_OK) return s;
   }
@@ -312,6 +336,7 @@ gpq_status gpq_phold_step(gpq_phold* h, uint32_t nsteps, int* done, void* stream
   GPQ_CHECK_ARG(h, "handle is NULL");
   if (!h->populated) return GPQ_ERR_NOT_READY;
   h->finalized = false;
+  if (h->gaq) return gpq::gaq_engine_run(h->gaq, h->dev(), nsteps, done, &h->gaq_windows, gpq::as_stream(stream, h->own));
   return run_plain(h, nsteps, done, gpq::as_stream(stream, h->own));
 }
 
@@ -319,6 +344,25 @@ gpq_status gpq_phold_result_get(gpq_phold* h, gpq_phold_result* out, void* strea
   GPQ_CHECK_ARG(h && out, "NULL argument");
   if (!h->populated) return GPQ_ERR_NOT_READY;
   cudaStream_t st = gpq::as_stream(stream, h->own);
+  if (h->gaq) {
+    uint64_t v[4];
+    uint32_t pmin = kInfBits;
+    gpq_status gs = gpq::gaq_engine_finalize(h->gaq, h->dev(), v, &pmin, st);
+    if (gs != GPQ_OK) return gs;
+    GPQ_CUDA_TRY(cudaMemcpyAsync(h->h_ctrl, h->ctrl, sizeof(PholdCtrl), cudaMemcpyDeviceToHost, st));
+    GPQ_CUDA_TRY(cudaStreamSynchronize(st));
+    std::memset(out, 0, sizeof(*out));
+    out->committed = v[0];
+    out->pending = v[1];
+    out->pending_csum = v[2];
+    out->digest = v[3];
+    out->steps = h->gaq_windows;
+    out->final_min = gpq_u2f(pmin);
+    out->elapsed_ms = h->elapsed_ms;
+    out->status = (int32_t)h->h_ctrl->err;
+    h->finalized = true;
+    return (gpq_status)h->h_ctrl->err;
+  }
   PholdAcc a{};
   a.pending_min = kInfBits;
   GPQ_CUDA_TRY(cudaMemcpyAsync(h->acc, &a, sizeof(PholdAcc), cudaMemcpyHostToDevice, st));
@@ -357,7 +401,9 @@ gpq_status gpq_phold_launch_info(gpq_phold* h, uint32_t* grid, uint32_t* block, 
   GPQ_CHECK_ARG(h, "handle is NULL");
   if (grid) *grid = h->last_grid;
   if (block) *block = h->block;
-  if (launches_per_run) *launches_per_run = (h->cfg.loop_mode == GPQ_LOOP_PERSISTENT) ? 1u : h->phase;
+  if (launches_per_run)
+    *launches_per_run = h->gaq ? (uint32_t)(h->gaq_windows * gpq::gaq_engine_launches_per_window())
+                               : (h->cfg.loop_mode == GPQ_LOOP_PERSISTENT) ? 1u : h->phase;
   return GPQ_OK;
 }
 

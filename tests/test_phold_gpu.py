@@ -61,7 +61,8 @@ def test_children_match_oracle(gpu_lib):
     assert np.array_equal(ch["id"], ev["id"])
 
 
-QUEUE_SHAPES = [("laq", 4), ("laq", 8), ("laq", 16), ("laq", 32), ("lhq", 1), ("lhq", 8), ("lhq", 32), ("lsq", 1)]
+QUEUE_SHAPES = [("laq", 4), ("laq", 8), ("laq", 16), ("laq", 32), ("lhq", 1), ("lhq", 8), ("lhq", 32), ("lsq", 1),
+                ("gaq", 8)]
 
 
 @pytest.mark.parametrize("loop", ["plain", "persistent"])
@@ -77,7 +78,8 @@ def test_phold_plain_workload_bit_exact(gpu_lib, loop, queue, lanes):
 @pytest.mark.parametrize("queue,loop,lanes,block", [
     ("laq", "plain", 8, 256), ("laq", "persistent", 4, 128), ("laq", "persistent", 8, 256),
     ("laq", "persistent", 16, 512), ("laq", "persistent", 32, 256),
-    ("lhq", "persistent", 8, 128), ("lhq", "plain", 4, 256), ("lsq", "persistent", 1, 128), ("lsq", "plain", 1, 256)])
+    ("lhq", "persistent", 8, 128), ("lhq", "plain", 4, 256), ("lsq", "persistent", 1, 128), ("lsq", "plain", 1, 256),
+    ("gaq", "plain", 8, 256)])
 def test_phold_large_reduced_bit_exact(gpu_lib, queue, loop, lanes, block):
     """The 65,536-LP ring workload cut to end time 3 (checked by the threaded oracle)."""
     cfgd = dict(num_lps=65536, events_per_lp=64, lookahead=0.1, end_time=3.0, seed=7, dest_mode=1, ring_width=16)
@@ -102,7 +104,7 @@ def test_phold_large_reduced_bit_exact(gpu_lib, queue, loop, lanes, block):
 ])
 @pytest.mark.parametrize("queue,loop,lanes", [("laq", "plain", 32), ("laq", "persistent", 4), ("laq", "persistent", 8),
                                               ("laq", "persistent", 32), ("lhq", "persistent", 8), ("lhq", "plain", 1),
-                                              ("lsq", "persistent", 1), ("lsq", "plain", 1)])
+                                              ("lsq", "persistent", 1), ("lsq", "plain", 1), ("gaq", "plain", 8)])
 def test_phold_edge_shapes(gpu_lib, cfgd, kw, queue, loop, lanes):
     o = _oracle(cfgd)
     r, s = _run(cfgd, queue=queue, loop=loop, lanes_per_lp=lanes, **kw)
