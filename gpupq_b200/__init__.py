@@ -59,7 +59,8 @@ class PholdConfig(ctypes.Structure):
         ("ctas_per_sm", ctypes.c_uint32),
         ("max_steps", ctypes.c_uint32),
         ("lanes_per_lp", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 3),
+        ("node_size", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 2),
     ]
 
 
@@ -183,7 +184,7 @@ def presets():
 
 def make_phold_config(num_lps, events_per_lp, lookahead, end_time, seed, dest_mode=DEST_UNIFORM,
                       ring_width=16, ring_frac=0.9, queue="laq", capacity=256, insert_capacity=64,
-                      loop="persistent", block_threads=0, ctas_per_sm=0, max_steps=0, lanes_per_lp=0):
+                      loop="persistent", block_threads=0, ctas_per_sm=0, max_steps=0, lanes_per_lp=0, node_size=0):
     c = PholdConfig()
     c.seed = seed
     c.num_lps = num_lps
@@ -201,6 +202,7 @@ def make_phold_config(num_lps, events_per_lp, lookahead, end_time, seed, dest_mo
     c.ctas_per_sm = ctas_per_sm
     c.max_steps = max_steps
     c.lanes_per_lp = lanes_per_lp
+    c.node_size = node_size
     return c
 
 

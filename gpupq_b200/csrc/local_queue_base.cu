@@ -130,6 +130,7 @@ gpq_status make_queue(const gpq_queue_config& cfg, std::unique_ptr<QueueImpl>& o
     case GPQ_QUEUE_LHQ:
     case GPQ_QUEUE_LSQ: return make_lpq_queue(cfg, out);
     case GPQ_QUEUE_GAQ: return make_gaq_queue(cfg, out);
+    case GPQ_QUEUE_HQ: return make_hq_queue(cfg, out);
     default:
       set_last_error("queue kind %u is not available", cfg.kind);
       return GPQ_ERR_UNSUPPORTED;

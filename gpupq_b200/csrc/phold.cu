@@ -12,7 +12,9 @@
 
 #include "host_common.h"
 #include "phold_host.h"
+#include "gaq.cuh"
 #include "gaq_engine.h"
+#include "hq_kernels.cuh"
 #include "phold_kernels.cuh"
 
 namespace {
@@ -96,6 +98,13 @@ struct gpq_phold {
   PholdKernelSet ks{};
   gpq::GaqEngine* gaq = nullptr;  // global array queue state (queue_kind == GPQ_QUEUE_GAQ)
   uint64_t gaq_windows = 0;
+  // parallel heap (queue_kind == GPQ_QUEUE_HQ): one CTA runs the heap
+  HqDev hq{};
+  gpq_item* hq_sort[2] = {nullptr, nullptr};
+  uint32_t* hq_hist = nullptr;
+  uint32_t* hq_mm = nullptr;
+  uint64_t hq_windows = 0;
+  bool is_hq = false;
   size_t window_smem() const { return phold_window_smem_bytes(block, ks.group, ks.group_smem); }
 
   ~gpq_phold() {
@@ -104,6 +113,9 @@ struct gpq_phold {
       if (p) cudaFree(p);
     if (h_ctrl) cudaFreeHost(h_ctrl);
     if (gaq) gpq::gaq_engine_destroy(gaq);
+    for (void* p : {(void*)hq.nodes, (void*)hq.cnt, (void*)hq.meta, (void*)hq_sort[0], (void*)hq_sort[1],
+                    (void*)hq_hist, (void*)hq_mm})
+      if (p) cudaFree(p);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (own) cudaStreamDestroy(own);
@@ -126,10 +138,6 @@ gpq_status gpq_phold_create(const gpq_phold_config* cfg_in, gpq_phold** out) {
   gpq_status st = validate(cfg_in);
   if (st != GPQ_OK) return st;
   gpq_phold_config c = *cfg_in;
-  if (c.queue_kind == GPQ_QUEUE_HQ) {
-    gpq::set_last_error("queue kind %u not available in the PHOLD engine", c.queue_kind);
-    return GPQ_ERR_UNSUPPORTED;
-  }
   st = gpq::normalize_queue_config(&c);
   if (st != GPQ_OK) return st;
 
@@ -153,7 +161,25 @@ gpq_status gpq_phold_create(const gpq_phold_config* cfg_in, gpq_phold** out) {
   TRY(cudaEventCreate(&h->ev0));
   TRY(cudaEventCreate(&h->ev1));
   const size_t L = c.num_lps;
-  if (c.queue_kind != GPQ_QUEUE_GAQ) {
+  if (c.queue_kind == GPQ_QUEUE_HQ) {
+    const uint32_t r = c.node_size ? c.node_size : 1024;
+    if (!gpq::is_pow2(r) || r < 2 || r > kHqMaxR || c.num_lps > (1u << 21)) {
+      gpq::set_last_error("heap queue: node_size must be a power of two in [2, %u] and num_lps <= 2^21", kHqMaxR);
+      return fail(GPQ_ERR_INVALID);
+    }
+    const uint64_t N = (uint64_t)c.num_lps * c.events_per_lp;
+    h->is_hq = true;
+    h->hq.r = r;
+    h->hq.maxnodes = (uint32_t)((N + r - 1) / r + 2);
+    TRY(cudaMalloc(&h->hq.nodes, (size_t)h->hq.maxnodes * r * sizeof(gpq_item)));
+    TRY(cudaMalloc(&h->hq.cnt, (size_t)h->hq.maxnodes * sizeof(uint32_t)));
+    TRY(cudaMalloc(&h->hq.meta, 4 * sizeof(uint32_t)));
+    TRY(cudaMalloc(&h->hq_sort[0], N * sizeof(gpq_item)));
+    TRY(cudaMalloc(&h->hq_sort[1], N * sizeof(gpq_item)));
+    TRY(cudaMalloc(&h->hq_hist, gpq::radix_hist_words((uint32_t)N) * sizeof(uint32_t)));
+    TRY(cudaMalloc(&h->hq_mm, 2 * sizeof(uint32_t)));
+    TRY(cudaFuncSetAttribute(hq_phold_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hq_smem_bytes(r)));
+  } else if (c.queue_kind != GPQ_QUEUE_GAQ) {
     TRY(cudaMalloc(&h->items, (L << h->cap_log2) * sizeof(gpq_item)));
     TRY(cudaMalloc(&h->qa, L * sizeof(uint32_t)));
     TRY(cudaMalloc(&h->qb, L * sizeof(uint32_t)));
@@ -171,6 +197,10 @@ gpq_status gpq_phold_create(const gpq_phold_config* cfg_in, gpq_phold** out) {
   TRY(cudaMalloc(&h->ctrl, sizeof(PholdCtrl)));
   TRY(cudaMalloc(&h->acc, sizeof(PholdAcc)));
   TRY(cudaMallocHost(&h->h_ctrl, sizeof(PholdCtrl)));
+  if (h->is_hq) {
+    *out = h;
+    return GPQ_OK;
+  }
   if (c.queue_kind == GPQ_QUEUE_GAQ) {
     gpq_status gs = gpq::gaq_engine_create(c, &h->gaq);
     if (gs != GPQ_OK) return fail(gs);
@@ -224,6 +254,38 @@ gpq_status gpq_phold_populate(gpq_phold* h, const gpq_item* initial, uint64_t n,
   GPQ_CUDA_TRY(cudaMemsetAsync(h->icnt, 0, 2 * L * sizeof(uint32_t), st));
   h->phase = 0;
   h->gaq_windows = 0;
+  h->hq_windows = 0;
+  if (h->is_hq) {
+    const uint32_t N = c.num_lps * c.events_per_lp;
+    gaq_zero_stats_kernel<<<std::max(1u, std::min<uint32_t>((c.num_lps + 255) / 256, 4096)), 256, 0, st>>>(h->dev());
+    const uint32_t mm[2] = {0xffffffffu, 0u};
+    GPQ_CUDA_TRY(cudaMemcpyAsync(h->hq_mm, mm, sizeof(mm), cudaMemcpyHostToDevice, st));
+    gaq_initial_kernel<<<std::max(1u, std::min<uint32_t>((N + 255) / 256, 8192)), 256, 0, st>>>(
+        params_of(c), c.num_lps, c.events_per_lp, src, h->hq_sort[0], h->hq_mm);
+    GPQ_CUDA_TRY(cudaGetLastError());
+    uint32_t hmm[2];
+    GPQ_CUDA_TRY(cudaMemcpyAsync(hmm, h->hq_mm, sizeof(hmm), cudaMemcpyDeviceToHost, st));
+    GPQ_CUDA_TRY(cudaStreamSynchronize(st));
+    gpq_item* sorted = nullptr;
+    gpq_status ss = gpq::radix_sort_by_ts(h->hq_sort[0], h->hq_sort[1], N, hmm[0], hmm[1], h->hq_hist, &sorted, st);
+    if (ss != GPQ_OK) return ss;
+    // The sorted population laid out in level order is a valid heap of full nodes.
+    GPQ_CUDA_TRY(cudaMemcpyAsync(h->hq.nodes, sorted, (size_t)N * sizeof(gpq_item), cudaMemcpyDeviceToDevice, st));
+    const uint32_t r = h->hq.r;
+    const uint32_t nfull = N / r, rem = N % r;
+    std::vector<uint32_t> cnt(h->hq.maxnodes, 0);
+    for (uint32_t i = 0; i < nfull; ++i) cnt[i] = r;
+    if (rem) cnt[nfull] = rem;
+    const uint32_t last = (N == 0) ? 0 : (rem ? nfull : nfull - 1);
+    GPQ_CUDA_TRY(cudaMemcpyAsync(h->hq.cnt, cnt.data(), cnt.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    const uint32_t meta[4] = {last, 0, 0, 0};
+    GPQ_CUDA_TRY(cudaMemcpyAsync(h->hq.meta, meta, sizeof(meta), cudaMemcpyHostToDevice, st));
+    GPQ_CUDA_TRY(cudaStreamSynchronize(st));
+    h->populated = true;
+    h->finalized = false;
+    h->elapsed_ms = 0.f;
+    return GPQ_OK;
+  }
   if (h->gaq) {
     gpq_status gs = gpq::gaq_engine_populate(h->gaq, h->dev(), src, st);
     if (gs != GPQ_OK) return gs;
@@ -275,6 +337,18 @@ static gpq_status run_plain(gpq_phold* h, uint32_t nsteps, int* done, cudaStream
   return GPQ_OK;
 }
 
+// Parallel heap: one CTA runs up to nsteps windows (0 = all) of the heap.
+static gpq_status run_hq(gpq_phold* h, uint32_t nsteps, int* done, cudaStream_t st) {
+  hq_phold_kernel<<<1, 512, hq_smem_bytes(h->hq.r), st>>>(h->dev(), h->hq, nsteps);
+  GPQ_CUDA_TRY(cudaGetLastError());
+  uint32_t meta[2];
+  GPQ_CUDA_TRY(cudaMemcpyAsync(meta, h->hq.meta, sizeof(meta), cudaMemcpyDeviceToHost, st));
+  GPQ_CUDA_TRY(cudaStreamSynchronize(st));
+  h->hq_windows += meta[1];
+  if (done) *done = (nsteps == 0 || meta[1] < nsteps) ? 1 : 0;
+  return GPQ_OK;
+}
+
 static gpq_status run_persistent(gpq_phold* h, cudaStream_t st) {
   const gpq_phold_config& c = h->cfg;
   const size_t smem = h->window_smem();
@@ -317,11 +391,15 @@ gpq_status gpq_phold_run(gpq_phold* h, void* stream) {
   h->finalized = false;
   GPQ_CUDA_TRY(cudaEventRecord(h->ev0, st));
   gpq_status s;
-  if (h->gaq) s = gpq::gaq_engine_run(h->gaq, h->dev(), 0, nullptr, &h->gaq_windows, st);
+  if (h->is_hq) {
+    const uint64_t cap = h->cfg.max_steps;
+    s = (cap && h->hq_windows >= cap) ? GPQ_OK : run_hq(h, cap ? (uint32_t)(cap - h->hq_windows) : 0u, nullptr, st);
+  }
+  else if (h->gaq) s = gpq::gaq_engine_run(h->gaq, h->dev(), 0, nullptr, &h->gaq_windows, st);
   else s = (h->cfg.loop_mode == GPQ_LOOP_PERSISTENT) ? run_persistent(h, st) : run_plain(h, 0, nullptr, st);
   if (s != GPQ_OK) return s;
   GPQ_CUDA_TRY(cudaEventRecord(h->ev1, st));
-  if (!h->gaq && h->cfg.loop_mode == GPQ_LOOP_PERSISTENT) {
+  if (!h->gaq && !h->is_hq && h->cfg.loop_mode == GPQ_LOOP_PERSISTENT) {
     s = sync_phase(h, st);
     if (s != GPQ_OK) return s;
   }
@@ -336,6 +414,10 @@ gpq_status gpq_phold_step(gpq_phold* h, uint32_t nsteps, int* done, void* stream
   GPQ_CHECK_ARG(h, "handle is NULL");
   if (!h->populated) return GPQ_ERR_NOT_READY;
   h->finalized = false;
+  if (h->is_hq) {
+    if (nsteps == 0) nsteps = 0xffffffffu;
+    return run_hq(h, nsteps, done, gpq::as_stream(stream, h->own));
+  }
   if (h->gaq) return gpq::gaq_engine_run(h->gaq, h->dev(), nsteps, done, &h->gaq_windows, gpq::as_stream(stream, h->own));
   return run_plain(h, nsteps, done, gpq::as_stream(stream, h->own));
 }
@@ -344,6 +426,31 @@ gpq_status gpq_phold_result_get(gpq_phold* h, gpq_phold_result* out, void* strea
   GPQ_CHECK_ARG(h && out, "NULL argument");
   if (!h->populated) return GPQ_ERR_NOT_READY;
   cudaStream_t st = gpq::as_stream(stream, h->own);
+  if (h->is_hq) {
+    unsigned long long* acc = reinterpret_cast<unsigned long long*>(h->acc);
+    GPQ_CUDA_TRY(cudaMemsetAsync(acc, 0, 4 * sizeof(unsigned long long), st));
+    const uint32_t inf = kInfBits;
+    GPQ_CUDA_TRY(cudaMemcpyAsync(h->hq_mm, &inf, 4, cudaMemcpyHostToDevice, st));
+    hq_finalize_kernel<<<512, 256, 0, st>>>(h->dev(), h->hq, acc, h->hq_mm);
+    GPQ_CUDA_TRY(cudaGetLastError());
+    unsigned long long v[4];
+    uint32_t pmin = kInfBits;
+    GPQ_CUDA_TRY(cudaMemcpyAsync(v, acc, sizeof(v), cudaMemcpyDeviceToHost, st));
+    GPQ_CUDA_TRY(cudaMemcpyAsync(&pmin, h->hq_mm, 4, cudaMemcpyDeviceToHost, st));
+    GPQ_CUDA_TRY(cudaMemcpyAsync(h->h_ctrl, h->ctrl, sizeof(PholdCtrl), cudaMemcpyDeviceToHost, st));
+    GPQ_CUDA_TRY(cudaStreamSynchronize(st));
+    std::memset(out, 0, sizeof(*out));
+    out->committed = v[0];
+    out->pending = v[1];
+    out->pending_csum = v[2];
+    out->digest = v[3];
+    out->steps = h->hq_windows;
+    out->final_min = gpq_u2f(pmin);
+    out->elapsed_ms = h->elapsed_ms;
+    out->status = (int32_t)h->h_ctrl->err;
+    h->finalized = true;
+    return (gpq_status)h->h_ctrl->err;
+  }
   if (h->gaq) {
     uint64_t v[4];
     uint32_t pmin = kInfBits;
@@ -402,7 +509,8 @@ gpq_status gpq_phold_launch_info(gpq_phold* h, uint32_t* grid, uint32_t* block, 
   if (grid) *grid = h->last_grid;
   if (block) *block = h->block;
   if (launches_per_run)
-    *launches_per_run = h->gaq ? (uint32_t)(h->gaq_windows * gpq::gaq_engine_launches_per_window())
+    *launches_per_run = h->is_hq ? 1u
+                      : h->gaq ? (uint32_t)(h->gaq_windows * gpq::gaq_engine_launches_per_window())
                                : (h->cfg.loop_mode == GPQ_LOOP_PERSISTENT) ? 1u : h->phase;
   return GPQ_OK;
 }

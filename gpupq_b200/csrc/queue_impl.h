@@ -31,6 +31,7 @@ class QueueImpl {
 gpq_status make_laq_queue(const gpq_queue_config& cfg, std::unique_ptr<QueueImpl>& out);
 gpq_status make_lpq_queue(const gpq_queue_config& cfg, std::unique_ptr<QueueImpl>& out);
 gpq_status make_gaq_queue(const gpq_queue_config& cfg, std::unique_ptr<QueueImpl>& out);
+gpq_status make_hq_queue(const gpq_queue_config& cfg, std::unique_ptr<QueueImpl>& out);
 gpq_status make_queue(const gpq_queue_config& cfg, std::unique_ptr<QueueImpl>& out);
 
 }  // namespace gpq

@@ -12,7 +12,11 @@ independent of each queue's internal layout:
   * a step dequeues, per LP, the earliest items whose timestamp lies below the window
     bound (min + LOOKAHEAD), at most `max_per_lp` of them (the reference takes one per LP:
     src/phold.cu:84-94, src/global_array_queue.cu:147-179, src/heap_queue.cu:478-547);
-  * items are ordered by timestamp; the rebuild breaks ties by (ts bits, LP, id).
+  * items are ordered by timestamp; the rebuild breaks ties by (ts bits, LP, id);
+  * the heap queue takes its candidates from the root only: the reference stops its scan
+    of the merged buffer at the root's maximum (src/heap_queue.cu:1588-1592, "the next
+    event for an LP is not in the root but in a child node"), and the root of a heap in
+    order holds the `root_size` globally smallest items (`root_size` = node size).
 
 Used to check the reference's own known-answer vectors (tests/golden/reference_kats.json)
 and, on the GPU, the rebuilt queues against the same semantics.
@@ -31,8 +35,9 @@ def key(item):
 
 
 class QueueModel:
-    def __init__(self, num_lps: int):
+    def __init__(self, num_lps: int, root_size: int = 0):
         self.num_lps = num_lps
+        self.root_size = root_size  # 0: every queued item is a candidate
         self.lps = [[] for _ in range(num_lps)]
         self.pending = []
         self.enqueued = 0
@@ -54,10 +59,15 @@ class QueueModel:
         return min(heads) if heads else float("inf")
 
     def dequeue(self, bound: float, max_per_lp: int = 0):
+        limit = [len(q) for q in self.lps]
+        if self.root_size:
+            limit = [0] * self.num_lps
+            for it in self.global_items()[: self.root_size]:
+                limit[it[1]] += 1
         out = []
         for lp, q in enumerate(self.lps):
             n = 0
-            while q and q[0][0] < bound and (max_per_lp == 0 or n < max_per_lp):
+            while q and n < limit[lp] and q[0][0] < bound and (max_per_lp == 0 or n < max_per_lp):
                 out.append(q.pop(0))
                 n += 1
         self.dequeued += len(out)

@@ -66,7 +66,7 @@ def test_quicksort_wrapping_ranges():
 
 
 def _apply_queue_kat(k):
-    m = QueueModel(k["num_lps"])
+    m = QueueModel(k["num_lps"], root_size=k.get("node_size", 0) if k.get("kind") == "hq" else 0)
     nid = 0
     batches = k.get("insert_batches") or [k["inserts"]]
     for b in batches:

@@ -37,6 +37,8 @@ def _run(cfgd, **kw):
 
 
 def _assert_same(r, s, o, check_steps=True):
+    """Bit-exact outputs.  The window count is compared too, except for the parallel heap,
+    whose root takes at most one node (r items) per window and so may need more windows."""
     assert r["status_code"] == 0, r
     assert np.array_equal(s["count"], o["count"])
     assert np.array_equal(s["csum"], o["csum"])
@@ -62,7 +64,7 @@ def test_children_match_oracle(gpu_lib):
 
 
 QUEUE_SHAPES = [("laq", 4), ("laq", 8), ("laq", 16), ("laq", 32), ("lhq", 1), ("lhq", 8), ("lhq", 32), ("lsq", 1),
-                ("gaq", 8)]
+                ("gaq", 8), ("hq", 8)]
 
 
 @pytest.mark.parametrize("loop", ["plain", "persistent"])
@@ -71,22 +73,31 @@ def test_phold_plain_workload_bit_exact(gpu_lib, loop, queue, lanes):
     """1024 LPs x 16 events, lookahead 1.0, end 100, uniform destinations, seed 42."""
     o = _oracle(C1)
     r, s = _run(C1, loop=loop, queue=queue, lanes_per_lp=lanes)
-    _assert_same(r, s, o)
+    _assert_same(r, s, o, check_steps=queue != "hq")
     assert r["committed"] == 820705
+
+
+@pytest.mark.parametrize("node_size", [2, 16, 256, 1024])
+def test_phold_heap_queue_node_sizes(gpu_lib, node_size):
+    """The parallel heap with nodes from 2 to 1024 items (deep and shallow heaps)."""
+    cfgd = dict(num_lps=300, events_per_lp=7, lookahead=0.3, end_time=25.0, seed=21, dest_mode=1, ring_width=5)
+    o = _oracle(cfgd)
+    r, s = _run(cfgd, queue="hq", node_size=node_size)
+    _assert_same(r, s, o, check_steps=False)
 
 
 @pytest.mark.parametrize("queue,loop,lanes,block", [
     ("laq", "plain", 8, 256), ("laq", "persistent", 4, 128), ("laq", "persistent", 8, 256),
     ("laq", "persistent", 16, 512), ("laq", "persistent", 32, 256),
     ("lhq", "persistent", 8, 128), ("lhq", "plain", 4, 256), ("lsq", "persistent", 1, 128), ("lsq", "plain", 1, 256),
-    ("gaq", "plain", 8, 256)])
+    ("gaq", "plain", 8, 256), ("hq", "persistent", 8, 256)])
 def test_phold_large_reduced_bit_exact(gpu_lib, queue, loop, lanes, block):
     """The 65,536-LP ring workload cut to end time 3 (checked by the threaded oracle)."""
     cfgd = dict(num_lps=65536, events_per_lp=64, lookahead=0.1, end_time=3.0, seed=7, dest_mode=1, ring_width=16)
     o = _oracle_cached(cfgd)
     r, s = _run(cfgd, queue=queue, loop=loop, capacity=256, insert_capacity=64, lanes_per_lp=lanes,
                 block_threads=block)
-    _assert_same(r, s, o)
+    _assert_same(r, s, o, check_steps=queue != "hq")
 
 
 @pytest.mark.parametrize("cfgd,kw", [
@@ -104,11 +115,12 @@ def test_phold_large_reduced_bit_exact(gpu_lib, queue, loop, lanes, block):
 ])
 @pytest.mark.parametrize("queue,loop,lanes", [("laq", "plain", 32), ("laq", "persistent", 4), ("laq", "persistent", 8),
                                               ("laq", "persistent", 32), ("lhq", "persistent", 8), ("lhq", "plain", 1),
-                                              ("lsq", "persistent", 1), ("lsq", "plain", 1), ("gaq", "plain", 8)])
+                                              ("lsq", "persistent", 1), ("lsq", "plain", 1), ("gaq", "plain", 8),
+                                              ("hq", "persistent", 8)])
 def test_phold_edge_shapes(gpu_lib, cfgd, kw, queue, loop, lanes):
     o = _oracle(cfgd)
     r, s = _run(cfgd, queue=queue, loop=loop, lanes_per_lp=lanes, **kw)
-    _assert_same(r, s, o)
+    _assert_same(r, s, o, check_steps=queue != "hq")
 
 
 def test_host_initial_events_path(gpu_lib):

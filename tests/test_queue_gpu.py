@@ -13,7 +13,7 @@ from oracle.queue_model import QueueModel
 pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "reference_kats.json")
-KINDS = ["laq", "lhq", "lsq", "gaq"]
+KINDS = ["laq", "lhq", "lsq", "gaq", "hq"]
 
 
 def _items(pairs, id0=0):
@@ -79,9 +79,9 @@ def test_random_ops_match_model(gpu_lib, kind, seed):
     rng = random.Random(seed)
     L = rng.choice([1, 3, 37, 300])
     cap = 128
-    m = QueueModel(L)
+    m = QueueModel(L, root_size=16 if kind == "hq" else 0)
     nid = 0
-    with G.Queue(kind, L, capacity=cap, insert_capacity=64) as q:
+    with G.Queue(kind, L, capacity=cap, insert_capacity=64, node_size=16) as q:
         for step in range(40):
             n = rng.randint(0, 60)
             pairs = []
