@@ -120,6 +120,17 @@ _SIGS = {
                        ctypes.c_int),
     "gpq_queue_counts": ([_VP, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64), _VP],
                          ctypes.c_int),
+    "gpq_astar_create": ([_VP, ctypes.POINTER(_VP)], ctypes.c_int),
+    "gpq_astar_destroy": ([_VP], ctypes.c_int),
+    "gpq_astar_solve": ([_VP, _VP, ctypes.c_uint32, _VP, _VP], ctypes.c_int),
+    "gpq_astar_last_stats": ([_VP, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
+                              ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32),
+                              ctypes.POINTER(ctypes.c_uint32)], ctypes.c_int),
+    "gpq_astar_path": ([_VP, ctypes.c_uint32, _VP, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32), _VP],
+                       ctypes.c_int),
+    "gpq_astar_gcost": ([_VP, ctypes.c_uint32, _VP, ctypes.c_uint64, _VP], ctypes.c_int),
+    "gpq_astar_query": ([ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                         ctypes.c_double, ctypes.c_double, _VP], ctypes.c_int),
 }
 
 
@@ -389,3 +400,92 @@ class PinnedArray:
             self.array = None
             lib().gpq_host_free(self._p)
             self._p = ctypes.c_void_p()
+
+
+# ---- A* grid search (include/gpq/astar.h, gpq_astar_* in include/gpq.h) ----
+
+ASTAR_INF = 0xFFFFFFFF
+ASTAR_GRID_DTYPE = np.dtype([("seed", "<u8"), ("width", "<u4"), ("height", "<u4"), ("block_thr", "<u4"),
+                             ("conn", "<u4"), ("start", "<u4"), ("goal", "<u4")])
+ASTAR_RESULT_DTYPE = np.dtype([("cost", "<u4"), ("path_len", "<u4"), ("expanded", "<u8"), ("gsum", "<u8"),
+                               ("path_hash", "<u8"), ("pops", "<u8"), ("windows", "<u4"), ("status", "<i4")])
+
+
+class AstarConfig(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in ("tile", "window", "inbox_capacity", "open_capacity",
+                                               "frontier_capacity", "block_threads", "ctas_per_sm",
+                                               "max_rounds")] + [("reserved", ctypes.c_uint32 * 4)]
+
+
+def density_threshold(p: float) -> int:
+    """Obstacle density -> the 24-bit threshold of gpq_astar_grid.block_thr."""
+    return int(p * 16777216.0)
+
+
+def astar_grid(width, height, density, seed, conn=4, start=None, goal=None):
+    g = np.zeros(1, ASTAR_GRID_DTYPE)
+    g[0] = (seed, width, height, density_threshold(density), conn, 0 if start is None else start,
+            width * height - 1 if goal is None else goal)
+    return g
+
+
+def astar_queries(base_seed, n, conn, side_lo, side_hi, dens_lo, dens_hi, first=0):
+    """Grids of queries first .. first+n-1 of a batch (gpq_astar_query)."""
+    out = np.zeros(n, ASTAR_GRID_DTYPE)
+    for i in range(n):
+        check(lib().gpq_astar_query(base_seed, first + i, conn, side_lo, side_hi, dens_lo, dens_hi,
+                                    ctypes.c_void_p(out[i:].ctypes.data)), "gpq_astar_query")
+    return out
+
+
+class AStar:
+    """An A* engine handle (gpq_astar_create); solve() runs a batch of grids."""
+
+    def __init__(self, **cfg):
+        c = AstarConfig()
+        for k, v in cfg.items():
+            setattr(c, k, v)
+        self._h = ctypes.c_void_p()
+        check(lib().gpq_astar_create(ctypes.byref(c), ctypes.byref(self._h)), "gpq_astar_create")
+
+    def close(self):
+        if self._h:
+            lib().gpq_astar_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def solve(self, grids, results=None):
+        grids = np.ascontiguousarray(grids, ASTAR_GRID_DTYPE)
+        if results is None:
+            results = np.zeros(len(grids), ASTAR_RESULT_DTYPE)
+        check(lib().gpq_astar_solve(self._h, _ptr(grids), len(grids), _ptr(results), None), "gpq_astar_solve")
+        return results
+
+    def stats(self):
+        t, s = ctypes.c_float(), ctypes.c_float()
+        r, g, b = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        check(lib().gpq_astar_last_stats(self._h, ctypes.byref(t), ctypes.byref(s), ctypes.byref(r),
+                                         ctypes.byref(g), ctypes.byref(b)), "gpq_astar_last_stats")
+        return {"total_ms": t.value, "search_ms": s.value, "rounds": r.value, "grid": g.value, "block": b.value}
+
+    def path(self, index, capacity=1 << 20):
+        out = np.zeros(capacity, np.uint32)
+        n = ctypes.c_uint32()
+        check(lib().gpq_astar_path(self._h, index, _ptr(out), capacity, ctypes.byref(n), None), "gpq_astar_path")
+        return out[: n.value]
+
+    def gcost(self, index, cells):
+        out = np.zeros(cells, np.uint32)
+        check(lib().gpq_astar_gcost(self._h, index, _ptr(out), cells, None), "gpq_astar_gcost")
+        return out

@@ -22,6 +22,7 @@
 #include <stdint.h>
 
 #include "gpq/model.h" /* gpq_item, gpq_phold_params */
+#include "gpq/astar.h" /* gpq_astar_grid */
 
 #if defined(__GNUC__)
 #define GPQ_API __attribute__((visibility("default")))
@@ -219,6 +220,66 @@ GPQ_API gpq_status gpq_phold_launch_info(gpq_phold* h, uint32_t* grid, uint32_t*
 #define GPQ_STATIC_SCRATCH_BYTES (16u * 1024u * 1024u)
 GPQ_API gpq_status gpq_phold_run_static(const gpq_phold_config* cfg, const gpq_item* d_initial, uint32_t* d_count,
                                         uint64_t* d_csum, uint64_t* d_ohash, gpq_phold_result* out, void* stream);
+
+/* ---------------------------------------------------------------------------------- */
+/* 2b. A* grid search (the a_star model, src/a_star.cu:269-593, over sharded queues)   */
+/* ---------------------------------------------------------------------------------- */
+
+/* Engine knobs.  The open list of an instance is sharded by square tiles of the grid
+ * (`tile` x `tile` cells per shard); each round expands, per instance, every open item
+ * with f <= bound, where the window [min f, min f + window] moves when it is drained. */
+typedef struct gpq_astar_config {
+  uint32_t tile;              /* tile side, a power of two in [8, 256]; 0 = 64 */
+  uint32_t window;            /* window width on f; 0 = 4 move costs */
+  uint32_t inbox_capacity;    /* items one tile receives per round; 0 = 8 * tile */
+  uint32_t open_capacity;     /* items one tile keeps above the window; 0 = tile * tile */
+  uint32_t frontier_capacity; /* shared-memory frontier items (two buffers); 0 = 2048 */
+  uint32_t block_threads;     /* 128 or 256; 0 = 256 */
+  uint32_t ctas_per_sm;       /* 0 = as many as fit */
+  uint32_t max_rounds;        /* 0 = 2^20; reaching it is GPQ_ERR_TIMEOUT */
+  uint32_t reserved[4];
+} gpq_astar_config;
+
+typedef struct gpq_astar_result {
+  uint32_t cost;      /* C*; GPQ_ASTAR_INF (0xFFFFFFFF) when the goal is unreachable */
+  uint32_t path_len;  /* cells on the canonical path, start and goal included */
+  uint64_t expanded;  /* cells with g + h <= C* (every reached cell when unreachable) */
+  uint64_t gsum;      /* sum of gpq_astar_cell_hash over the expanded cells */
+  uint64_t path_hash; /* sum of gpq_astar_path_hash over the path, goal = position 0 */
+  uint64_t pops;      /* expansions performed, re-expansions included */
+  uint32_t windows;   /* window moves */
+  int32_t status;     /* gpq_status of this instance */
+} gpq_astar_result;
+
+typedef struct gpq_astar gpq_astar;
+
+GPQ_API gpq_status gpq_astar_create(const gpq_astar_config* cfg, gpq_astar** out);
+GPQ_API gpq_status gpq_astar_destroy(gpq_astar* a);
+
+/* Solve n instances (HOST array of grids) in one persistent launch; results to a HOST
+ * array of n.  Device buffers grow as needed and are kept for the next call.  An
+ * instance whose tile buffers overflow reports GPQ_ERR_INSERT_FULL / GPQ_ERR_QUEUE_FULL
+ * in its status (its other fields are then not meaningful).  Blocks on the stream. */
+GPQ_API gpq_status gpq_astar_solve(gpq_astar* a, const gpq_astar_grid* grids, uint32_t n,
+                                   gpq_astar_result* results, void* stream);
+
+/* Device time of the last solve: the whole call (grid generation, search, results) and
+ * the search launch alone; the number of rounds; the launch geometry. */
+GPQ_API gpq_status gpq_astar_last_stats(gpq_astar* a, float* total_ms, float* search_ms, uint32_t* rounds,
+                                        uint32_t* grid, uint32_t* block);
+
+/* The canonical path of instance `index` of the last solve, goal first (HOST array). */
+GPQ_API gpq_status gpq_astar_path(gpq_astar* a, uint32_t index, uint32_t* cells, uint32_t capacity,
+                                  uint32_t* length, void* stream);
+
+/* The g values of instance `index` of the last solve (HOST array of width * height). */
+GPQ_API gpq_status gpq_astar_gcost(gpq_astar* a, uint32_t index, uint32_t* g, uint64_t capacity, void* stream);
+
+/* Grid of query `index` of a batch: side log-uniform in [side_lo, side_hi], obstacle
+ * density uniform in [dens_lo, dens_hi], start and goal distinct and uniform over the
+ * free cells, all drawn from seed base_seed + index (host computation). */
+GPQ_API gpq_status gpq_astar_query(uint64_t base_seed, uint32_t index, uint32_t conn, uint32_t side_lo,
+                                   uint32_t side_hi, double dens_lo, double dens_hi, gpq_astar_grid* out);
 
 /* Page-locked host memory for the end-to-end path (host <-> device copies). */
 GPQ_API gpq_status gpq_host_alloc(uint64_t bytes, void** out);

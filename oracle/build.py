@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT_DIR, "libgpq_oracle.so")
-SOURCES = ["phold_oracle.cpp"]
+SOURCES = ["phold_oracle.cpp", "astar_oracle.cpp"]
 
 
 def build(force: bool = False) -> str:

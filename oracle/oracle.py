@@ -36,6 +36,17 @@ class OraclePholdSummary(ctypes.Structure):
     ]
 
 
+class OracleAstarGrid(ctypes.Structure):
+    _fields_ = [("seed", ctypes.c_uint64)] + [(n, ctypes.c_uint32) for n in
+                                              ("width", "height", "block_thr", "conn", "start", "goal")]
+
+
+class OracleAstarResult(ctypes.Structure):
+    _fields_ = [("cost", ctypes.c_uint32), ("path_len", ctypes.c_uint32), ("expanded", ctypes.c_uint64),
+                ("gsum", ctypes.c_uint64), ("path_hash", ctypes.c_uint64), ("pops", ctypes.c_uint64),
+                ("seconds", ctypes.c_double)]
+
+
 def lib():
     global _LIB
     if _LIB is None:
@@ -61,6 +72,15 @@ def lib():
         _LIB.oracle_ring_insert_sorted.argtypes = [i64p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                    ctypes.c_int64]
         _LIB.oracle_ring_quicksort.argtypes = [i64p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        _LIB.oracle_astar_query.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                            ctypes.c_uint32, ctypes.c_double, ctypes.c_double,
+                                            ctypes.POINTER(OracleAstarGrid)]
+        _LIB.oracle_astar_solve.argtypes = [ctypes.POINTER(OracleAstarGrid), ctypes.POINTER(OracleAstarResult),
+                                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32]
+        _LIB.oracle_astar_solve.restype = ctypes.c_int
+        _LIB.oracle_astar_batch.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int,
+                                            ctypes.c_void_p]
+        _LIB.oracle_astar_batch.restype = ctypes.c_double
     return _LIB
 
 
@@ -123,3 +143,53 @@ def initial(cfg):
 
 def logf(x):
     return lib().oracle_logf(float(x))
+
+
+ASTAR_FIELDS = ("seed", "width", "height", "block_thr", "conn", "start", "goal")
+
+
+def _astar_grid(g):
+    o = OracleAstarGrid()
+    for k in ASTAR_FIELDS:
+        setattr(o, k, int(g[k]))
+    return o
+
+
+def astar_query(base_seed, index, conn, side_lo, side_hi, dens_lo, dens_hi):
+    o = OracleAstarGrid()
+    lib().oracle_astar_query(base_seed, index, conn, side_lo, side_hi, dens_lo, dens_hi, ctypes.byref(o))
+    return {k: getattr(o, k) for k in ASTAR_FIELDS}
+
+
+def astar(grid, want_g=False, want_path=False):
+    """Solve one grid (a mapping with the gpq_astar_grid fields) sequentially."""
+    o = _astar_grid(grid)
+    r = OracleAstarResult()
+    cells = o.width * o.height
+    g = np.zeros(cells, np.uint32) if want_g else None
+    path = np.zeros(cells, np.uint32) if want_path else None
+    rc = lib().oracle_astar_solve(ctypes.byref(o), ctypes.byref(r),
+                                  ctypes.c_void_p(g.ctypes.data) if g is not None else None,
+                                  ctypes.c_void_p(path.ctypes.data) if path is not None else None,
+                                  cells if path is not None else 0)
+    if rc != 0:
+        raise RuntimeError("A* oracle self-check failed")
+    out = {"cost": r.cost, "path_len": r.path_len, "expanded": r.expanded, "gsum": r.gsum,
+           "path_hash": r.path_hash, "pops": r.pops, "seconds": r.seconds}
+    if g is not None:
+        out["g"] = g
+    if path is not None:
+        out["path"] = path[: r.path_len]
+    return out
+
+
+def astar_batch(grids, threads):
+    """Solve many grids, one per host thread at a time; returns (seconds, list of results)."""
+    arr = (OracleAstarGrid * len(grids))(*[_astar_grid(g) for g in grids])
+    res = (OracleAstarResult * len(grids))()
+    sec = lib().oracle_astar_batch(ctypes.cast(arr, ctypes.c_void_p), len(grids), threads,
+                                   ctypes.cast(res, ctypes.c_void_p))
+    if sec < 0:
+        raise RuntimeError("A* oracle self-check failed")
+    return sec, [{"cost": r.cost, "path_len": r.path_len, "expanded": r.expanded, "gsum": r.gsum,
+                  "path_hash": r.path_hash, "pops": r.pops} for r in res]
