@@ -124,8 +124,8 @@ _SIGS = {
     "gpq_astar_destroy": ([_VP], ctypes.c_int),
     "gpq_astar_solve": ([_VP, _VP, ctypes.c_uint32, _VP, _VP], ctypes.c_int),
     "gpq_astar_last_stats": ([_VP, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
-                              ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32),
-                              ctypes.POINTER(ctypes.c_uint32)], ctypes.c_int),
+                              ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint64),
+                              ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32)], ctypes.c_int),
     "gpq_astar_path": ([_VP, ctypes.c_uint32, _VP, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32), _VP],
                        ctypes.c_int),
     "gpq_astar_gcost": ([_VP, ctypes.c_uint32, _VP, ctypes.c_uint64, _VP], ctypes.c_int),
@@ -414,7 +414,7 @@ ASTAR_RESULT_DTYPE = np.dtype([("cost", "<u4"), ("path_len", "<u4"), ("expanded"
 class AstarConfig(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint32) for n in ("tile", "window", "inbox_capacity", "open_capacity",
                                                "frontier_capacity", "block_threads", "ctas_per_sm",
-                                               "max_rounds")] + [("reserved", ctypes.c_uint32 * 4)]
+                                               "max_rounds", "tile_worker")] + [("reserved", ctypes.c_uint32 * 3)]
 
 
 def density_threshold(p: float) -> int:
@@ -475,9 +475,11 @@ class AStar:
     def stats(self):
         t, s = ctypes.c_float(), ctypes.c_float()
         r, g, b = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        v = ctypes.c_uint64()
         check(lib().gpq_astar_last_stats(self._h, ctypes.byref(t), ctypes.byref(s), ctypes.byref(r),
-                                         ctypes.byref(g), ctypes.byref(b)), "gpq_astar_last_stats")
-        return {"total_ms": t.value, "search_ms": s.value, "rounds": r.value, "grid": g.value, "block": b.value}
+                                         ctypes.byref(v), ctypes.byref(g), ctypes.byref(b)), "gpq_astar_last_stats")
+        return {"total_ms": t.value, "search_ms": s.value, "rounds": r.value, "tile_visits": v.value,
+                "grid": g.value, "block": b.value}
 
     def path(self, index, capacity=1 << 20):
         out = np.zeros(capacity, np.uint32)

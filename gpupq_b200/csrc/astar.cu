@@ -38,6 +38,7 @@ struct gpq_astar {
   uint64_t n_cells = 0;
   float total_ms = 0.f, search_ms = 0.f;
   uint32_t rounds = 0, grid = 0, block = 0;
+  uint64_t visits = 0;
   bool solved = false;
 };
 
@@ -62,13 +63,15 @@ bool is_pow2(uint32_t x) { return x && !(x & (x - 1)); }
 
 gpq_status normalize(gpq_astar_config& c) {
   if (c.tile == 0) c.tile = 64;
-  GPQ_CHECK_ARG(is_pow2(c.tile) && c.tile >= 8 && c.tile <= 256, "tile must be a power of two in [8, 256]");
+  GPQ_CHECK_ARG(is_pow2(c.tile) && c.tile >= 8 && c.tile <= 128, "tile must be a power of two in [8, 128]");
   if (c.inbox_capacity == 0) c.inbox_capacity = 8 * c.tile;
   if (c.open_capacity == 0) c.open_capacity = c.tile * c.tile;
-  if (c.frontier_capacity == 0) c.frontier_capacity = 2048;
+  GPQ_CHECK_ARG(c.tile_worker <= 1, "tile_worker must be 0 (CTA) or 1 (warp)");
+  if (c.frontier_capacity == 0) c.frontier_capacity = c.tile_worker ? 256 : 2048;
   GPQ_CHECK_ARG(c.frontier_capacity >= 64 && c.frontier_capacity <= 8192, "frontier_capacity in [64, 8192]");
   if (c.block_threads == 0) c.block_threads = 256;
-  GPQ_CHECK_ARG(c.block_threads == 128 || c.block_threads == 256, "block_threads must be 128 or 256");
+  GPQ_CHECK_ARG(c.block_threads == 64 || c.block_threads == 128 || c.block_threads == 256,
+                "block_threads must be 64, 128 or 256");
   if (c.max_rounds == 0) c.max_rounds = 1u << 20;
   return GPQ_OK;
 }
@@ -137,11 +140,11 @@ gpq_status gpq_astar_query(uint64_t base_seed, uint32_t index, uint32_t conn, ui
   return GPQ_OK;
 }
 
-gpq_status gpq_astar_solve(gpq_astar* a, const gpq_astar_grid* grids, uint32_t n, gpq_astar_result* results,
-                           void* stream) {
-  GPQ_CHECK_ARG(a && grids && results, "NULL argument");
-  GPQ_CHECK_ARG(n >= 1 && n <= 65535, "need 1 <= n <= 65535 instances per solve");
-  const cudaStream_t st = gpq::as_stream(stream, a->own);
+}  // extern "C"
+
+// One launch over the batch with the current tile capacities.
+static gpq_status astar_solve_pass(gpq_astar* a, const gpq_astar_grid* grids, uint32_t n, gpq_astar_result* results,
+                                   cudaStream_t st) {
   const gpq_astar_config& c = a->cfg;
   const uint32_t ts = c.tile;
   // layout
@@ -166,6 +169,8 @@ gpq_status gpq_astar_solve(gpq_astar* a, const gpq_astar_grid* grids, uint32_t n
     I.tiles_y = (g.height + ts - 1) / ts;
     I.ub = (g.start == g.goal) ? 0u : kAstarInf;
     I.delta = c.window ? c.window : (g.conn == 4 ? 4u : 40u);
+    I.gx = g.goal % g.width;
+    I.gy = g.goal / g.width;
     const uint32_t h0 = gpq_astar_h(g.conn, g.start, g.goal, g.width);
     I.bound = (uint32_t)std::min<uint64_t>((uint64_t)h0 + I.delta, 0xFFFFFFFEull);
     I.done = 0;
@@ -181,7 +186,7 @@ gpq_status gpq_astar_solve(gpq_astar* a, const gpq_astar_grid* grids, uint32_t n
   a->n_cells = cell0;
   // buffers
   GPQ_TRY(grow(&a->gcost, a->cap_cells, cell0));
-  GPQ_TRY(grow(&a->blk, a->cap_cells / 32, cell0 / 32));
+  GPQ_TRY(grow(&a->blk, a->cap_cells / 32 + 1, cell0 / 32 + 1));  // +1: tile loads read one word ahead
   a->cap_cells = std::max(a->cap_cells, cell0);
   if (n > a->cap_inst) {
     GPQ_TRY(grow(&a->word0, 0, n));
@@ -211,16 +216,19 @@ gpq_status gpq_astar_solve(gpq_astar* a, const gpq_astar_grid* grids, uint32_t n
   d.in_cap = c.inbox_capacity;
   d.open_cap = c.open_capacity;
   d.ts = ts;
+  d.lts = (uint32_t)__builtin_ctz(ts);
   d.max_rounds = c.max_rounds;
   d.frontier_cap = c.frontier_capacity;
   d.spin_limit = gpq::spin_limit();
   // launch geometry
-  const size_t smem = 2ull * c.frontier_capacity * sizeof(uint2);
-  GPQ_CUDA_TRY(cudaFuncSetAttribute(astar_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const void* kern = c.tile_worker ? (const void*)astar_persistent_kernel<true> : (const void*)astar_persistent_kernel<false>;
+  const size_t smem = astar_worker_smem_bytes(ts, c.frontier_capacity) * (c.tile_worker ? c.block_threads / 32 : 1);
+  GPQ_CHECK_ARG(smem <= 227u * 1024u, "tile, frontier_capacity and workers need more than 227 KB of shared memory");
+  GPQ_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int dev = 0, sms = 0, per_sm = 0;
   GPQ_CUDA_TRY(cudaGetDevice(&dev));
   GPQ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  GPQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, astar_persistent_kernel, (int)c.block_threads, smem));
+  GPQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (int)c.block_threads, smem));
   if (per_sm < 1) {
     set_last_error("astar: kernel does not fit on an SM (block %u, smem %zu)", c.block_threads, smem);
     return GPQ_ERR_INVALID;
@@ -243,8 +251,7 @@ gpq_status gpq_astar_solve(gpq_astar* a, const gpq_astar_grid* grids, uint32_t n
   GPQ_CUDA_TRY(cudaGetLastError());
   GPQ_CUDA_TRY(cudaEventRecord(a->ev[1], st));
   void* args[] = {&d};
-  GPQ_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)astar_persistent_kernel, dim3(grid), dim3(c.block_threads),
-                                           args, smem, st));
+  GPQ_CUDA_TRY(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(c.block_threads), args, smem, st));
   GPQ_CUDA_TRY(cudaEventRecord(a->ev[2], st));
   GPQ_CUDA_TRY(cudaMemsetAsync(a->fin, 0, 2ull * n * sizeof(unsigned long long), st));
   const uint32_t fx = (uint32_t)std::min<uint64_t>((max_cells + 255) / 256, 64);
@@ -262,6 +269,7 @@ gpq_status gpq_astar_solve(gpq_astar* a, const gpq_astar_grid* grids, uint32_t n
   GPQ_CUDA_TRY(cudaEventElapsedTime(&a->total_ms, a->ev[0], a->ev[3]));
   GPQ_CUDA_TRY(cudaEventElapsedTime(&a->search_ms, a->ev[1], a->ev[2]));
   a->rounds = ctl.rounds;
+  a->visits = ctl.visits;
   a->solved = true;
   for (uint32_t i = 0; i < n; ++i) {
     const AstarInstDev& I = a->h_inst[i];
@@ -286,13 +294,48 @@ gpq_status gpq_astar_solve(gpq_astar* a, const gpq_astar_grid* grids, uint32_t n
   return GPQ_OK;
 }
 
-gpq_status gpq_astar_last_stats(gpq_astar* a, float* total_ms, float* search_ms, uint32_t* rounds, uint32_t* grid,
-                                uint32_t* block) {
+extern "C" {
+
+// A batch in which some instance overflowed its tile buffers runs again with four times
+// the capacities (at most twice); the capacities stay for later calls.
+gpq_status gpq_astar_solve(gpq_astar* a, const gpq_astar_grid* grids, uint32_t n, gpq_astar_result* results,
+                           void* stream) {
+  GPQ_CHECK_ARG(a && grids && results, "NULL argument");
+  GPQ_CHECK_ARG(n >= 1 && n <= 65535, "need 1 <= n <= 65535 instances per solve");
+  const cudaStream_t st = gpq::as_stream(stream, a->own);
+  float total = 0.f, search = 0.f;
+  uint32_t rounds = 0;
+  uint64_t visits = 0;
+  for (int attempt = 0;; ++attempt) {
+    const gpq_status s = astar_solve_pass(a, grids, n, results, st);
+    total += a->total_ms;
+    search += a->search_ms;
+    rounds += a->rounds;
+    visits += a->visits;
+    if (s != GPQ_OK) return s;
+    bool overflow = false;
+    for (uint32_t i = 0; i < n; ++i)
+      overflow |= results[i].status == GPQ_ERR_QUEUE_FULL || results[i].status == GPQ_ERR_INSERT_FULL;
+    if (!overflow || attempt == 2) break;
+    a->cfg.inbox_capacity *= 4;
+    a->cfg.open_capacity *= 4;
+    a->cap_tiles = 0;  // reallocate the tile buffers at the new capacities
+  }
+  a->total_ms = total;
+  a->search_ms = search;
+  a->rounds = rounds;
+  a->visits = visits;
+  return GPQ_OK;
+}
+
+gpq_status gpq_astar_last_stats(gpq_astar* a, float* total_ms, float* search_ms, uint32_t* rounds,
+                                uint64_t* tile_visits, uint32_t* grid, uint32_t* block) {
   GPQ_CHECK_ARG(a, "NULL handle");
   if (!a->solved) return GPQ_ERR_NOT_READY;
   if (total_ms) *total_ms = a->total_ms;
   if (search_ms) *search_ms = a->search_ms;
   if (rounds) *rounds = a->rounds;
+  if (tile_visits) *tile_visits = a->visits;
   if (grid) *grid = a->grid;
   if (block) *block = a->block;
   return GPQ_OK;

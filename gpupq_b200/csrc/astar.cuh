@@ -20,7 +20,8 @@
 //     window; the window moves to [min f of its open arrays, + delta], or the instance
 //     is done when that minimum exceeds UB.
 //
-// Work items are 8 bytes (cell, g); f = g + h(cell) is recomputed.  With a consistent
+// Work items are 8 bytes (y << 16 | x, g); f = g + h(x, y) is recomputed, so the hot loop
+// needs no division.  With a consistent
 // heuristic every cell with g + h <= C* ends with its exact g, whatever the order of
 // expansions, so the outputs (C*, the expanded set, the canonical path) do not depend
 // on the schedule; re-expansions only cost time.
@@ -44,6 +45,7 @@ struct AstarInstDev {
   uint32_t windows;
   uint32_t delta;      // window width on f
   unsigned long long pops;  // expansions performed (re-expansions included)
+  uint32_t gx, gy;     // goal coordinates
 };
 
 struct AstarTileDev {
@@ -63,6 +65,7 @@ struct AstarCtl {
   uint32_t err;
   uint32_t rounds;
   unsigned long long bar;
+  unsigned long long visits;  // tiles processed
 };
 
 struct AstarDev {
@@ -77,6 +80,7 @@ struct AstarDev {
   uint32_t n_inst, n_tiles;
   uint32_t in_cap, open_cap;
   uint32_t ts;      // tile side
+  uint32_t lts;     // log2(ts)
   uint32_t max_rounds;
   uint32_t frontier_cap;  // per shared frontier buffer
   uint64_t spin_limit;
@@ -93,6 +97,13 @@ __device__ __forceinline__ uint32_t astar_tile_of(const AstarDev& d, const Astar
   const uint32_t x = cell % I.g.width, y = cell / I.g.width;
   return I.tile0 + (y / d.ts) * I.tiles_x + x / d.ts;
 }
+
+__device__ __forceinline__ uint32_t astar_hxy(uint32_t conn, int x, int y, int gx, int gy) {
+  const uint32_t dx = (uint32_t)abs(x - gx), dy = (uint32_t)abs(y - gy);
+  return conn == 4 ? dx + dy : 10u * max(dx, dy) + 4u * min(dx, dy);
+}
+
+__device__ __forceinline__ uint32_t astar_pack(int x, int y) { return ((uint32_t)y << 16) | (uint32_t)x; }
 
 // Put tile t on the active list of round parity `par` (once per round).
 __device__ __forceinline__ void astar_activate(const AstarDev& d, uint32_t t, uint32_t par, bool count) {
@@ -114,17 +125,62 @@ __device__ __forceinline__ void astar_inbox_push(const AstarDev& d, AstarInstDev
   astar_activate(d, t, par, true);
 }
 
-// Shared state of the CTA working on one tile.
+// Shared state of the CTA working on one tile.  While a CTA holds a tile, the tile's g
+// values live in shared memory (gt) and only this CTA changes them; other tiles lower the
+// global copy with atomicMin (a filter for their sends) and the holder merges its copy
+// back with atomicMin when it lets go of the tile.
 struct AstarTileSmem {
-  uint2* fa;  // frontier buffers
+  uint2* fa;      // frontier buffers [frontier_cap]
   uint2* fb;
-  uint32_t n[2];
+  uint32_t* gt;   // [ts * ts] g of the tile's cells, local index ly * ts + lx
+  uint32_t* blk;  // [ts * ts / 32] blocked bits of the tile
+  uint32_t* chg;  // [ts * ts / 32] cells whose g dropped during this visit
+  uint32_t n[3];  // frontier fill, rotating by level
+  uint32_t ub;    // the instance's best goal cost as of this visit (stale values only prune less)
   uint32_t open_min;
   uint32_t open_cnt;
-  uint32_t t;
-  uint32_t inst;
   unsigned long long pops;
   uint32_t scan[33];
+};
+
+__host__ __device__ inline size_t astar_smem_bytes(uint32_t ts, uint32_t frontier_cap) {
+  return 2ull * frontier_cap * sizeof(uint2) + (size_t)ts * ts * sizeof(uint32_t) + 2ull * (ts * ts / 32) * sizeof(uint32_t);
+}
+
+// Geometry of the tile being processed.
+struct AstarTileGeo {
+  uint32_t x0, y0, tw, th, ts;
+  __device__ __forceinline__ bool inside(int x, int y) const {
+    return x >= (int)x0 && y >= (int)y0 && x < (int)(x0 + tw) && y < (int)(y0 + th);
+  }
+  uint32_t lts;
+  __device__ __forceinline__ uint32_t local(int x, int y) const {
+    return (((uint32_t)y - y0) << lts) + ((uint32_t)x - x0);
+  }
+};
+
+// The threads that process one tile visit: the whole CTA, or one warp (WARP), in which
+// case every warp of the CTA works on its own tile with its own slice of shared memory.
+template <bool WARP>
+struct AstarWorker {
+  uint32_t tid;  // thread within the worker
+  uint32_t n;    // threads in the worker
+  uint32_t id;   // worker within the CTA
+  __device__ __forceinline__ AstarWorker() {
+    if (WARP) {
+      tid = threadIdx.x & 31u;
+      n = 32u;
+      id = threadIdx.x >> 5;
+    } else {
+      tid = threadIdx.x;
+      n = blockDim.x;
+      id = 0;
+    }
+  }
+  __device__ __forceinline__ void sync() const {
+    if (WARP) __syncwarp();
+    else __syncthreads();
+  }
 };
 
 // Frontier push: into the shared buffer, or (when it is full) into the tile's own inbox
@@ -150,37 +206,100 @@ __device__ __forceinline__ void astar_open_push(const AstarDev& d, AstarInstDev*
   }
 }
 
-// Expand one frontier item of tile t (one thread).
-__device__ __forceinline__ void astar_expand(const AstarDev& d, AstarInstDev* Ip, const AstarInstDev& I,
-                                             AstarTileSmem& sm, uint2* next, uint32_t which, uint32_t t, uint32_t npar,
-                                             uint2 it, uint32_t bound, uint32_t* pops) {
-  const uint32_t cell = it.x, g = it.y;
-  uint32_t* G = d.gcost + I.cell0;
-  if (ldcg_u32(&G[cell]) != g) return;  // a better path reached the cell meanwhile
-  ++*pops;
-  const uint32_t w = I.g.width, h = I.g.height, conn = I.g.conn;
-  const int x = (int)(cell % w), y = (int)(cell / w);
-  const int nk = conn == 4 ? 4 : 8;
-  for (int k = 0; k < nk; ++k) {
-    const int nx = x + gpq_astar_dx(k), ny = y + gpq_astar_dy(k);
-    if (nx < 0 || ny < 0 || nx >= (int)w || ny >= (int)h) continue;
-    const uint32_t nb = (uint32_t)ny * w + (uint32_t)nx;
-    if (astar_blocked(d, I, nb)) continue;
-    if (k >= 4 && (astar_blocked(d, I, (uint32_t)y * w + (uint32_t)nx) || astar_blocked(d, I, (uint32_t)ny * w + (uint32_t)x)))
-      continue;
-    const uint32_t ng = g + gpq_astar_cost(conn, k);
-    const uint32_t old = atomicMin(&G[nb], ng);
-    if (ng >= old) continue;
-    const uint32_t nf = ng + gpq_astar_h(conn, nb, I.g.goal, w);
-    if (nb == I.g.goal) atomicMin(&Ip->ub, ng);
-    if (nf > ldcg_u32(&Ip->ub)) continue;
-    const uint2 child = make_uint2(nb, ng);
-    const uint32_t nt = astar_tile_of(d, I, nb);
-    if (nt == t) {
-      if (nf <= bound) astar_frontier_push(d, Ip, sm, next, which, t, npar, child);
-      else astar_open_push(d, Ip, sm, t, child, nf);
-    } else {
-      astar_inbox_push(d, Ip, nt, npar, child);
+__device__ __forceinline__ bool astar_cell_blocked(const AstarDev& d, const AstarInstDev& I, const AstarTileSmem& sm,
+                                                   const AstarTileGeo& tg, int x, int y) {
+  if (tg.inside(x, y)) {
+    const uint32_t l = tg.local(x, y);
+    return (sm.blk[l >> 5] >> (l & 31u)) & 1u;
+  }
+  return astar_blocked(d, I, (uint32_t)y * I.g.width + (uint32_t)x);
+}
+
+// Expand frontier items src[ib .. ib + 32 / M) with one warp, one lane per (item, move):
+// lane = item * M + move, M = 4 or 8 moves (all lanes call; ib is warp-uniform).  A level
+// of few items thus costs the latency of one move, not of M moves in a row.  Children
+// are appended with one shared atomic per warp and target: the frontier and the open
+// array are the two hot counters of a level.
+__device__ __forceinline__ void astar_expand_warp(const AstarDev& d, AstarInstDev* Ip, const AstarInstDev& I,
+                                                  AstarTileSmem& sm, const AstarTileGeo& tg, const uint2* src,
+                                                  uint32_t ib, uint32_t n, uint2* next, uint32_t which, uint32_t t,
+                                                  uint32_t npar, uint32_t bound, uint32_t* pops) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t lt = (1u << lane) - 1u;
+  const uint32_t conn = I.g.conn;
+  const uint32_t M = conn == 4 ? 4u : 8u;
+  const uint32_t k = lane & (M - 1u);
+  const uint32_t i = ib + lane / M;
+  uint32_t kind = 0;  // 1 frontier, 2 open array, 3 another tile's inbox
+  uint2 child = make_uint2(0, 0);
+  uint32_t nf = kAstarInf;
+  if (i < n) {
+    const uint2 it = src[i];
+    const int x = (int)(it.x & 0xffffu), y = (int)(it.x >> 16);
+    const uint32_t g = it.y;
+    if (sm.gt[tg.local(x, y)] == g) {  // else a better path reached the cell meanwhile
+      if (k == 0) ++*pops;
+      const uint32_t w = I.g.width, h = I.g.height;
+      const int nx = x + gpq_astar_dx((int)k), ny = y + gpq_astar_dy((int)k);
+      if (nx >= 0 && ny >= 0 && nx < (int)w && ny < (int)h) {
+        const bool in = tg.inside(nx, ny);
+        const uint32_t l = in ? tg.local(nx, ny) : 0u;
+        bool ok = !(in ? ((sm.blk[l >> 5] >> (l & 31u)) & 1u) : astar_blocked(d, I, (uint32_t)ny * w + (uint32_t)nx));
+        if (ok && k >= 4) ok = !astar_cell_blocked(d, I, sm, tg, nx, y) && !astar_cell_blocked(d, I, sm, tg, x, ny);
+        if (ok) {
+          const uint32_t ng = g + gpq_astar_cost(conn, (int)k);
+          if (in) {
+            ok = ng < atomicMin(&sm.gt[l], ng);
+            if (ok) atomicOr(&sm.chg[l >> 5], 1u << (l & 31u));
+          } else {
+            ok = ng < atomicMin(&d.gcost[I.cell0 + (uint32_t)ny * w + (uint32_t)nx], ng);
+          }
+          if (ok) {
+            const int gx = (int)I.gx, gy = (int)I.gy;
+            nf = ng + astar_hxy(conn, nx, ny, gx, gy);
+            if (nx == gx && ny == gy) {
+              atomicMin(&Ip->ub, ng);
+              atomicMin(&sm.ub, ng);
+            }
+            if (nf <= sm.ub) {
+              child = make_uint2(astar_pack(nx, ny), ng);
+              kind = in ? (nf <= bound ? 1u : 2u) : 3u;
+              if (kind == 3u) {
+                const uint32_t nt = I.tile0 + ((uint32_t)ny >> d.lts) * I.tiles_x + ((uint32_t)nx >> d.lts);
+                astar_inbox_push(d, Ip, nt, npar, child);
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+  const uint32_t mf = __ballot_sync(GPQ_FULL_MASK, kind == 1u);
+  if (mf) {
+    const uint32_t leader = (uint32_t)(__ffs(mf) - 1);
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(&sm.n[which], (uint32_t)__popc(mf));
+    base = __shfl_sync(GPQ_FULL_MASK, base, leader);
+    if (kind == 1u) {
+      const uint32_t pos = base + __popc(mf & lt);
+      if (pos < d.frontier_cap) next[pos] = child;
+      else astar_inbox_push(d, Ip, t, npar, child);  // full: the tile's own next round
+    }
+  }
+  const uint32_t mo = __ballot_sync(GPQ_FULL_MASK, kind == 2u);
+  if (mo) {
+    const uint32_t leader = (uint32_t)(__ffs(mo) - 1);
+    const uint32_t fmin = __reduce_min_sync(GPQ_FULL_MASK, kind == 2u ? nf : kAstarInf);
+    uint32_t base = 0;
+    if (lane == leader) {
+      base = atomicAdd(&sm.open_cnt, (uint32_t)__popc(mo));
+      atomicMin(&sm.open_min, fmin);
+    }
+    base = __shfl_sync(GPQ_FULL_MASK, base, leader);
+    if (kind == 2u) {
+      const uint32_t pos = base + __popc(mo & lt);
+      if (pos < d.open_cap) d.open[(size_t)t * d.open_cap + pos] = child;
+      else gpq_set_error(&Ip->err, GPQ_ERR_QUEUE_FULL);
     }
   }
 }
@@ -212,48 +331,98 @@ __device__ __forceinline__ uint32_t astar_block_scan(uint32_t flag, uint32_t* sc
   return off;
 }
 
-// Process tile t in round s (the whole CTA).
-__device__ void astar_process_tile(const AstarDev& d, uint32_t t, uint32_t s, AstarTileSmem& sm) {
+template <bool WARP>
+__device__ __forceinline__ uint32_t astar_worker_scan(uint32_t flag, uint32_t* scratch, uint32_t* total) {
+  if (WARP) {
+    const uint32_t bal = __ballot_sync(GPQ_FULL_MASK, flag);
+    *total = (uint32_t)__popc(bal);
+    return (uint32_t)__popc(bal & ((1u << (threadIdx.x & 31u)) - 1u));
+  }
+  return astar_block_scan(flag, scratch, total);
+}
+
+// Process tile t in round s (one worker).
+template <bool WARP>
+__device__ void astar_process_tile(const AstarDev& d, uint32_t t, uint32_t s, AstarTileSmem& sm,
+                                   const AstarWorker<WARP>& wk) {
   const uint32_t par = s & 1u, npar = par ^ 1u;
   AstarTileDev* T = d.tiles + t;
   AstarInstDev* Ip = d.inst + T->inst;
   const AstarInstDev I = *Ip;  // static fields; ub/bound are read through Ip
   uint32_t* G = d.gcost + I.cell0;
-  if (threadIdx.x == 0) {
+  const uint32_t ts = d.ts, words = ts * ts / 32;
+  AstarTileGeo tg;
+  tg.ts = ts;
+  tg.lts = d.lts;
+  tg.x0 = T->tx * ts;
+  tg.y0 = T->ty * ts;
+  tg.tw = min(ts, I.g.width - tg.x0);
+  tg.th = min(ts, I.g.height - tg.y0);
+  if (wk.tid == 0) {
     sm.n[0] = 0;
     sm.n[1] = 0;
+    sm.n[2] = 0;
     sm.pops = 0;
     sm.open_cnt = T->open_cnt;
     sm.open_min = kAstarInf;
   }
-  __syncthreads();
+  wk.sync();
   const uint32_t k_in = min(ldcg_u32(&T->in_cnt[par]), d.in_cap);
   const uint32_t bound = ldcg_u32(&Ip->bound);
   if (ldcg_u32(&Ip->done)) {
-    if (threadIdx.x == 0) {
+    if (wk.tid == 0) {
       T->in_cnt[par] = 0;
       T->queued[par] = 0;
       T->open_cnt = 0;
       T->open_min = kAstarInf;
     }
-    __syncthreads();
+    wk.sync();
     return;
   }
-  uint32_t ub = ldcg_u32(&Ip->ub);
+  const uint32_t ub = ldcg_u32(&Ip->ub);
+  if (wk.tid == 0) {
+    sm.ub = ub;
+    atomicAdd(&d.ctl->visits, 1ull);
+  }
+  // 0. the tile's g values and blocked bits into shared memory
+  for (uint32_t j = wk.tid; j < words; j += wk.n) {
+    sm.blk[j] = 0;
+    sm.chg[j] = 0;
+  }
+  for (uint32_t l = wk.tid; l < ts * ts; l += wk.n) {
+    const uint32_t lx = l % ts, ly = l / ts;
+    sm.gt[l] = (lx < tg.tw && ly < tg.th) ? ldcg_u32(&G[(tg.y0 + ly) * I.g.width + tg.x0 + lx]) : kAstarInf;
+  }
+  wk.sync();
+  {
+    const uint32_t segw = ts < 32 ? ts : 32u, segs = ts / segw;
+    for (uint32_t j = wk.tid; j < tg.th * segs; j += wk.n) {
+      const uint32_t ly = j / segs, lx0 = (j % segs) * segw;
+      if (lx0 >= tg.tw) continue;
+      const uint64_t b0 = I.cell0 + (uint64_t)(tg.y0 + ly) * I.g.width + tg.x0 + lx0;
+      uint32_t bits = __funnelshift_r(__ldg(&d.blk[b0 >> 5]), __ldg(&d.blk[(b0 >> 5) + 1]), (uint32_t)(b0 & 31u));
+      const uint32_t nb = min(segw, tg.tw - lx0);
+      if (nb < 32) bits &= (1u << nb) - 1u;
+      const uint32_t l0 = ly * ts + lx0;
+      atomicOr(&sm.blk[l0 >> 5], bits << (l0 & 31u));
+    }
+  }
+  wk.sync();
   // 1. the open array, when the window reached it: expand-now items leave, the rest is
   //    compacted in place (a chunk is read completely before any of it is written)
   const uint32_t n_open = sm.open_cnt;
   if (n_open > 0 && ldcg_u32(&T->open_min) <= bound) {
     uint2* O = d.open + (size_t)t * d.open_cap;
     uint32_t kept = 0;
-    for (uint32_t c0 = 0; c0 < n_open; c0 += blockDim.x) {
-      const uint32_t i = c0 + threadIdx.x;
+    for (uint32_t c0 = 0; c0 < n_open; c0 += wk.n) {
+      const uint32_t i = c0 + wk.tid;
       uint2 it = make_uint2(0, kAstarInf);
       uint32_t keep = 0, f = kAstarInf;
       if (i < n_open) {
         it = O[i];
-        if (ldcg_u32(&G[it.x]) == it.y) {
-          f = it.y + gpq_astar_h(I.g.conn, it.x, I.g.goal, I.g.width);
+        const int x = (int)(it.x & 0xffffu), y = (int)(it.x >> 16);
+        if (sm.gt[tg.local(x, y)] == it.y) {
+          f = it.y + astar_hxy(I.g.conn, x, y, (int)I.gx, (int)I.gy);
           if (f <= ub) {
             if (f <= bound) astar_frontier_push(d, Ip, sm, sm.fa, 0, t, npar, it);
             else keep = 1;
@@ -261,61 +430,70 @@ __device__ void astar_process_tile(const AstarDev& d, uint32_t t, uint32_t s, As
         }
       }
       uint32_t total;
-      const uint32_t off = astar_block_scan(keep, sm.scan, &total);
+      const uint32_t off = astar_worker_scan<WARP>(keep, sm.scan, &total);
       if (keep) {
         O[kept + off] = it;
         atomicMin(&sm.open_min, f);
       }
       kept += total;
     }
-    if (threadIdx.x == 0) sm.open_cnt = kept;
-    __syncthreads();
-  } else if (threadIdx.x == 0) {
+    if (wk.tid == 0) sm.open_cnt = kept;
+    wk.sync();
+  } else if (wk.tid == 0) {
     sm.open_min = ldcg_u32(&T->open_min);
   }
-  __syncthreads();
-  // 2. the inbox
+  wk.sync();
+  // 2. the inbox (senders lowered the global g of these cells before sending)
   {
     const uint2* B = d.inbox + ((size_t)par * d.n_tiles + t) * d.in_cap;
-    for (uint32_t i = threadIdx.x; i < k_in; i += blockDim.x) {
+    for (uint32_t i = wk.tid; i < k_in; i += wk.n) {
       const uint2 it = B[i];
-      if (ldcg_u32(&G[it.x]) != it.y) continue;
-      const uint32_t f = it.y + gpq_astar_h(I.g.conn, it.x, I.g.goal, I.g.width);
+      const int x = (int)(it.x & 0xffffu), y = (int)(it.x >> 16);
+      if (sm.gt[tg.local(x, y)] != it.y) continue;
+      const uint32_t f = it.y + astar_hxy(I.g.conn, x, y, (int)I.gx, (int)I.gy);
       if (f > ub) continue;
       if (f <= bound) astar_frontier_push(d, Ip, sm, sm.fa, 0, t, npar, it);
       else astar_open_push(d, Ip, sm, t, it, f);
     }
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
+  wk.sync();
+  if (wk.tid == 0) {
     T->in_cnt[par] = 0;
     T->queued[par] = 0;
   }
-  // 3. level-by-level expansion of the frontier inside the tile
+  // 3. level-by-level expansion of the frontier inside the tile; level i reads buffer
+  //    i % 2 with fill n[i % 3], fills the other buffer and n[(i + 1) % 3], and clears
+  //    n[(i + 2) % 3] (read at level i - 1, filled at level i + 1): one barrier a level
   uint32_t pops = 0;
-  uint32_t cur = 0;
-  for (;;) {
-    const uint32_t n = min(sm.n[cur], d.frontier_cap);
+  for (uint32_t lv = 0;; ++lv) {
+    const uint32_t c3 = lv % 3u;
+    const uint32_t n = min(sm.n[c3], d.frontier_cap);
     if (n == 0) break;
-    uint2* src = cur ? sm.fb : sm.fa;
-    uint2* dst = cur ? sm.fa : sm.fb;
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
-      astar_expand(d, Ip, I, sm, dst, cur ^ 1u, t, npar, src[i], bound, &pops);
-    __syncthreads();
-    if (threadIdx.x == 0) sm.n[cur] = 0;
-    cur ^= 1u;
-    __syncthreads();
+    uint2* src = (lv & 1u) ? sm.fb : sm.fa;
+    uint2* dst = (lv & 1u) ? sm.fa : sm.fb;
+    if (wk.tid == 0) sm.n[(c3 + 2u) % 3u] = 0;
+    const uint32_t ipw = I.g.conn == 4 ? 8u : 4u;  // items per warp pass
+    for (uint32_t ib = (wk.tid >> 5) * ipw; ib < n; ib += (wk.n >> 5) * ipw)
+      astar_expand_warp(d, Ip, I, sm, tg, src, ib, n, dst, (c3 + 1u) % 3u, t, npar, bound, &pops);
+    wk.sync();
+  }
+  // 4. merge the tile's g values back
+  for (uint32_t l = wk.tid; l < ts * ts; l += wk.n) {
+    if ((sm.chg[l >> 5] >> (l & 31u)) & 1u) {
+      const uint32_t lx = l % ts, ly = l / ts;
+      atomicMin(&G[(tg.y0 + ly) * I.g.width + tg.x0 + lx], sm.gt[l]);
+    }
   }
   pops = warp_sum_u32(pops);
   if ((threadIdx.x & 31u) == 0 && pops) atomicAdd(&sm.pops, (unsigned long long)pops);
-  __syncthreads();
-  if (threadIdx.x == 0) {
+  wk.sync();
+  if (wk.tid == 0) {
     const uint32_t oc = min(sm.open_cnt, d.open_cap);
     T->open_cnt = oc;
     T->open_min = oc ? sm.open_min : kAstarInf;
     if (sm.pops) atomicAdd(&Ip->pops, sm.pops);
   }
-  __syncthreads();
+  wk.sync();
 }
 
 // Phase W for one instance (one warp): a drained window moves on, or the instance ends.
@@ -351,15 +529,28 @@ __device__ void astar_window_step(const AstarDev& d, uint32_t i, uint32_t npar) 
   }
 }
 
-// The persistent search loop over all instances.  Dynamic shared memory: two frontier
-// buffers of frontier_cap items.
+// The persistent search loop over all instances.  Dynamic shared memory: one slice of
+// astar_worker_smem_bytes(ts, frontier_cap) per worker (per warp when WARP).
+static constexpr uint32_t kAstarMaxWorkers = 8;  // 256 threads / 32
+
+__host__ __device__ inline size_t astar_worker_smem_bytes(uint32_t ts, uint32_t frontier_cap) {
+  return (astar_smem_bytes(ts, frontier_cap) + 15u) & ~(size_t)15u;
+}
+
+template <bool WARP>
 static __global__ void __launch_bounds__(256) astar_persistent_kernel(AstarDev d) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ AstarTileSmem sm;
+  __shared__ AstarTileSmem sms[kAstarMaxWorkers];
   __shared__ uint32_t s_t;
-  if (threadIdx.x == 0) {
-    sm.fa = reinterpret_cast<uint2*>(smem_raw);
+  const AstarWorker<WARP> wk;
+  AstarTileSmem& sm = sms[wk.id];
+  if (wk.tid == 0) {
+    unsigned char* base = smem_raw + (size_t)wk.id * astar_worker_smem_bytes(d.ts, d.frontier_cap);
+    sm.fa = reinterpret_cast<uint2*>(base);
     sm.fb = sm.fa + d.frontier_cap;
+    sm.gt = reinterpret_cast<uint32_t*>(sm.fb + d.frontier_cap);
+    sm.blk = sm.gt + d.ts * d.ts;
+    sm.chg = sm.blk + d.ts * d.ts / 32;
   }
   __syncthreads();
   const unsigned long long nb = gridDim.x;
@@ -370,12 +561,19 @@ static __global__ void __launch_bounds__(256) astar_persistent_kernel(AstarDev d
     const uint32_t par = s & 1u, npar = par ^ 1u;
     const uint32_t n = ldcg_u32(&d.ctl->al_cnt[par]);
     for (;;) {
-      if (threadIdx.x == 0) s_t = atomicAdd(&d.ctl->work[par], 1u);
-      __syncthreads();
-      const uint32_t j = s_t;
-      __syncthreads();
+      uint32_t j;
+      if (WARP) {
+        j = 0;
+        if (wk.tid == 0) j = atomicAdd(&d.ctl->work[par], 1u);
+        j = __shfl_sync(GPQ_FULL_MASK, j, 0);
+      } else {
+        if (threadIdx.x == 0) s_t = atomicAdd(&d.ctl->work[par], 1u);
+        __syncthreads();
+        j = s_t;
+        __syncthreads();
+      }
       if (j >= n) break;
-      astar_process_tile(d, d.al[(size_t)par * d.n_tiles + j], s, sm);
+      astar_process_tile<WARP>(d, d.al[(size_t)par * d.n_tiles + j], s, sm, wk);
     }
     bar_target += nb;
     if (!grid_barrier(&d.ctl->bar, bar_target, d.spin_limit, &d.ctl->err)) return;
@@ -428,7 +626,7 @@ static __global__ void astar_init_kernel(AstarDev d) {
   d.gcost[I.cell0 + I.g.start] = 0;
   const uint32_t t = astar_tile_of(d, I, I.g.start);
   d.tiles[t].in_cnt[0] = 1;
-  d.inbox[(size_t)t * d.in_cap] = make_uint2(I.g.start, 0);
+  d.inbox[(size_t)t * d.in_cap] = make_uint2(astar_pack((int)(I.g.start % I.g.width), (int)(I.g.start / I.g.width)), 0);
   d.tiles[t].queued[0] = 1;
   d.al[i] = t;
   if (i == 0) d.ctl->al_cnt[0] = d.n_inst;

@@ -229,15 +229,16 @@ GPQ_API gpq_status gpq_phold_run_static(const gpq_phold_config* cfg, const gpq_i
  * (`tile` x `tile` cells per shard); each round expands, per instance, every open item
  * with f <= bound, where the window [min f, min f + window] moves when it is drained. */
 typedef struct gpq_astar_config {
-  uint32_t tile;              /* tile side, a power of two in [8, 256]; 0 = 64 */
+  uint32_t tile;              /* tile side, a power of two in [8, 128]; 0 = 64 */
   uint32_t window;            /* window width on f; 0 = 4 move costs */
   uint32_t inbox_capacity;    /* items one tile receives per round; 0 = 8 * tile */
   uint32_t open_capacity;     /* items one tile keeps above the window; 0 = tile * tile */
-  uint32_t frontier_capacity; /* shared-memory frontier items (two buffers); 0 = 2048 */
-  uint32_t block_threads;     /* 128 or 256; 0 = 256 */
+  uint32_t frontier_capacity; /* shared-memory frontier items (two buffers); 0 = 2048 (256 per warp) */
+  uint32_t block_threads;     /* 64, 128 or 256; 0 = 256 */
   uint32_t ctas_per_sm;       /* 0 = as many as fit */
   uint32_t max_rounds;        /* 0 = 2^20; reaching it is GPQ_ERR_TIMEOUT */
-  uint32_t reserved[4];
+  uint32_t tile_worker;       /* who processes one tile visit: 0 = a CTA, 1 = a warp */
+  uint32_t reserved[3];
 } gpq_astar_config;
 
 typedef struct gpq_astar_result {
@@ -257,16 +258,19 @@ GPQ_API gpq_status gpq_astar_create(const gpq_astar_config* cfg, gpq_astar** out
 GPQ_API gpq_status gpq_astar_destroy(gpq_astar* a);
 
 /* Solve n instances (HOST array of grids) in one persistent launch; results to a HOST
- * array of n.  Device buffers grow as needed and are kept for the next call.  An
- * instance whose tile buffers overflow reports GPQ_ERR_INSERT_FULL / GPQ_ERR_QUEUE_FULL
- * in its status (its other fields are then not meaningful).  Blocks on the stream. */
+ * array of n.  Device buffers grow as needed and are kept for the next call.  When an
+ * instance overflows its tile buffers the batch runs again with four times the inbox
+ * and open capacities (at most twice; the larger capacities stay); an instance that
+ * still overflows reports GPQ_ERR_INSERT_FULL / GPQ_ERR_QUEUE_FULL in its status (its
+ * other fields are then not meaningful).  Blocks on the stream. */
 GPQ_API gpq_status gpq_astar_solve(gpq_astar* a, const gpq_astar_grid* grids, uint32_t n,
                                    gpq_astar_result* results, void* stream);
 
 /* Device time of the last solve: the whole call (grid generation, search, results) and
- * the search launch alone; the number of rounds; the launch geometry. */
+ * the search launch alone; the number of rounds and of tile visits; the launch geometry.
+ * Any pointer may be NULL. */
 GPQ_API gpq_status gpq_astar_last_stats(gpq_astar* a, float* total_ms, float* search_ms, uint32_t* rounds,
-                                        uint32_t* grid, uint32_t* block);
+                                        uint64_t* tile_visits, uint32_t* grid, uint32_t* block);
 
 /* The canonical path of instance `index` of the last solve, goal first (HOST array). */
 GPQ_API gpq_status gpq_astar_path(gpq_astar* a, uint32_t index, uint32_t* cells, uint32_t capacity,

@@ -40,11 +40,14 @@ def _manhattan(w, hgt, goal):
     return np.abs(c % w - goal % w) + np.abs(c // w - goal // w)
 
 
-@pytest.mark.parametrize("tile", [8, 16, 32, 64, 128, 256])
-def test_tile_sizes(gpu_lib, tile):
+@pytest.mark.parametrize("worker", [0, 1])
+@pytest.mark.parametrize("tile", [8, 16, 32, 64, 128])
+def test_tile_sizes(gpu_lib, tile, worker):
+    if worker and tile == 128:
+        pytest.skip("a warp per 128 x 128 tile needs more shared memory than a CTA has")
     grids = np.concatenate([G.astar_grid(300, 200, 0.2, 5, conn=4, start=17, goal=300 * 200 - 40),
                             G.astar_grid(257, 129, 0.25, 6, conn=8, start=0, goal=257 * 129 - 1)])
-    with G.AStar(tile=tile) as a:
+    with G.AStar(tile=tile, tile_worker=worker, block_threads=128 if worker else 256) as a:
         _check(a.solve(grids), grids)
 
 
@@ -56,10 +59,11 @@ def test_window_widths(gpu_lib, window):
         _check(a.solve(grids), grids)
 
 
-def test_batched_queries(gpu_lib):
+@pytest.mark.parametrize("worker", [0, 1])
+def test_batched_queries(gpu_lib, worker):
     """The first 96 queries of the batched workload (8-connected 10/14, octile)."""
     grids = G.astar_queries(11, 96, 8, 64, 1024, 0.1, 0.3)
-    with G.AStar(tile=32) as a:
+    with G.AStar(tile=32, tile_worker=worker) as a:
         res = a.solve(grids)
         _check(res, grids)
         again = a.solve(grids)
@@ -85,9 +89,12 @@ def test_edge_grids(gpu_lib):
         G.astar_grid(16, 16, 0.6, 2),                         # dense
         G.astar_grid(65, 63, 0.3, 12, conn=8, start=64, goal=65 * 62),  # sides off the tile grid
     ])
+    for worker in (0, 1):
+        with G.AStar(tile=16, tile_worker=worker) as a:
+            res = a.solve(grids)
+            _check(res, grids)
     with G.AStar(tile=16) as a:
         res = a.solve(grids)
-        _check(res, grids)
         assert res[0]["cost"] == G.ASTAR_INF and res[0]["path_len"] == 0
         assert res[1]["cost"] == 0 and res[1]["expanded"] == 1 and res[1]["path_len"] == 1
 
@@ -99,8 +106,16 @@ def test_small_frontier_spills_stay_exact(gpu_lib):
 
 
 def test_overflow_is_reported(gpu_lib):
-    """Tile buffers too small for the search: the instance reports an error status."""
+    """Tile buffers far too small even after two fourfold retries: the instance reports an
+    error status instead of a wrong answer."""
     grids = G.astar_grid(256, 256, 0.1, 5, conn=8)
-    with G.AStar(tile=64, inbox_capacity=2, open_capacity=4) as a:
+    with G.AStar(tile=64, inbox_capacity=1, open_capacity=1) as a:
         res = a.solve(grids)
         assert res[0]["status"] in (3, 4)
+
+
+def test_overflow_retries_with_larger_buffers(gpu_lib):
+    """Small tile buffers: the batch reruns with larger ones and the results are exact."""
+    grids = G.astar_queries(11, 24, 8, 64, 1024, 0.1, 0.3)
+    with G.AStar(tile=32, window=400, inbox_capacity=16, open_capacity=64) as a:
+        _check(a.solve(grids), grids)
