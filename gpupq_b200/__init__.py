@@ -131,6 +131,16 @@ _SIGS = {
     "gpq_astar_gcost": ([_VP, ctypes.c_uint32, _VP, ctypes.c_uint64, _VP], ctypes.c_int),
     "gpq_astar_query": ([ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                          ctypes.c_double, ctypes.c_double, _VP], ctypes.c_int),
+    "gpq_astar_session_create": ([_VP, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(_VP)],
+                                 ctypes.c_int),
+    "gpq_astar_session_destroy": ([_VP], ctypes.c_int),
+    "gpq_astar_session_admit": ([_VP, _VP, ctypes.POINTER(ctypes.c_uint32)], ctypes.c_int),
+    "gpq_astar_session_step": ([_VP, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32), _VP], ctypes.c_int),
+    "gpq_astar_session_collect": ([_VP, _VP, _VP, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32), _VP],
+                                  ctypes.c_int),
+    "gpq_astar_session_usage": ([_VP, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
+                                 ctypes.POINTER(ctypes.c_uint32)], ctypes.c_int),
+    "gpq_astar_session_bytes": ([_VP, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32], ctypes.c_uint64),
 }
 
 
@@ -491,3 +501,56 @@ class AStar:
         out = np.zeros(cells, np.uint32)
         check(lib().gpq_astar_gcost(self._h, index, _ptr(out), cells, None), "gpq_astar_gcost")
         return out
+
+
+class AStarSession:
+    """Resident A* instances (gpq_astar_session_*): admit, step, collect."""
+
+    def __init__(self, max_cells, max_tiles, max_instances, **cfg):
+        c = AstarConfig()
+        for k, v in cfg.items():
+            setattr(c, k, v)
+        self._h = ctypes.c_void_p()
+        check(lib().gpq_astar_session_create(ctypes.byref(c), max_cells, max_tiles, max_instances,
+                                             ctypes.byref(self._h)), "gpq_astar_session_create")
+        self.max_instances = max_instances
+
+    def close(self):
+        if self._h:
+            lib().gpq_astar_session_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def admit(self, grid):
+        """Slot number, or None when the instance does not fit now."""
+        g = np.ascontiguousarray(np.atleast_1d(grid), ASTAR_GRID_DTYPE)
+        slot = ctypes.c_uint32()
+        st = lib().gpq_astar_session_admit(self._h, _ptr(g), ctypes.byref(slot))
+        if st == 6:
+            return None
+        check(st, "gpq_astar_session_admit")
+        return slot.value
+
+    def step(self, rounds=0):
+        n = ctypes.c_uint32()
+        check(lib().gpq_astar_session_step(self._h, rounds, ctypes.byref(n), None), "gpq_astar_session_step")
+        return n.value
+
+    def collect(self):
+        slots = np.zeros(self.max_instances, np.uint32)
+        res = np.zeros(self.max_instances, ASTAR_RESULT_DTYPE)
+        n = ctypes.c_uint32()
+        check(lib().gpq_astar_session_collect(self._h, _ptr(slots), _ptr(res), self.max_instances,
+                                              ctypes.byref(n), None), "gpq_astar_session_collect")
+        return slots[: n.value], res[: n.value]
+
+    def usage(self):
+        c, t, i = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint32()
+        check(lib().gpq_astar_session_usage(self._h, ctypes.byref(c), ctypes.byref(t), ctypes.byref(i)),
+              "gpq_astar_session_usage")
+        return c.value, t.value, i.value

@@ -61,7 +61,11 @@ gpq_status grow(T** p, uint64_t have, uint64_t need) {
 
 bool is_pow2(uint32_t x) { return x && !(x & (x - 1)); }
 
-gpq_status normalize(gpq_astar_config& c) {
+}  // namespace
+
+namespace gpq {
+
+gpq_status astar_normalize(gpq_astar_config& c) {
   if (c.tile == 0) c.tile = 64;
   GPQ_CHECK_ARG(is_pow2(c.tile) && c.tile >= 8 && c.tile <= 128, "tile must be a power of two in [8, 128]");
   if (c.inbox_capacity == 0) c.inbox_capacity = 8 * c.tile;
@@ -76,7 +80,7 @@ gpq_status normalize(gpq_astar_config& c) {
   return GPQ_OK;
 }
 
-}  // namespace
+}  // namespace gpq
 
 extern "C" {
 
@@ -85,7 +89,7 @@ gpq_status gpq_astar_create(const gpq_astar_config* cfg, gpq_astar** out) {
   *out = nullptr;
   gpq_astar_config c{};
   if (cfg) c = *cfg;
-  GPQ_TRY(normalize(c));
+  GPQ_TRY(gpq::astar_normalize(c));
   gpq_astar* a = new (std::nothrow) gpq_astar();
   if (!a) return GPQ_ERR_NOMEM;
   a->cfg = c;
@@ -246,17 +250,18 @@ static gpq_status astar_solve_pass(gpq_astar* a, const gpq_astar_grid* grids, ui
   const uint64_t words = cell0 / 32;
   astar_bitmap_kernel<<<(uint32_t)std::min<uint64_t>((words + 255) / 256, (uint64_t)sms * 64), 256, 0, st>>>(
       a->inst, n, a->word0, words, a->blk);
-  astar_tiles_init_kernel<<<(n + 127) / 128, 128, 0, st>>>(d);
-  astar_init_kernel<<<(n + 127) / 128, 128, 0, st>>>(d);
+  astar_tiles_init_kernel<<<std::min<uint32_t>(n, 4096), 128, 0, st>>>(d, nullptr, n);
+  astar_init_kernel<<<(n + 127) / 128, 128, 0, st>>>(d, nullptr, n, 0u);
   GPQ_CUDA_TRY(cudaGetLastError());
   GPQ_CUDA_TRY(cudaEventRecord(a->ev[1], st));
-  void* args[] = {&d};
+  uint32_t s0 = 0, step_rounds = 0;
+  void* args[] = {&d, &s0, &step_rounds};
   GPQ_CUDA_TRY(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(c.block_threads), args, smem, st));
   GPQ_CUDA_TRY(cudaEventRecord(a->ev[2], st));
   GPQ_CUDA_TRY(cudaMemsetAsync(a->fin, 0, 2ull * n * sizeof(unsigned long long), st));
   const uint32_t fx = (uint32_t)std::min<uint64_t>((max_cells + 255) / 256, 64);
-  astar_finalize_kernel<<<dim3(fx, n), 256, 0, st>>>(d, a->fin);
-  astar_path_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>(d, a->pout, 0xFFFFFFFFu, nullptr, 0);
+  astar_finalize_kernel<<<dim3(fx, n), 256, 0, st>>>(d, nullptr, a->fin);
+  astar_path_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>(d, nullptr, n, a->pout, 0xFFFFFFFFu, nullptr, 0);
   GPQ_CUDA_TRY(cudaGetLastError());
   GPQ_CUDA_TRY(cudaEventRecord(a->ev[3], st));
   std::vector<unsigned long long> fin(2ull * n), pout(3ull * n);
@@ -356,7 +361,8 @@ gpq_status gpq_astar_path(gpq_astar* a, uint32_t index, uint32_t* cells, uint32_
   d.gcost = a->gcost;
   d.blk = a->blk;
   d.n_inst = a->n_inst;
-  astar_path_kernel<<<(a->n_inst * 32 + 255) / 256, 256, 0, st>>>(d, a->pout, index, a->path_buf, capacity);
+  astar_path_kernel<<<(a->n_inst * 32 + 255) / 256, 256, 0, st>>>(d, nullptr, a->n_inst, a->pout, index, a->path_buf,
+                                                                   capacity);
   GPQ_CUDA_TRY(cudaGetLastError());
   unsigned long long po[3];
   GPQ_CUDA_TRY(cudaMemcpyAsync(po, a->pout + 3ull * index, sizeof(po), cudaMemcpyDeviceToHost, st));

@@ -32,6 +32,11 @@
 
 static constexpr uint32_t kAstarInf = GPQ_ASTAR_INF;
 
+namespace gpq {
+// Defaults and limits of the engine knobs (host side, astar.cu).
+gpq_status astar_normalize(gpq_astar_config& c);
+}  // namespace gpq
+
 struct AstarInstDev {
   gpq_astar_grid g;
   uint64_t cell0;      // first cell in the shared g array and bitmap (a multiple of 32)
@@ -497,7 +502,7 @@ __device__ void astar_process_tile(const AstarDev& d, uint32_t t, uint32_t s, As
 }
 
 // Phase W for one instance (one warp): a drained window moves on, or the instance ends.
-__device__ void astar_window_step(const AstarDev& d, uint32_t i, uint32_t npar) {
+static __device__ void astar_window_step(const AstarDev& d, uint32_t i, uint32_t npar) {
   AstarInstDev* Ip = d.inst + i;
   const uint32_t lane = threadIdx.x & 31u;
   if (ldcg_u32(&Ip->done)) return;
@@ -537,8 +542,10 @@ __host__ __device__ inline size_t astar_worker_smem_bytes(uint32_t ts, uint32_t 
   return (astar_smem_bytes(ts, frontier_cap) + 15u) & ~(size_t)15u;
 }
 
+// Rounds s0, s0 + 1, ... until every instance is done, or until `step_rounds` rounds ran
+// (0 = no limit): a resident session resumes at the next round in its next launch.
 template <bool WARP>
-static __global__ void __launch_bounds__(256) astar_persistent_kernel(AstarDev d) {
+static __global__ void __launch_bounds__(256) astar_persistent_kernel(AstarDev d, uint32_t s0, uint32_t step_rounds) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ AstarTileSmem sms[kAstarMaxWorkers];
   __shared__ uint32_t s_t;
@@ -557,7 +564,7 @@ static __global__ void __launch_bounds__(256) astar_persistent_kernel(AstarDev d
   unsigned long long bar_target = 0;
   const uint32_t warps_total = gridDim.x * (blockDim.x >> 5);
   const uint32_t gwarp = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  for (uint32_t s = 0;; ++s) {
+  for (uint32_t s = s0;; ++s) {
     const uint32_t par = s & 1u, npar = par ^ 1u;
     const uint32_t n = ldcg_u32(&d.ctl->al_cnt[par]);
     for (;;) {
@@ -590,6 +597,7 @@ static __global__ void __launch_bounds__(256) astar_persistent_kernel(AstarDev d
       if (blockIdx.x == 0 && threadIdx.x == 0) gpq_set_error(&d.ctl->err, GPQ_ERR_TIMEOUT);
       break;
     }
+    if (step_rounds && s + 1 - s0 >= step_rounds) break;
   }
 }
 
@@ -617,42 +625,67 @@ static __global__ void astar_bitmap_kernel(const AstarInstDev* inst, uint32_t n_
   }
 }
 
-// Initial state: g = inf everywhere (done by a memset), g[start] = 0, the start item in
-// the start tile's inbox, the start tiles on the round-0 active list.
-static __global__ void astar_init_kernel(AstarDev d) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= d.n_inst) return;
+// Initial state of instances list[0, n) (all instances when list == nullptr): g = inf
+// (done by a memset), g[start] = 0, the start item in the start tile's inbox of round
+// parity par, the start tile on that round's active list.
+static __global__ void astar_init_kernel(AstarDev d, const uint32_t* list, uint32_t n, uint32_t par) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const uint32_t i = list ? list[j] : j;
   AstarInstDev& I = d.inst[i];
   d.gcost[I.cell0 + I.g.start] = 0;
   const uint32_t t = astar_tile_of(d, I, I.g.start);
-  d.tiles[t].in_cnt[0] = 1;
-  d.inbox[(size_t)t * d.in_cap] = make_uint2(astar_pack((int)(I.g.start % I.g.width), (int)(I.g.start / I.g.width)), 0);
-  d.tiles[t].queued[0] = 1;
-  d.al[i] = t;
-  if (i == 0) d.ctl->al_cnt[0] = d.n_inst;
+  d.tiles[t].in_cnt[par] = 1;
+  d.inbox[((size_t)par * d.n_tiles + t) * d.in_cap] =
+      make_uint2(astar_pack((int)(I.g.start % I.g.width), (int)(I.g.start / I.g.width)), 0);
+  astar_activate(d, t, par, false);
 }
 
-static __global__ void astar_tiles_init_kernel(AstarDev d) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t nthreads = gridDim.x * blockDim.x;
-  for (uint32_t inst = i; inst < d.n_inst; inst += nthreads) {
+// Tile records of instances list[0, n) (all when list == nullptr): one block per instance.
+static __global__ void astar_tiles_init_kernel(AstarDev d, const uint32_t* list, uint32_t n) {
+  for (uint32_t j = blockIdx.x; j < n; j += gridDim.x) {
+    const uint32_t inst = list ? list[j] : j;
     const AstarInstDev& I = d.inst[inst];
-    for (uint32_t ty = 0; ty < I.tiles_y; ++ty)
-      for (uint32_t tx = 0; tx < I.tiles_x; ++tx) {
-        AstarTileDev T{};
-        T.inst = inst;
-        T.tx = tx;
-        T.ty = ty;
-        T.open_min = kAstarInf;
-        d.tiles[I.tile0 + ty * I.tiles_x + tx] = T;
-      }
+    const uint32_t nt = I.tiles_x * I.tiles_y;
+    for (uint32_t k = threadIdx.x; k < nt; k += blockDim.x) {
+      AstarTileDev T{};
+      T.inst = inst;
+      T.tx = k % I.tiles_x;
+      T.ty = k / I.tiles_x;
+      T.open_min = kAstarInf;
+      d.tiles[I.tile0 + k] = T;
+    }
   }
+}
+
+// Blocked bits of instances list[0, n): blockIdx.y = position in the list.  Instance
+// cell ranges start on 32-cell boundaries.
+static __global__ void astar_bitmap_list_kernel(const AstarInstDev* inst, const uint32_t* list, uint32_t* blk) {
+  const AstarInstDev& I = inst[list[blockIdx.y]];
+  const uint64_t cells = (uint64_t)I.g.width * I.g.height;
+  const uint64_t words = (cells + 31) / 32, w0 = I.cell0 / 32;
+  for (uint64_t wi = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; wi < words; wi += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t w = 0;
+    for (uint32_t b = 0; b < 32; ++b) {
+      const uint64_t c = wi * 32 + b;
+      if (c < cells && gpq_astar_blocked(&I.g, (uint32_t)c)) w |= 1u << b;
+    }
+    blk[w0 + wi] = w;
+  }
+}
+
+// Slots that are in use (on[slot] != 0) and whose search has ended, appended to out.
+static __global__ void astar_done_list_kernel(const AstarInstDev* inst, const uint8_t* on, uint32_t n_slots,
+                                              uint32_t* out, uint32_t* out_n) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_slots; i += gridDim.x * blockDim.x)
+    if (on[i] && inst[i].done) out[atomicAdd(out_n, 1u)] = i;
 }
 
 // Per-instance expanded set (g + h <= C*, or every reached cell when the goal is not
 // reachable): count and hash.  Block per (instance, chunk): blockIdx.y = instance.
-static __global__ void astar_finalize_kernel(AstarDev d, unsigned long long* out /* [n_inst][2] */) {
-  const uint32_t i = blockIdx.y;
+static __global__ void astar_finalize_kernel(AstarDev d, const uint32_t* list, unsigned long long* out /* [n][2] */) {
+  const uint32_t j = blockIdx.y;
+  const uint32_t i = list ? list[j] : j;
   const AstarInstDev& I = d.inst[i];
   const uint32_t cs = I.ub;
   const uint64_t cells = (uint64_t)I.g.width * I.g.height;
@@ -669,8 +702,8 @@ static __global__ void astar_finalize_kernel(AstarDev d, unsigned long long* out
   cnt = warp_sum_u64(cnt);
   hs = warp_sum_u64(hs);
   if ((threadIdx.x & 31u) == 0 && cnt) {
-    atomicAdd(&out[2 * i], cnt);
-    atomicAdd(&out[2 * i + 1], hs);
+    atomicAdd(&out[2 * j], cnt);
+    atomicAdd(&out[2 * j + 1], hs);
   }
 }
 
@@ -678,15 +711,16 @@ static __global__ void astar_finalize_kernel(AstarDev d, unsigned long long* out
 // smallest-id neighbour p with g[p] + c(p, cell) == g[cell] and g[p] + h(p) <= C*.
 // out[3 * i] = length, out[3 * i + 1] = hash, out[3 * i + 2] = 1 when the walk failed.
 // When path != nullptr the cells of instance `want` are written (goal first, <= cap).
-static __global__ void astar_path_kernel(AstarDev d, unsigned long long* out, uint32_t want, uint32_t* path,
-                                         uint32_t cap) {
-  const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+static __global__ void astar_path_kernel(AstarDev d, const uint32_t* list, uint32_t n, unsigned long long* out,
+                                         uint32_t want, uint32_t* path, uint32_t cap) {
+  const uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t lane = threadIdx.x & 31u;
-  if (i >= d.n_inst) return;
+  if (j >= n) return;
+  const uint32_t i = list ? list[j] : j;
   const AstarInstDev& I = d.inst[i];
   const uint32_t cs = I.ub;
   if (cs == kAstarInf) {
-    if (lane == 0) { out[3 * i] = 0; out[3 * i + 1] = 0; out[3 * i + 2] = 0; }
+    if (lane == 0) { out[3 * j] = 0; out[3 * j + 1] = 0; out[3 * j + 2] = 0; }
     return;
   }
   const uint32_t* G = d.gcost + I.cell0;
@@ -726,8 +760,8 @@ static __global__ void astar_path_kernel(AstarDev d, unsigned long long* out, ui
     cur = cand;
   }
   if (lane == 0) {
-    out[3 * i] = len;
-    out[3 * i + 1] = hs;
-    out[3 * i + 2] = fail;
+    out[3 * j] = len;
+    out[3 * j + 1] = hs;
+    out[3 * j + 2] = fail;
   }
 }

@@ -279,6 +279,41 @@ GPQ_API gpq_status gpq_astar_path(gpq_astar* a, uint32_t index, uint32_t* cells,
 /* The g values of instance `index` of the last solve (HOST array of width * height). */
 GPQ_API gpq_status gpq_astar_gcost(gpq_astar* a, uint32_t index, uint32_t* g, uint64_t capacity, void* stream);
 
+/* Resident A* instances for serving.  No counterpart in the reference, whose agents run
+ * to completion inside one a_star launch (src/a_star.cu:269-593).  A session reserves a
+ * cell space (max_cells: g values and blocked bits, 4.125 bytes a cell) and a tile space
+ * (max_tiles tile records with their inboxes and open arrays) once; admitted instances
+ * take free ranges of both, all running instances advance together, a bounded number of
+ * rounds per step (one persistent launch), and finished ones are collected and give
+ * their ranges back.  Between steps everything stays in device memory. */
+typedef struct gpq_astar_session gpq_astar_session;
+
+GPQ_API gpq_status gpq_astar_session_create(const gpq_astar_config* cfg, uint64_t max_cells, uint32_t max_tiles,
+                                            uint32_t max_instances, gpq_astar_session** out);
+GPQ_API gpq_status gpq_astar_session_destroy(gpq_astar_session* s);
+
+/* Admit one instance; *slot names it until it is collected.  GPQ_ERR_NOMEM (and nothing
+ * changes) when its cells or tiles do not fit in the free ranges now. */
+GPQ_API gpq_status gpq_astar_session_admit(gpq_astar_session* s, const gpq_astar_grid* grid, uint32_t* slot);
+
+/* Initialize the instances admitted since the last step, then advance every running
+ * instance by at most `rounds` rounds (0 = until all are done).  *running = instances
+ * admitted and not yet collected.  Blocks on the stream. */
+GPQ_API gpq_status gpq_astar_session_step(gpq_astar_session* s, uint32_t rounds, uint32_t* running, void* stream);
+
+/* Results of up to `capacity` finished instances (HOST arrays), which leave the session.
+ * *n = how many. */
+GPQ_API gpq_status gpq_astar_session_collect(gpq_astar_session* s, uint32_t* slots, gpq_astar_result* results,
+                                             uint32_t capacity, uint32_t* n, void* stream);
+
+/* Cells and tiles held by admitted instances, and their number. */
+GPQ_API gpq_status gpq_astar_session_usage(gpq_astar_session* s, uint64_t* cells_used, uint64_t* tiles_used,
+                                           uint32_t* instances);
+
+/* Device bytes a session of these sizes reserves. */
+GPQ_API uint64_t gpq_astar_session_bytes(const gpq_astar_config* cfg, uint64_t max_cells, uint32_t max_tiles,
+                                         uint32_t max_instances);
+
 /* Grid of query `index` of a batch: side log-uniform in [side_lo, side_hi], obstacle
  * density uniform in [dens_lo, dens_hi], start and goal distinct and uniform over the
  * free cells, all drawn from seed base_seed + index (host computation). */

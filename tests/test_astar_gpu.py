@@ -119,3 +119,33 @@ def test_overflow_retries_with_larger_buffers(gpu_lib):
     grids = G.astar_queries(11, 24, 8, 64, 1024, 0.1, 0.3)
     with G.AStar(tile=32, window=400, inbox_capacity=16, open_capacity=64) as a:
         _check(a.solve(grids), grids)
+
+
+@pytest.mark.parametrize("rounds", [1, 7, 0])
+def test_session_stream_matches_oracle(gpu_lib, rounds):
+    """Instances admitted while others run, into a session too small for all of them at
+    once (admissions are refused and ranges are reused): every result is exact."""
+    grids = G.astar_queries(11, 40, 8, 64, 400, 0.1, 0.3)
+    want = {i: O.astar({k: int(g[k]) for k in O.ASTAR_FIELDS}) for i, g in enumerate(grids)}
+    got, slot_of, pending = {}, {}, list(range(len(grids)))
+    refused = 0
+    with G.AStarSession(max_cells=400 * 400 * 3, max_tiles=400, max_instances=8, tile=32) as s:
+        for _ in range(100000):
+            while pending:
+                slot = s.admit(grids[pending[0]])
+                if slot is None:
+                    refused += 1
+                    break
+                slot_of[slot] = pending.pop(0)
+            s.step(rounds)
+            slots, res = s.collect()
+            for sl, r in zip(slots, res):
+                got[slot_of.pop(int(sl))] = r
+            if not pending and not slot_of:
+                break
+        assert s.usage() == (0, 0, 0)
+    assert refused > 0 and len(got) == len(grids)
+    for i, r in got.items():
+        assert r["status"] == 0
+        for k in FIELDS:
+            assert int(r[k]) == want[i][k], (i, k)
