@@ -141,6 +141,17 @@ _SIGS = {
     "gpq_astar_session_usage": ([_VP, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
                                  ctypes.POINTER(ctypes.c_uint32)], ctypes.c_int),
     "gpq_astar_session_bytes": ([_VP, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32], ctypes.c_uint64),
+    "gpq_phold_session_create": ([ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                  ctypes.c_uint32, ctypes.POINTER(_VP)], ctypes.c_int),
+    "gpq_phold_session_destroy": ([_VP], ctypes.c_int),
+    "gpq_phold_session_admit": ([_VP, ctypes.POINTER(PholdConfig), ctypes.POINTER(ctypes.c_uint32)], ctypes.c_int),
+    "gpq_phold_session_step": ([_VP, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32), _VP], ctypes.c_int),
+    "gpq_phold_session_collect": ([_VP, _VP, ctypes.POINTER(PholdResult), ctypes.c_uint32,
+                                   ctypes.POINTER(ctypes.c_uint32), _VP], ctypes.c_int),
+    "gpq_phold_session_usage": ([_VP, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint32)],
+                                ctypes.c_int),
+    "gpq_phold_session_bytes": ([ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32],
+                                ctypes.c_uint64),
 }
 
 
@@ -554,3 +565,50 @@ class AStarSession:
         check(lib().gpq_astar_session_usage(self._h, ctypes.byref(c), ctypes.byref(t), ctypes.byref(i)),
               "gpq_astar_session_usage")
         return c.value, t.value, i.value
+
+
+class PholdSession:
+    """Resident PHOLD runs (gpq_phold_session_*): admit, step, collect."""
+
+    def __init__(self, max_lps, max_instances, capacity=256, insert_capacity=64, lanes_per_lp=8):
+        self._h = ctypes.c_void_p()
+        check(lib().gpq_phold_session_create(max_lps, capacity, insert_capacity, max_instances, lanes_per_lp,
+                                             ctypes.byref(self._h)), "gpq_phold_session_create")
+        self.max_instances = max_instances
+
+    def close(self):
+        if self._h:
+            lib().gpq_phold_session_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def admit(self, cfg: PholdConfig):
+        slot = ctypes.c_uint32()
+        st = lib().gpq_phold_session_admit(self._h, ctypes.byref(cfg), ctypes.byref(slot))
+        if st == 6:
+            return None
+        check(st, "gpq_phold_session_admit")
+        return slot.value
+
+    def step(self, windows=0):
+        n = ctypes.c_uint32()
+        check(lib().gpq_phold_session_step(self._h, windows, ctypes.byref(n), None), "gpq_phold_session_step")
+        return n.value
+
+    def collect(self):
+        slots = np.zeros(self.max_instances, np.uint32)
+        res = (PholdResult * self.max_instances)()
+        n = ctypes.c_uint32()
+        check(lib().gpq_phold_session_collect(self._h, _ptr(slots), res, self.max_instances, ctypes.byref(n), None),
+              "gpq_phold_session_collect")
+        return [(int(slots[j]), res[j]) for j in range(n.value)]
+
+    def usage(self):
+        a, b = ctypes.c_uint64(), ctypes.c_uint32()
+        check(lib().gpq_phold_session_usage(self._h, ctypes.byref(a), ctypes.byref(b)), "gpq_phold_session_usage")
+        return a.value, b.value

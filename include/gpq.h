@@ -320,6 +320,38 @@ GPQ_API uint64_t gpq_astar_session_bytes(const gpq_astar_config* cfg, uint64_t m
 GPQ_API gpq_status gpq_astar_query(uint64_t base_seed, uint32_t index, uint32_t conn, uint32_t side_lo,
                                    uint32_t side_hi, double dens_lo, double dens_hi, gpq_astar_grid* out);
 
+/* Resident PHOLD instances: many runs of different sizes in one persistent launch
+ * (batched runs, and the PHOLD side of serving).  No counterpart in the reference, which
+ * runs one model per process (src/des.cu:74-214).  A session reserves an LP space of
+ * max_lps local array queues (capacity items each, insert_capacity children per window)
+ * once; an admitted run takes a free LP range, and all running instances advance
+ * together one window per grid barrier, each inside its own safe window
+ * [min_i, min_i + lookahead_i), so each run commits exactly what it commits alone (same
+ * committed count, steps, digest, pending events).  Finished runs are collected and give
+ * their LPs back. */
+typedef struct gpq_phold_session gpq_phold_session;
+
+GPQ_API gpq_status gpq_phold_session_create(uint32_t max_lps, uint32_t capacity, uint32_t insert_capacity,
+                                            uint32_t max_instances, uint32_t lanes_per_lp,
+                                            gpq_phold_session** out);
+GPQ_API gpq_status gpq_phold_session_destroy(gpq_phold_session* s);
+
+/* Admit one run (its queue_kind, capacity, insert_capacity and loop fields are ignored:
+ * the session's local array queues are used); GPQ_ERR_NOMEM when its LPs do not fit now. */
+GPQ_API gpq_status gpq_phold_session_admit(gpq_phold_session* s, const gpq_phold_config* cfg, uint32_t* slot);
+
+/* Populate the runs admitted since the last step, then advance every running instance by
+ * at most `windows` windows (0 = until all are done).  Blocks on the stream. */
+GPQ_API gpq_status gpq_phold_session_step(gpq_phold_session* s, uint32_t windows, uint32_t* running, void* stream);
+
+/* Results of up to `capacity` finished runs (HOST arrays; elapsed_ms is 0), which leave
+ * the session. */
+GPQ_API gpq_status gpq_phold_session_collect(gpq_phold_session* s, uint32_t* slots, gpq_phold_result* results,
+                                             uint32_t capacity, uint32_t* n, void* stream);
+GPQ_API gpq_status gpq_phold_session_usage(gpq_phold_session* s, uint64_t* lps_used, uint32_t* instances);
+GPQ_API uint64_t gpq_phold_session_bytes(uint32_t max_lps, uint32_t capacity, uint32_t insert_capacity,
+                                         uint32_t max_instances);
+
 /* Page-locked host memory for the end-to-end path (host <-> device copies). */
 GPQ_API gpq_status gpq_host_alloc(uint64_t bytes, void** out);
 GPQ_API gpq_status gpq_host_free(void* p);
