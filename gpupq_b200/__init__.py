@@ -612,3 +612,87 @@ class PholdSession:
         a, b = ctypes.c_uint64(), ctypes.c_uint32()
         check(lib().gpq_phold_session_usage(self._h, ctypes.byref(a), ctypes.byref(b)), "gpq_phold_session_usage")
         return a.value, b.value
+
+
+# ---- serving (gpq_serve_* in include/gpq.h) ----
+
+REQ_ASTAR, REQ_PHOLD = 0, 1
+SERVE_BATCHED, SERVE_PLAIN = 0, 1
+
+
+class AstarGridC(ctypes.Structure):
+    _fields_ = [("seed", ctypes.c_uint64)] + [(n, ctypes.c_uint32) for n in
+                                              ("width", "height", "block_thr", "conn", "start", "goal")]
+
+
+class AstarResultC(ctypes.Structure):
+    _fields_ = [("cost", ctypes.c_uint32), ("path_len", ctypes.c_uint32), ("expanded", ctypes.c_uint64),
+                ("gsum", ctypes.c_uint64), ("path_hash", ctypes.c_uint64), ("pops", ctypes.c_uint64),
+                ("windows", ctypes.c_uint32), ("status", ctypes.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class ServeRequest(ctypes.Structure):
+    _fields_ = [("arrival", ctypes.c_double), ("kind", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("astar", AstarGridC), ("phold", PholdConfig)]
+
+
+class ServeResponse(ctypes.Structure):
+    _fields_ = [("admitted", ctypes.c_double), ("finished", ctypes.c_double), ("status", ctypes.c_int32),
+                ("reserved", ctypes.c_uint32), ("astar", AstarResultC), ("phold", PholdResult)]
+
+
+class ServeConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget", ctypes.c_uint64), ("mode", ctypes.c_uint32), ("realtime", ctypes.c_uint32),
+                ("astar_rounds", ctypes.c_uint32), ("phold_windows", ctypes.c_uint32),
+                ("astar_share", ctypes.c_double), ("astar", AstarConfig), ("phold_capacity", ctypes.c_uint32),
+                ("phold_insert_capacity", ctypes.c_uint32), ("phold_lanes_per_lp", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32 * 5)]
+
+
+class ServeStats(ctypes.Structure):
+    _fields_ = [("makespan", ctypes.c_double), ("throughput", ctypes.c_double), ("p50", ctypes.c_double),
+                ("p99", ctypes.c_double), ("p999", ctypes.c_double), ("steps", ctypes.c_uint64),
+                ("max_resident", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+_SIGS.update({
+    "gpq_serve_run": ([ctypes.POINTER(ServeConfig), _VP, ctypes.c_uint32, _VP, ctypes.POINTER(ServeStats)],
+                      ctypes.c_int),
+    "gpq_serve_stream": ([ctypes.c_uint64, ctypes.c_double, ctypes.c_double, ctypes.c_double, _VP,
+                          ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)], ctypes.c_int),
+})
+
+
+def serve_stream(seed, rate, duration, astar_fraction=0.8):
+    """The mixed request stream (gpq_serve_stream) as a ctypes array."""
+    n = ctypes.c_uint32()
+    check(lib().gpq_serve_stream(seed, rate, duration, astar_fraction, None, 0, ctypes.byref(n)), "gpq_serve_stream")
+    reqs = (ServeRequest * max(n.value, 1))()
+    check(lib().gpq_serve_stream(seed, rate, duration, astar_fraction, ctypes.cast(reqs, ctypes.c_void_p), n.value,
+                                 ctypes.byref(n)), "gpq_serve_stream")
+    return reqs, n.value
+
+
+def serve(reqs, n, mode=SERVE_BATCHED, budget=0, realtime=True, astar_rounds=0, phold_windows=0, astar_share=0.0,
+          **astar_cfg):
+    """Run gpq_serve_run; returns (responses, stats dict)."""
+    c = ServeConfig()
+    c.hbm_budget = budget
+    c.astar_share = astar_share
+    c.mode = mode
+    c.realtime = 1 if realtime else 0
+    c.astar_rounds = astar_rounds
+    c.phold_windows = phold_windows
+    for k, v in astar_cfg.items():
+        setattr(c.astar, k, v)
+    out = (ServeResponse * max(n, 1))()
+    st = ServeStats()
+    check(lib().gpq_serve_run(ctypes.byref(c), ctypes.cast(reqs, ctypes.c_void_p), n,
+                              ctypes.cast(out, ctypes.c_void_p), ctypes.byref(st)), "gpq_serve_run")
+    return out, st.as_dict()

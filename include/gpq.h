@@ -352,6 +352,73 @@ GPQ_API gpq_status gpq_phold_session_usage(gpq_phold_session* s, uint64_t* lps_u
 GPQ_API uint64_t gpq_phold_session_bytes(uint32_t max_lps, uint32_t capacity, uint32_t insert_capacity,
                                          uint32_t max_instances);
 
+/* ---------------------------------------------------------------------------------- */
+/* 2c. Serving: a stream of A* queries and PHOLD runs                                  */
+/* ---------------------------------------------------------------------------------- */
+
+#define GPQ_REQ_ASTAR 0u
+#define GPQ_REQ_PHOLD 1u
+#define GPQ_SERVE_BATCHED 0u /* continuous batching over the resident sessions */
+#define GPQ_SERVE_PLAIN 1u   /* one request per launch, in arrival order */
+
+typedef struct gpq_serve_request {
+  double arrival;  /* seconds after the stream starts */
+  uint32_t kind;   /* GPQ_REQ_ASTAR or GPQ_REQ_PHOLD */
+  uint32_t reserved;
+  gpq_astar_grid astar;
+  gpq_phold_config phold;
+} gpq_serve_request;
+
+typedef struct gpq_serve_response {
+  double admitted; /* seconds after the start when the request got its resources */
+  double finished; /* seconds after the start when its result was on the host */
+  int32_t status;  /* gpq_status of the request */
+  uint32_t reserved;
+  gpq_astar_result astar;
+  gpq_phold_result phold; /* elapsed_ms is 0 in batched mode */
+} gpq_serve_response;
+
+typedef struct gpq_serve_config {
+  uint64_t hbm_budget;            /* device bytes for resident request state; 0 = 120 GiB */
+  uint32_t mode;                  /* GPQ_SERVE_BATCHED or GPQ_SERVE_PLAIN */
+  uint32_t realtime;              /* 1: admit no request before its arrival (host clock);
+                                     0: every request has arrived at the start */
+  uint32_t astar_rounds;          /* A* rounds per step; 0 = 32 */
+  uint32_t phold_windows;         /* PHOLD windows per step; 0 = 32 */
+  double astar_share;             /* part of the budget for A* state; 0 = 0.75 */
+  gpq_astar_config astar;
+  uint32_t phold_capacity;        /* per-LP queue capacity; 0 = 256 */
+  uint32_t phold_insert_capacity; /* per-LP children per window; 0 = 64 */
+  uint32_t phold_lanes_per_lp;    /* 0 = 8 */
+  uint32_t reserved[5];
+} gpq_serve_config;
+
+typedef struct gpq_serve_stats {
+  double makespan;   /* seconds from the start to the last result */
+  double throughput; /* requests per second of makespan */
+  double p50, p99, p999; /* latency (finished - arrival) percentiles in seconds */
+  uint64_t steps;    /* engine steps (batched) or launches (plain) */
+  uint32_t max_resident;
+  uint32_t reserved;
+} gpq_serve_stats;
+
+/* Serve n requests (HOST arrays).  Batched: requests are admitted in arrival order as
+ * long as their state fits the budget (A* cells and tiles, PHOLD LPs), stay resident,
+ * and advance together step by step; each result equals the request's result alone.
+ * Plain: each request runs alone with its own launch (gpq_astar_solve, gpq_phold_run),
+ * one after another.  A request that can never fit reports GPQ_ERR_NOMEM. */
+GPQ_API gpq_status gpq_serve_run(const gpq_serve_config* cfg, const gpq_serve_request* reqs, uint32_t n,
+                                 gpq_serve_response* out, gpq_serve_stats* stats);
+
+/* The mixed request stream: Poisson arrivals at `rate` per second for `duration`
+ * seconds; a request is an A* query with probability astar_fraction (4-connected, unit
+ * costs, side log-uniform in [128, 4096], obstacle density 0.2, gpq_astar_query with
+ * base seed `seed`), else a PHOLD run (LPs log-uniform in [256, 65536], 32 events per
+ * LP, lookahead 0.5, end time 200, uniform destinations, seed + index).  Writes up to
+ * `capacity` requests; with out == NULL only counts them. */
+GPQ_API gpq_status gpq_serve_stream(uint64_t seed, double rate, double duration, double astar_fraction,
+                                    gpq_serve_request* out, uint32_t capacity, uint32_t* n);
+
 /* Page-locked host memory for the end-to-end path (host <-> device copies). */
 GPQ_API gpq_status gpq_host_alloc(uint64_t bytes, void** out);
 GPQ_API gpq_status gpq_host_free(void* p);
