@@ -151,6 +151,143 @@ def run_reference(args):
     return 0
 
 
+# ---- the other forms of the hot path (rank 0, one GPU) ----
+
+ASTAR_BYTES_PER_EXPANSION = {4: 17 + 5 * 4 + 20, 8: 17 + 5 * 8 + 20}  # pop + closed mark + neighbours + push
+
+
+def _timed(fn, warmup, steps):
+    for _ in range(warmup):
+        fn()
+    t0 = time.perf_counter()
+    out = [fn() for _ in range(steps)]
+    return out, time.perf_counter() - t0
+
+
+def bench_astar_plain(G, O, args, peak):
+    """One 2048 x 2048 grid (Bernoulli(0.2), seed 3, corner to corner, 4-connected, 1024
+    shards of 64 x 64): expansions (cells with f <= C*) per second of device time."""
+    g = G.astar_grid(2048, 2048, 0.2, 3)
+    with G.AStar(tile=32) as a:
+        def step():
+            r = a.solve(g)
+            return r[0], a.stats()
+        out, wall = _timed(step, args.warmup, args.steps)
+    exp = int(out[0][0]["expanded"])
+    dev_s = sum(st["total_ms"] for _, st in out) / 1e3
+    want = O.astar({k: int(g[0][k]) for k in O.ASTAR_FIELDS})
+    exact = all(int(r[k]) == want[k] for r, _ in out for k in ("cost", "expanded", "gsum", "path_len", "path_hash"))
+    achieved = exp * ASTAR_BYTES_PER_EXPANSION[4] * args.steps / dev_s / 1e9
+    return {"workload": "astar_plain_2048x2048_p0.2_4conn_1024shards", "metric": "A* expansions/s",
+            "value": exp * args.steps / dev_s, "unit": "expansions/s", "cost": int(out[0][0]["cost"]),
+            "expanded": exp, "ms_per_query": 1e3 * dev_s / args.steps, "exact_vs_oracle": exact,
+            "e2e": {"value": exp * args.steps / wall, "unit": "expansions/s", "h2d_bytes_per_step": 32,
+                    "d2h_bytes_per_step": 48},
+            "roofline": {"bound": "latency (critical path of ~4100 dependent expansions)", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak},
+            "cpu_baseline": {"value": want["expanded"] / want["seconds"], "unit": "expansions/s", "cores": 1,
+                             "kind": "port", "sample": "the whole query, sequential std::priority_queue A*"}}
+
+
+def bench_astar_batched(G, O, args, peak):
+    """10,000 queries in one persistent launch: side log-uniform in [64, 1024], density
+    uniform in [0.1, 0.3], 8-connected 10/14, octile, seeds 11 + i."""
+    q = G.astar_queries(11, 10000, 8, 64, 1024, 0.1, 0.3)
+    with G.AStar(tile=64, window=100) as a:
+        def step():
+            r = a.solve(q)
+            return r, a.stats()
+        out, wall = _timed(step, args.warmup, args.steps)
+        exp = int(out[0][0]["expanded"].sum())
+        dev_s = sum(st["total_ms"] for _, st in out) / 1e3
+        # the plain form: one launch per query, on the first 200
+        pe, pt = 0, 0.0
+        for i in range(200):
+            r = a.solve(q[i:i + 1])
+            pe += int(r[0]["expanded"])
+            pt += a.stats()["total_ms"] / 1e3
+    sample = [{k: int(q[i][k]) for k in O.ASTAR_FIELDS} for i in range(300)]
+    threads = os.cpu_count() or 1
+    sec, res = O.astar_batch(sample, threads)
+    exact = all(int(out[0][0][i][k]) == res[i][k] for i in range(300)
+                for k in ("cost", "expanded", "gsum", "path_len", "path_hash"))
+    achieved = exp * ASTAR_BYTES_PER_EXPANSION[8] * args.steps / dev_s / 1e9
+    return {"workload": "astar_batched_10000q_side64-1024_8conn", "metric": "A* expansions/s (batched)",
+            "value": exp * args.steps / dev_s, "unit": "expansions/s", "queries": len(q),
+            "ms_per_batch": 1e3 * dev_s / args.steps, "bad_status": int((out[0][0]["status"] != 0).sum()),
+            "plain_value": pe / pt, "plain_sample": "first 200 queries, one launch each",
+            "batched_over_plain": (exp * args.steps / dev_s) / (pe / pt), "exact_vs_oracle_first_300": exact,
+            "e2e": {"value": exp * args.steps / wall, "unit": "expansions/s",
+                    "h2d_bytes_per_step": int(q.nbytes), "d2h_bytes_per_step": int(len(q) * 48)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak},
+            "cpu_baseline": {"value": sum(r["expanded"] for r in res) / sec, "unit": "expansions/s", "cores": threads,
+                             "kind": "port", "sample": "first 300 queries, one sequential A* per host thread"}}
+
+
+def bench_phold_batched(G, O, args, peak):
+    """The PHOLD runs of the first second of the served stream (LPs log-uniform in
+    [256, 65536], 32 events per LP, lookahead 0.5, end time 200), all in one launch."""
+    reqs, n = G.serve_stream(99, 2000.0, 1.0)
+    runs = [reqs[i].phold for i in range(n) if reqs[i].kind == G.REQ_PHOLD]
+    lps = sum(r.num_lps for r in runs)
+    with G.PholdSession(max_lps=lps, max_instances=len(runs)) as s:
+        def step():
+            for r in runs:
+                s.admit(r)
+            t0 = time.perf_counter()
+            s.step(0)
+            got = s.collect()
+            return got, time.perf_counter() - t0
+        out, _ = _timed(step, args.warmup, args.steps)
+    ev = sum(r.committed for _, r in out[0][0])
+    dt = sum(t for _, t in out)
+    pe, pt = 0, 0.0
+    for r in runs[:16]:
+        c = G.make_phold_config(r.num_lps, 32, 0.5, 200.0, r.seed)
+        with G.Phold(c) as h:
+            h.populate()
+            h.run()
+            rr = h.result()
+            pe += rr["committed"]
+            pt += rr["elapsed_ms"] / 1e3
+    achieved = ev * BYTES_PER_EVENT * args.steps / dt / 1e9
+    return {"workload": f"phold_batched_{len(runs)}runs_lp256-65536_x32_T200", "metric": "PHOLD events/s (batched)",
+            "value": ev * args.steps / dt, "unit": "events/s", "runs": len(runs), "lps": lps,
+            "ms_per_batch": 1e3 * dt / args.steps, "plain_value": pe / pt,
+            "plain_sample": "first 16 runs, one persistent launch each (device time)",
+            "batched_over_plain": (ev * args.steps / dt) / (pe / pt),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak},
+            "timing": "host wall clock around the session step (populate, all windows, collect)"}
+
+
+def bench_served(G, args, duration):
+    """The mixed stream: Poisson 2000/s, 80% A* (4-connected, side log-uniform in [128,
+    4096], p 0.2), 20% PHOLD (LPs log-uniform in [256, 65536], 32 ev/LP, T 200), a 120 GiB
+    budget; continuous batching vs one request per launch."""
+    reqs, n = G.serve_stream(99, 2000.0, duration)
+    out, st = G.serve(reqs, n, mode=G.SERVE_BATCHED, realtime=True, budget=120 << 30, tile=64)
+    bad = sum(1 for i in range(n) if out[i].status != 0)
+    m = min(n, 150)
+    pout, pst = G.serve(reqs, m, mode=G.SERVE_PLAIN, realtime=True, tile=64)
+    bout, bst = G.serve(reqs, m, mode=G.SERVE_BATCHED, realtime=True, budget=120 << 30, tile=64)
+    exact = True
+    for i in range(m):
+        if reqs[i].kind == G.REQ_ASTAR:
+            exact &= all(getattr(bout[i].astar, k) == getattr(pout[i].astar, k)
+                         for k in ("cost", "path_len", "expanded", "gsum", "path_hash"))
+        else:
+            exact &= all(getattr(bout[i].phold, k) == getattr(pout[i].phold, k)
+                         for k in ("committed", "steps", "pending", "pending_csum", "digest"))
+    r = lambda d: {k: (round(v, 6) if isinstance(v, float) else v) for k, v in d.items()}
+    return {"workload": f"served_poisson2000_{duration:g}s_80astar_20phold", "metric": "served queries/s",
+            "value": st["throughput"], "unit": "queries/s", "requests": n, "bad_status": bad,
+            "offered_rate": 2000.0, "batched": r(st),
+            "prefix": {"requests": m, "batched": r(bst), "plain": r(pst),
+                       "batched_over_plain_throughput": bst["throughput"] / pst["throughput"],
+                       "exact_mix_equals_alone": exact},
+            "latency_unit": "s (finished - arrival, host clock)"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -165,6 +302,8 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (library defaults)")
     ap.add_argument("--retune", action="store_true", help="ignore the autotuner cache")
     ap.add_argument("--tune-windows", type=int, default=200)
+    ap.add_argument("--no-forms", action="store_true", help="skip the A*, batched and served sections")
+    ap.add_argument("--served-seconds", type=float, default=1.0, help="length of the served request stream")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -310,6 +449,14 @@ def main():
                          f"std::priority_queue port of the reference loop on {threads} threads"}
 
     h.close()
+    forms = None
+    if rank == 0 and not args.no_forms:
+        from oracle import oracle as O
+        peak, _ = load_peaks()
+        forms = {"astar_plain": bench_astar_plain(G, O, args, peak),
+                 "astar_batched": bench_astar_batched(G, O, args, peak),
+                 "phold_batched": bench_phold_batched(G, O, args, peak),
+                 "served": bench_served(G, args, args.served_seconds)}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
@@ -330,6 +477,7 @@ def main():
             "gpu_launches": int(args.steps * info["launches_per_run"]),
             "clocks": clocks,
             "wall_s_timed": t_wall,
+            "forms": forms,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:
