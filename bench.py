@@ -288,6 +288,36 @@ def bench_served(G, args, duration):
             "latency_unit": "s (finished - arrival, host clock)"}
 
 
+def run_case(name):
+    """Small named workloads for profiling captures (each runs its kernel twice)."""
+    import gpupq_b200 as G
+    if name == "astar_batched_1000":
+        q = G.astar_queries(11, 1000, 8, 64, 1024, 0.1, 0.3)
+        with G.AStar(tile=64, window=100) as a:
+            for _ in range(2):
+                r = a.solve(q)
+            print(a.stats(), int(r["expanded"].sum()), int(r["pops"].sum()), int((r["status"] != 0).sum()))
+    elif name == "astar_plain_2048":
+        g = G.astar_grid(2048, 2048, 0.2, 3)
+        with G.AStar(tile=32) as a:
+            for _ in range(2):
+                r = a.solve(g)
+            print(a.stats(), int(r[0]["expanded"]))
+    elif name == "phold_batched_36":
+        reqs, n = G.serve_stream(99, 2000.0, 0.1)
+        runs = [reqs[i].phold for i in range(n) if reqs[i].kind == G.REQ_PHOLD][:40]
+        with G.PholdSession(max_lps=sum(r.num_lps for r in runs), max_instances=len(runs)) as s:
+            for _ in range(2):
+                for r in runs:
+                    s.admit(r)
+                s.step(0)
+                got = s.collect()
+            print(len(got), sum(r.committed for _, r in got))
+    else:
+        raise SystemExit(f"unknown case {name}")
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -304,7 +334,11 @@ def main():
     ap.add_argument("--tune-windows", type=int, default=200)
     ap.add_argument("--no-forms", action="store_true", help="skip the A*, batched and served sections")
     ap.add_argument("--served-seconds", type=float, default=1.0, help="length of the served request stream")
+    ap.add_argument("--case", default=None, choices=["astar_batched_1000", "astar_plain_2048", "phold_batched_36"],
+                    help="run one small named workload twice and exit (profiling captures)")
     args = ap.parse_args()
+    if args.case:
+        return run_case(args.case)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
