@@ -74,6 +74,8 @@ __global__ void laq_take_kernel(LaqDev q, uint32_t L, const uint32_t* cnt, const
   }
 }
 
+__global__ void laq_set_bound_kernel(float* bound, float value) { *bound = value; }
+
 __global__ void laq_clear_kernel(LaqDev q, uint32_t lp, LocalQueueCounters* ctr) {
   const uint32_t n = q.wr[lp] - q.rd[lp];
   q.rd[lp] = q.wr[lp];
@@ -83,8 +85,31 @@ __global__ void laq_clear_kernel(LaqDev q, uint32_t lp, LocalQueueCounters* ctr)
 class LaqQueue final : public LocalQueueBase {
  public:
   ~LaqQueue() override {
-    for (void* p : {(void*)ring_, (void*)rd_, (void*)wr_})
+    for (void* p : {(void*)ring_, (void*)rd_, (void*)wr_, (void*)bound_})
       if (p) cudaFree(p);
+  }
+
+  gpq_status device_view(gpq_device_queue* v) override {
+    v->ring = ring_;
+    v->rd = rd_;
+    v->wr = wr_;
+    v->ibuf = ibuf_;
+    v->icnt = icnt_;
+    v->bound = bound_;
+    v->enqueued = &ctr_->enqueued;
+    v->dequeued = &ctr_->dequeued;
+    v->err = &ctr_->err;
+    v->num_lps = L_;
+    v->cap_log2 = cap_log2_;
+    v->ibc = ibc_;
+    v->reserved = 0;
+    return GPQ_OK;
+  }
+
+  gpq_status set_bound(float b, cudaStream_t st) override {
+    laq_set_bound_kernel<<<1, 1, 0, st>>>(bound_, b);
+    GPQ_CUDA_TRY(cudaGetLastError());
+    return GPQ_OK;
   }
 
   gpq_status init(const gpq_queue_config& c) {
@@ -101,6 +126,8 @@ class LaqQueue final : public LocalQueueBase {
     GPQ_CUDA_TRY(cudaMalloc(&wr_, (size_t)L_ * sizeof(uint32_t)));
     GPQ_CUDA_TRY(cudaMemsetAsync(rd_, 0, (size_t)L_ * sizeof(uint32_t), own_));
     GPQ_CUDA_TRY(cudaMemsetAsync(wr_, 0, (size_t)L_ * sizeof(uint32_t), own_));
+    GPQ_CUDA_TRY(cudaMalloc(&bound_, sizeof(float)));
+    laq_set_bound_kernel<<<1, 1, 0, own_>>>(bound_, gpq_u2f(kInfBits));
     const size_t smem = 8 * laq_group_smem_bytes(ibc_, 32);
     GPQ_CUDA_TRY(cudaFuncSetAttribute(laq_post_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     GPQ_CUDA_TRY(cudaStreamSynchronize(own_));
@@ -193,6 +220,7 @@ class LaqQueue final : public LocalQueueBase {
 
  private:
   gpq_item* ring_ = nullptr;
+  float* bound_ = nullptr;  // window bound read by queue_peek on the device
   uint32_t* rd_ = nullptr;
   uint32_t* wr_ = nullptr;
   uint32_t cap_log2_ = 0;

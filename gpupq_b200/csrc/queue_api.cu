@@ -87,4 +87,18 @@ gpq_status gpq_queue_counts(gpq_queue* q, uint64_t* enqueued, uint64_t* dequeued
   return q->impl->counts(enqueued, dequeued, gpq::as_stream(stream, q->impl->stream()));
 }
 
+gpq_status gpq_queue_device_view(gpq_queue* q, gpq_device_queue* out) {
+  GPQ_CHECK_ARG(q && out, "NULL argument");
+  const gpq_status s = q->impl->device_view(out);
+  if (s == GPQ_ERR_UNSUPPORTED) gpq::set_last_error("device-side access is available for the local array queue only");
+  return s;
+}
+
+gpq_status gpq_queue_set_bound(gpq_queue* q, float bound, void* stream) {
+  GPQ_CHECK_ARG(q, "NULL argument");
+  const gpq_status s = q->impl->set_bound(bound, gpq::as_stream(stream, q->impl->stream()));
+  if (s == GPQ_ERR_UNSUPPORTED) gpq::set_last_error("device-side access is available for the local array queue only");
+  return s;
+}
+
 }  // extern "C"

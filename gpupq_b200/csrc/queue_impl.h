@@ -26,6 +26,9 @@ class QueueImpl {
   virtual gpq_status clear(uint32_t lp, cudaStream_t st) = 0;
   virtual gpq_status dump(uint32_t lp, gpq_item* out, uint64_t out_capacity, uint64_t* n_out, cudaStream_t st) = 0;
   virtual gpq_status counts(uint64_t* enqueued, uint64_t* dequeued, cudaStream_t st) = 0;
+  // Device-side access for model kernels (include/gpq/queue.cuh); local array queue only.
+  virtual gpq_status device_view(gpq_device_queue*) { return GPQ_ERR_UNSUPPORTED; }
+  virtual gpq_status set_bound(float, cudaStream_t) { return GPQ_ERR_UNSUPPORTED; }
 };
 
 gpq_status make_laq_queue(const gpq_queue_config& cfg, std::unique_ptr<QueueImpl>& out);

@@ -1,0 +1,112 @@
+/*
+ * gpq/queue.cuh -- the reference's device queue functions for model kernels, over a
+ * gpupq_b200 local array queue.
+ *
+ * The reference binds queue_insert / queue_peek / queue_set_done / queue_is_empty /
+ * queue_length / queue_clear / queue_insert_or_update to one queue implementation by
+ * macro (src/queue.cuh:7-70) and model kernels call them per LP (PHOLD:
+ * src/phold.cu:81-117).  Including this header in a CUDA translation unit gives those
+ * names as inline __device__ functions over the device view of a gpq_queue (local array
+ * queue), so a handler written like the reference's compiles against the library:
+ *
+ *     gpq_item* ev = NULL;
+ *     int index = queue_peek(&ev, lp);          // head of lp's run if ts < the window bound
+ *     if (index != -1) {
+ *       gpq_item child = ...;                  // the model's event function
+ *       queue_set_done(index);
+ *       bool ok = queue_insert(child);         // visible after the next gpq_queue_post
+ *     }
+ *
+ * The host binds a queue once (gpq_queue_bind, below: it copies the view into this
+ * translation unit's __device__ variable), then per step sets the window
+ * (gpq_queue_set_bound), launches the model kernel, and merges the inserted items
+ * (gpq_queue_post) -- the reference's des_run loop (src/des.cu:154-214).
+ *
+ * Differences from the reference: items are gpq_item (the reference's `event.node` is
+ * `lp`); queue_insert reports a full insert buffer by returning false and by the error
+ * word that the next gpq_queue_post returns, instead of an assert; queue_insert_or_update
+ * inserts (the reference's default build, without LOCAL_ARRAY_QUEUE_UPDATE_ELEMENTS).
+ */
+#ifndef GPQ_QUEUE_CUH
+#define GPQ_QUEUE_CUH
+
+#include <cuda_runtime.h>
+
+#include "gpq.h"
+
+typedef gpq_item queue_item;
+
+/* The queue the device functions of this translation unit work on. */
+static __device__ gpq_device_queue gpq_bound_queue;
+
+/* Bind q for the device functions of this translation unit (host; blocks on nothing but
+ * the symbol copy). */
+static inline gpq_status gpq_queue_bind(gpq_queue* q) {
+  gpq_device_queue v;
+  const gpq_status s = gpq_queue_device_view(q, &v);
+  if (s != GPQ_OK) return s;
+  return cudaMemcpyToSymbol(gpq_bound_queue, &v, sizeof(v)) == cudaSuccess ? GPQ_OK : GPQ_ERR_CUDA;
+}
+
+/* queue_insert (src/queue.cuh:46-47): reserve a slot in the item's LP buffer. */
+static __device__ __forceinline__ bool queue_insert(queue_item item) {
+  const gpq_device_queue& q = gpq_bound_queue;
+  const uint32_t pos = atomicAdd(&q.icnt[item.lp], 1u);
+  if (pos >= q.ibc) {
+    atomicCAS(q.err, 0u, (uint32_t)GPQ_ERR_INSERT_FULL);
+    return false;
+  }
+  q.ibuf[(size_t)item.lp * q.ibc + pos] = item;
+  atomicAdd(q.enqueued, 1ull);
+  return true;
+}
+
+/* queue_peek (src/queue.cuh:49-51): the index of lp's earliest item if it lies inside
+ * the window (ts < bound), else -1; *item points at it until queue_set_done/post. */
+static __device__ __forceinline__ int queue_peek(queue_item** item, int lp) {
+  const gpq_device_queue& q = gpq_bound_queue;
+  const uint32_t rd = q.rd[lp];
+  if (rd == q.wr[lp]) return -1;
+  const uint32_t slot = rd & ((1u << q.cap_log2) - 1u);
+  queue_item* it = q.ring + ((size_t)lp << q.cap_log2) + slot;
+  if (!(it->ts < *q.bound)) return -1;
+  *item = it;
+  return (int)(((uint32_t)lp << q.cap_log2) | slot);
+}
+
+/* queue_set_done (src/queue.cuh:53-54): the peeked item leaves lp's run. */
+static __device__ __forceinline__ void queue_set_done(int index) {
+  const gpq_device_queue& q = gpq_bound_queue;
+  const uint32_t lp = (uint32_t)index >> q.cap_log2;
+  q.rd[lp] += 1u;
+  atomicAdd(q.dequeued, 1ull);
+}
+
+/* queue_is_empty (src/queue.cuh:59-60): nothing queued and nothing inserted since the
+ * last post (src/local_array_queue.cu:807-810). */
+static __device__ __forceinline__ bool queue_is_empty(int lp) {
+  const gpq_device_queue& q = gpq_bound_queue;
+  return q.rd[lp] == q.wr[lp] && q.icnt[lp] == 0u;
+}
+
+/* queue_length (src/queue.cuh:62-63): items in lp's run. */
+static __device__ __forceinline__ int queue_length(int lp) {
+  const gpq_device_queue& q = gpq_bound_queue;
+  return (int)(q.wr[lp] - q.rd[lp]);
+}
+
+/* queue_clear (src/queue.cuh:65-66): drop lp's run. */
+static __device__ __forceinline__ void queue_clear(int lp) {
+  const gpq_device_queue& q = gpq_bound_queue;
+  const uint32_t n = q.wr[lp] - q.rd[lp];
+  q.rd[lp] = q.wr[lp];
+  atomicAdd(q.dequeued, (unsigned long long)n);
+}
+
+/* queue_insert_or_update (src/queue.cuh:68-69). */
+static __device__ __forceinline__ void queue_insert_or_update(queue_item item, int lp) {
+  item.lp = (uint32_t)lp;
+  queue_insert(item);
+}
+
+#endif /* GPQ_QUEUE_CUH */
