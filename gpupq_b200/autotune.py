@@ -16,6 +16,9 @@ from . import GpqError, Phold, make_phold_config
 
 DEFAULT_CACHE = os.environ.get("GPQ_TUNE_CACHE", os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib",
                                                               "tune_cache.json"))
+# Shapes measured on whole runs (not the tuner's short samples) and shipped with the
+# package; consulted when the local cache has no entry for the workload class.
+SHIPPED = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned_shapes.json")
 
 DEFAULT_SPACE = {
     "lanes_per_lp": [8, 16, 32],
@@ -68,6 +71,9 @@ def tune_phold(cfgd, queue="laq", loop="persistent", windows=200, space=None, ca
     data = _load(cache)
     if not force and key in data:
         return dict(data[key]["best"])
+    shipped = _load(SHIPPED)
+    if not force and key in shipped:
+        return dict(shipped[key]["best"])
     space = dict(DEFAULT_SPACE, **(space or {}))
     names = list(space.keys())
     results = []
