@@ -50,29 +50,50 @@ static __global__ void rs_hist_kernel(const gpq_item* __restrict__ in, uint32_t 
   hist[threadIdx.x * ntiles + tile] = cnt[threadIdx.x];
 }
 
-// In-place exclusive scan of `total` counts (one CTA of 1024 threads).
-static __global__ void rs_scan_kernel(uint32_t* a, uint32_t total) {
-  __shared__ uint32_t part[1024];
-  __shared__ uint32_t carry;
-  if (threadIdx.x == 0) carry = 0;
-  __syncthreads();
-  for (uint32_t base = 0; base < total; base += blockDim.x) {
-    const uint32_t i = base + threadIdx.x;
-    const uint32_t v = (i < total) ? a[i] : 0u;
-    part[threadIdx.x] = v;
-    __syncthreads();
-    for (uint32_t o = 1; o < blockDim.x; o <<= 1) {
-      const uint32_t t = (threadIdx.x >= o) ? part[threadIdx.x - o] : 0u;
-      __syncthreads();
-      part[threadIdx.x] += t;
-      __syncthreads();
-    }
-    if (i < total) a[i] = carry + part[threadIdx.x] - v;
-    __syncthreads();
-    if (threadIdx.x == blockDim.x - 1) carry += part[threadIdx.x];
-    __syncthreads();
+// In-place exclusive scan of `total` counts (one CTA of 1024 threads): each thread owns
+// a contiguous run of ceil(total / 1024) entries, sums it, the CTA scans the 1024 sums
+// (warp shuffles + one round over the warp totals), and each thread writes its run.
+__device__ __forceinline__ uint32_t rs_scan_block(uint32_t* a, uint32_t total) {
+  __shared__ uint32_t wsum[32];
+  __shared__ uint32_t s_all;
+  const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+  const uint32_t per = (total + blockDim.x - 1) / blockDim.x;
+  const uint32_t b0 = min(t * per, total), b1 = min(b0 + per, total);
+  uint32_t sum = 0;
+  for (uint32_t i = b0; i < b1; ++i) sum += a[i];
+  uint32_t incl = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t u = __shfl_up_sync(GPQ_FULL_MASK, incl, o);
+    if (lane >= (uint32_t)o) incl += u;
   }
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t nw = blockDim.x >> 5;
+    const uint32_t v = lane < nw ? wsum[lane] : 0u;
+    uint32_t wi = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t u = __shfl_up_sync(GPQ_FULL_MASK, wi, o);
+      if (lane >= (uint32_t)o) wi += u;
+    }
+    if (lane < nw) wsum[lane] = wi - v;
+    if (lane == nw - 1) s_all = wi;
+  }
+  __syncthreads();
+  uint32_t run = wsum[warp] + incl - sum;
+  for (uint32_t i = b0; i < b1; ++i) {
+    const uint32_t v = a[i];
+    a[i] = run;
+    run += v;
+  }
+  const uint32_t all = s_all;
+  __syncthreads();
+  return all;
 }
+
+static __global__ void rs_scan_kernel(uint32_t* a, uint32_t total) { rs_scan_block(a, total); }
 
 // Stable scatter of one tile: items are taken in tile order (round j holds items
 // j*256 + t); an item's rank among same-digit items of the tile is the count in earlier
@@ -179,7 +200,8 @@ static __global__ void gaq_split_kernel(const gpq_item* __restrict__ arr, uint32
 }
 
 static __global__ void gaq_stage_kernel(const gpq_item* __restrict__ arr, const uint32_t* info, GaqDev g, uint32_t L,
-                                        uint32_t* err) {
+                                        uint32_t* err, const uint32_t* gate = nullptr) {
+  if (gate && !*gate) return;
   const uint32_t c = info[0];
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c; i += gridDim.x * blockDim.x) {
     const gpq_item e = arr[i];
@@ -194,7 +216,8 @@ static __global__ void gaq_stage_kernel(const gpq_item* __restrict__ arr, const 
 // them into the LP's outputs in that order, and write their children to the window's
 // child buffer (one global reservation per CTA and round).
 template <int G>
-static __global__ void gaq_process_kernel(PholdDev d, GaqDev g, uint32_t* err) {
+static __global__ void gaq_process_kernel(PholdDev d, GaqDev g, uint32_t* err, const uint32_t* gate = nullptr) {
+  if (gate && !*gate) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ uint32_t cta_n, cta_base, kmin_s, kmax_s;
   const LaneGroup<G> grp;
@@ -317,4 +340,248 @@ static __global__ void gaq_zero_stats_kernel(PholdDev d) {
     d.csum[lp] = 0;
     d.ohash[lp] = 0;
   }
+}
+
+// ---- the window loop as a replayable sequence (CUDA graph) ----
+//
+// The host-driven loop reads the head and the child key range back every window.  Here
+// every size lives in device memory (GaqWin): the first kernel of a window decides
+// whether it runs (gate), finds the safe prefix, and the later kernels -- launched with
+// grids sized for the largest array -- read their sizes and exit early.  One window is
+// captured once into a CUDA graph and replayed many times between host checks; windows
+// replayed after the end are no-ops.
+
+// The window loop sorts each window's children with smaller radix tiles than the bulk
+// sort (more CTAs for a few hundred thousand items).
+static constexpr uint32_t kWinRsPer = 4;
+static constexpr uint32_t kWinRsTile = kRsThreads * kWinRsPer;
+
+struct GaqWin {
+  uint32_t c, nc, kmin, kmax;   // as GaqDev::info: prefix length, children, child key range
+  uint32_t n, cur, passes, ntiles;
+  uint32_t gate;                // this window runs
+  uint32_t done;                // the minimum reached the end time (or an error stopped the run)
+  uint32_t windows;             // windows executed
+  uint32_t stop_at;             // do not start window number stop_at (pause)
+  uint32_t total, pad[3];
+};
+
+// One CTA: the safe prefix by a multi-way search -- the answer lies in [lo, hi] (items
+// before lo are below the limit, items from hi on are not); every round each thread
+// probes one position of [lo, hi), probes below the limit raise lo past them, the others
+// lower hi to them, so the range shrinks by about blockDim each round.
+static __global__ void gaq_win_begin_kernel(const gpq_item* arr0, const gpq_item* arr1, GaqWin* w, float la, float T,
+                                            const uint32_t* err) {
+  __shared__ uint32_t s_run, s_lo, s_hi, s_lim;
+  if (threadIdx.x == 0) {
+    uint32_t run = 0;
+    if (!w->done) {
+      if (*err) w->done = 1;
+      else if (w->windows < w->stop_at) {
+        const gpq_item* a = w->cur ? arr1 : arr0;
+        if (w->n == 0 || !(a[0].ts < T)) w->done = 1;
+        else {
+          run = 1;
+          s_lim = min(gpq_f2u(GPQ_FADD(a[0].ts, la)), gpq_f2u(T));
+        }
+      }
+    }
+    s_run = run;
+    s_lo = 0;
+    s_hi = w->n;
+  }
+  __syncthreads();
+  if (!s_run) {
+    if (threadIdx.x == 0) w->gate = 0;
+    return;
+  }
+  const gpq_item* a = w->cur ? arr1 : arr0;
+  const uint32_t lim = s_lim;
+  for (;;) {
+    const uint32_t lo = s_lo, hi = s_hi;
+    __syncthreads();  // everyone has read the range before it changes
+    if (lo >= hi) break;
+    const uint32_t pos = lo + (uint32_t)(((uint64_t)(hi - lo) * threadIdx.x) / blockDim.x);
+    if (gpq_f2u(a[pos].ts) < lim) atomicMax(&s_lo, pos + 1);
+    else atomicMin(&s_hi, pos);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    w->c = s_lo;
+    w->nc = 0;
+    w->kmin = 0xffffffffu;
+    w->kmax = 0;
+    w->gate = 1;
+    w->windows += 1;
+  }
+}
+
+// The stage kernel takes the array through a pointer chosen by the window's buffer.
+static __global__ void gaq_win_stage_kernel(const gpq_item* arr0, const gpq_item* arr1, GaqWin* w, GaqDev g,
+                                            uint32_t L, uint32_t* err) {
+  if (!w->gate) return;
+  const gpq_item* a = w->cur ? arr1 : arr0;
+  const uint32_t c = w->c;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c; i += gridDim.x * blockDim.x) {
+    const gpq_item e = a[i];
+    if (e.lp >= L) { gpq_set_error(err, GPQ_ERR_INVALID); continue; }
+    const uint32_t slot = atomicAdd(&g.stg_cnt[e.lp], 1u);
+    if (slot < g.ibc) g.stg[(size_t)e.lp * g.ibc + slot] = e;
+    else gpq_set_error(err, GPQ_ERR_INSERT_FULL);
+  }
+}
+
+static __global__ void gaq_win_sort_setup_kernel(GaqWin* w, uint32_t cap, uint32_t ch_cap, uint32_t* err) {
+  if (threadIdx.x != 0 || blockIdx.x != 0 || !w->gate) return;
+  const uint32_t nc = min(w->nc, ch_cap);
+  w->nc = nc;
+  uint32_t passes = 0;
+  if (nc > 1 && w->kmax > w->kmin) passes = (32u - __clz(w->kmax - w->kmin) + 7u) / 8u;
+  w->passes = passes;
+  w->ntiles = (nc + kWinRsTile - 1) / kWinRsTile;
+  const uint64_t total = (uint64_t)w->n - w->c + nc;
+  if (total > cap) {
+    gpq_set_error(err, GPQ_ERR_QUEUE_FULL);
+    w->gate = 0;
+    w->done = 1;
+    return;
+  }
+  w->total = (uint32_t)total;
+}
+
+__device__ __forceinline__ bool gaq_win_pass(const GaqWin* w, uint32_t p) { return w->gate && p < w->passes; }
+
+static __global__ void gaq_win_hist_kernel(const gpq_item* ch, const gpq_item* ch_tmp, const GaqWin* w, uint32_t p,
+                                           uint32_t* hist) {
+  if (!gaq_win_pass(w, p) || blockIdx.x >= w->ntiles) return;
+  __shared__ uint32_t cnt[256];
+  const gpq_item* in = (p & 1u) ? ch_tmp : ch;
+  const uint32_t tile = blockIdx.x, ntiles = w->ntiles, n = w->nc, kmin = w->kmin, shift = 8u * p;
+  cnt[threadIdx.x] = 0;
+  __syncthreads();
+  const uint32_t base = tile * kWinRsTile;
+  for (uint32_t j = 0; j < kWinRsPer; ++j) {
+    const uint32_t i = base + j * kRsThreads + threadIdx.x;
+    if (i < n) atomicAdd(&cnt[rs_digit(in[i], kmin, shift)], 1u);
+  }
+  __syncthreads();
+  hist[threadIdx.x * ntiles + tile] = cnt[threadIdx.x];
+}
+
+// The digit offsets of a pass on many CTAs: block d scans digit d's counts across the
+// tiles (hist[d * ntiles + tile], exclusive) and leaves the digit's total in dig[d]; then
+// one CTA turns dig into exclusive digit offsets.  The scatter adds both.
+static __global__ void gaq_win_rowscan_kernel(const GaqWin* w, uint32_t p, uint32_t* hist, uint32_t* dig) {
+  if (!gaq_win_pass(w, p)) return;
+  const uint32_t ntiles = w->ntiles;
+  const uint32_t tot = rs_scan_block(hist + (size_t)blockIdx.x * ntiles, ntiles);
+  if (threadIdx.x == 0) dig[blockIdx.x] = tot;
+}
+
+static __global__ void gaq_win_digscan_kernel(const GaqWin* w, uint32_t p, uint32_t* dig) {
+  if (!gaq_win_pass(w, p)) return;
+  rs_scan_block(dig, 256u);
+}
+
+static __global__ void gaq_win_scatter_kernel(gpq_item* ch, gpq_item* ch_tmp, const GaqWin* w, uint32_t p,
+                                              const uint32_t* __restrict__ off, const uint32_t* __restrict__ dig) {
+  if (!gaq_win_pass(w, p) || blockIdx.x >= w->ntiles) return;
+  __shared__ uint32_t run[256];
+  __shared__ uint32_t wc[kRsThreads / 32][256];
+  const gpq_item* in = (p & 1u) ? ch_tmp : ch;
+  gpq_item* out = (p & 1u) ? ch : ch_tmp;
+  const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+  const uint32_t tile = blockIdx.x, ntiles = w->ntiles, n = w->nc, kmin = w->kmin, shift = 8u * p;
+  run[t] = 0;
+  const uint32_t base = tile * kWinRsTile;
+  for (uint32_t j = 0; j < kWinRsPer; ++j) {
+    for (uint32_t x = t; x < (kRsThreads / 32) * 256; x += kRsThreads) (&wc[0][0])[x] = 0;
+    __syncthreads();
+    const uint32_t i = base + j * kRsThreads + t;
+    const bool valid = i < n;
+    gpq_item e;
+    uint32_t dgt = 0;
+    if (valid) {
+      e = in[i];
+      dgt = rs_digit(e, kmin, shift);
+    }
+    const uint32_t peers = __match_any_sync(GPQ_FULL_MASK, valid ? dgt : (0x100u + lane));
+    if (valid && lane == (uint32_t)(__ffs(peers) - 1)) wc[warp][dgt] = __popc(peers);
+    __syncthreads();
+    if (valid) {
+      uint32_t pre = 0;
+      for (uint32_t q = 0; q < warp; ++q) pre += wc[q][dgt];
+      const uint32_t below = __popc(peers & ((1u << lane) - 1u));
+      out[dig[dgt] + off[dgt * ntiles + tile] + run[dgt] + pre + below] = e;
+    }
+    __syncthreads();
+    uint32_t sum = 0;
+    for (uint32_t q = 0; q < kRsThreads / 32; ++q) sum += wc[q][t];
+    run[t] += sum;
+    __syncthreads();
+  }
+}
+
+// Merge-path splits of the window's merge: split[b] = A items among the first b * kMpTile
+// outputs, one thread per tile boundary (all searches at once).
+__device__ __forceinline__ void gaq_win_merge_inputs(const gpq_item* arr0, const gpq_item* arr1, const gpq_item* ch,
+                                                     const gpq_item* ch_tmp, const GaqWin* w, const gpq_item** A,
+                                                     uint32_t* na, const gpq_item** B, uint32_t* nb) {
+  *A = (w->cur ? arr1 : arr0) + w->c;
+  *na = w->n - w->c;
+  *B = (w->passes & 1u) ? ch_tmp : ch;
+  *nb = w->nc;
+}
+
+static __global__ void gaq_win_splits_kernel(const gpq_item* arr0, const gpq_item* arr1, const gpq_item* ch,
+                                             const gpq_item* ch_tmp, const GaqWin* w, uint32_t* split) {
+  if (!w->gate) return;
+  const uint32_t total = w->total;
+  const uint32_t tiles = (total + kMpTile - 1) / kMpTile;
+  const gpq_item *A, *B;
+  uint32_t na, nb;
+  gaq_win_merge_inputs(arr0, arr1, ch, ch_tmp, w, &A, &na, &B, &nb);
+  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b <= tiles; b += gridDim.x * blockDim.x)
+    split[b] = mp_search(A, na, B, nb, min(b * kMpTile, total));
+}
+
+// Merge the array's unsafe suffix with the sorted children into the other buffer.
+static __global__ void gaq_win_merge_kernel(gpq_item* arr0, gpq_item* arr1, const gpq_item* ch, const gpq_item* ch_tmp,
+                                            const GaqWin* w, const uint32_t* __restrict__ split) {
+  if (!w->gate) return;
+  const uint32_t total = w->total;
+  const uint32_t d0 = blockIdx.x * kMpTile;
+  if (d0 >= total) return;
+  const gpq_item *A, *B;
+  uint32_t na, nb;
+  gaq_win_merge_inputs(arr0, arr1, ch, ch_tmp, w, &A, &na, &B, &nb);
+  gpq_item* out = w->cur ? arr0 : arr1;
+  extern __shared__ __align__(16) unsigned char mp_smem[];
+  gpq_item* s = reinterpret_cast<gpq_item*>(mp_smem);  // [kMpTile] inputs
+  gpq_item* o = s + kMpTile;                           // [kMpTile] merged, then stored coalesced
+  const uint32_t d1 = min(d0 + kMpTile, total);
+  const uint32_t a0 = split[blockIdx.x], a1 = split[blockIdx.x + 1];
+  const uint32_t b0 = d0 - a0, b1 = d1 - a1;
+  const uint32_t la = a1 - a0, lb = b1 - b0;
+  for (uint32_t x = threadIdx.x; x < la; x += kMpThreads) s[x] = A[a0 + x];
+  for (uint32_t x = threadIdx.x; x < lb; x += kMpThreads) s[la + x] = B[b0 + x];
+  __syncthreads();
+  const uint32_t my0 = threadIdx.x * kMpPer;
+  if (my0 < la + lb) {
+    uint32_t ia = mp_search(s, la, s + la, lb, my0);
+    uint32_t ib = my0 - ia;
+    const uint32_t lim = min(my0 + kMpPer, la + lb);
+    for (uint32_t q = my0; q < lim; ++q) {
+      const bool take_a = ib >= lb || (ia < la && gpq_f2u(s[ia].ts) <= gpq_f2u(s[la + ib].ts));
+      o[q] = take_a ? s[ia++] : s[la + ib++];
+    }
+  }
+  __syncthreads();
+  for (uint32_t x = threadIdx.x; x < la + lb; x += kMpThreads) out[d0 + x] = o[x];
+}
+
+static __global__ void gaq_win_end_kernel(GaqWin* w) {
+  if (threadIdx.x != 0 || blockIdx.x != 0 || !w->gate) return;
+  w->n = w->total;
+  w->cur ^= 1u;
 }

@@ -59,19 +59,30 @@ struct GaqEngine {
   uint32_t* hist = nullptr;
   uint32_t* h_info = nullptr;  // pinned: [0..3] info, [4] head ts bits, [5] error
   unsigned long long* acc = nullptr;
+  GaqWin* win = nullptr;        // device window state of the graph-replayed loop
+  uint32_t* dig = nullptr;      // [256] digit totals / offsets of a radix pass
+  uint32_t* split = nullptr;    // merge-path splits of the window's merge
+  GaqWin* h_win = nullptr;      // pinned copy
+  cudaGraph_t graph = nullptr;  // one window
+  cudaGraphExec_t gexec = nullptr;
   uint32_t block = 256;
   static constexpr int G = 8;
 
   GaqDev dev() const { return GaqDev{stg, stg_cnt, ch, info, c.insert_capacity, cap}; }
   ~GaqEngine() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (graph) cudaGraphDestroy(graph);
     for (void* p : {(void*)arr[0], (void*)arr[1], (void*)ch, (void*)ch_tmp, (void*)stg, (void*)stg_cnt, (void*)info,
-                    (void*)hist, (void*)acc})
+                    (void*)hist, (void*)acc, (void*)win, (void*)dig, (void*)split})
       if (p) cudaFree(p);
     if (h_info) cudaFreeHost(h_info);
+    if (h_win) cudaFreeHost(h_win);
   }
 };
 
-uint32_t gaq_engine_launches_per_window() { return 5 + 3 * 3; }
+// Kernels of one window: begin, stage, process, sort set-up, 4 x (hist, row scan, digit
+// scan, scatter), splits, merge, end.
+uint32_t gaq_engine_launches_per_window() { return 4 + 4 * 4 + 3; }
 
 gpq_status gaq_engine_create(const gpq_phold_config& c, GaqEngine** out) {
   *out = nullptr;
@@ -98,9 +109,20 @@ gpq_status gaq_engine_create(const gpq_phold_config& c, GaqEngine** out) {
   if ((e = cudaMalloc(&g->stg, (size_t)c.num_lps * c.insert_capacity * sizeof(gpq_item))) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&g->stg_cnt, (size_t)c.num_lps * sizeof(uint32_t))) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&g->info, 8 * sizeof(uint32_t))) != cudaSuccess) return fail(e);
-  if ((e = cudaMalloc(&g->hist, radix_hist_words(g->cap) * sizeof(uint32_t))) != cudaSuccess) return fail(e);
+  // the bulk sort's tiles (kRsTile) and the window loop's smaller ones (kWinRsTile)
+  if ((e = cudaMalloc(&g->hist, (size_t)256 * std::max<uint32_t>(1u, (g->cap + kWinRsTile - 1) / kWinRsTile) *
+                                    sizeof(uint32_t))) != cudaSuccess)
+    return fail(e);
+  if ((e = cudaFuncSetAttribute(gaq_win_merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(2 * kMpTile * sizeof(gpq_item)))) != cudaSuccess)
+    return fail(e);
   if ((e = cudaMalloc(&g->acc, 8 * sizeof(unsigned long long))) != cudaSuccess) return fail(e);
   if ((e = cudaMallocHost(&g->h_info, 8 * sizeof(uint32_t))) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&g->win, sizeof(GaqWin))) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&g->dig, 256 * sizeof(uint32_t))) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&g->split, ((g->cap + kMpTile - 1) / kMpTile + 2) * sizeof(uint32_t))) != cudaSuccess)
+    return fail(e);
+  if ((e = cudaMallocHost(&g->h_win, sizeof(GaqWin))) != cudaSuccess) return fail(e);
   const size_t smem = (size_t)(g->block / GaqEngine::G) * c.insert_capacity * sizeof(uint64_t);
   if ((e = cudaFuncSetAttribute(gaq_process_kernel<GaqEngine::G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)smem)) != cudaSuccess)
@@ -128,52 +150,89 @@ gpq_status gaq_engine_populate(GaqEngine* g, const PholdDev& d, const gpq_item* 
   GPQ_CUDA_TRY(cudaMemcpyAsync(g->arr[0], sorted, (size_t)g->cap * sizeof(gpq_item), cudaMemcpyDeviceToDevice, st));
   g->cur = 0;
   g->n = g->cap;
+  *g->h_win = GaqWin{};
+  g->h_win->n = g->cap;
+  g->h_win->stop_at = 0xffffffffu;
+  GPQ_CUDA_TRY(cudaMemcpyAsync(g->win, g->h_win, sizeof(GaqWin), cudaMemcpyHostToDevice, st));
+  GPQ_CUDA_TRY(cudaStreamSynchronize(st));
   return GPQ_OK;
 }
 
+// Capture one window of the device-driven loop into a graph (once per engine).
+static gpq_status gaq_capture(GaqEngine* g, const PholdDev& d, cudaStream_t st) {
+  if (g->gexec) return GPQ_OK;
+  const gpq_phold_config& c = g->c;
+  GaqDev gd = g->dev();
+  gd.info = reinterpret_cast<uint32_t*>(g->win);  // c, nc, kmin, kmax
+  const uint32_t pgrid = std::max(1u, std::min<uint32_t>((c.num_lps + (g->block / GaqEngine::G) - 1) /
+                                                             (g->block / GaqEngine::G), 8192));
+  const size_t psmem = (size_t)(g->block / GaqEngine::G) * c.insert_capacity * sizeof(uint64_t);
+  const uint32_t sgrid = std::max(1u, std::min<uint32_t>((g->cap + 255) / 256, 8192));
+  const uint32_t max_tiles = std::max(1u, (g->cap + kWinRsTile - 1) / kWinRsTile);
+  const uint32_t mgrid = std::max(1u, (g->cap + kMpTile - 1) / kMpTile);
+  GPQ_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  gaq_win_begin_kernel<<<1, 1024, 0, st>>>(g->arr[0], g->arr[1], g->win, c.lookahead, c.end_time, &d.ctrl->err);
+  gaq_win_stage_kernel<<<sgrid, 256, 0, st>>>(g->arr[0], g->arr[1], g->win, gd, c.num_lps, &d.ctrl->err);
+  gaq_process_kernel<GaqEngine::G><<<pgrid, g->block, psmem, st>>>(d, gd, &d.ctrl->err, &g->win->gate);
+  gaq_win_sort_setup_kernel<<<1, 32, 0, st>>>(g->win, g->cap, g->cap, &d.ctrl->err);
+  for (uint32_t p = 0; p < 4; ++p) {
+    gaq_win_hist_kernel<<<max_tiles, kRsThreads, 0, st>>>(g->ch, g->ch_tmp, g->win, p, g->hist);
+    gaq_win_rowscan_kernel<<<256, 128, 0, st>>>(g->win, p, g->hist, g->dig);
+    gaq_win_digscan_kernel<<<1, 256, 0, st>>>(g->win, p, g->dig);
+    gaq_win_scatter_kernel<<<max_tiles, kRsThreads, 0, st>>>(g->ch, g->ch_tmp, g->win, p, g->hist, g->dig);
+  }
+  gaq_win_splits_kernel<<<(mgrid + 1 + 255) / 256, 256, 0, st>>>(g->arr[0], g->arr[1], g->ch, g->ch_tmp, g->win,
+                                                                  g->split);
+  gaq_win_merge_kernel<<<mgrid, kMpThreads, 2 * kMpTile * sizeof(gpq_item), st>>>(g->arr[0], g->arr[1], g->ch,
+                                                                                  g->ch_tmp, g->win, g->split);
+  gaq_win_end_kernel<<<1, 32, 0, st>>>(g->win);
+  const cudaError_t ce = cudaStreamEndCapture(st, &g->graph);
+  if (ce != cudaSuccess) {
+    set_last_error("global array queue: graph capture failed: %s", cudaGetErrorString(ce));
+    return GPQ_ERR_CUDA;
+  }
+  GPQ_CUDA_TRY(cudaGraphInstantiate(&g->gexec, g->graph, 0));
+  return GPQ_OK;
+}
+
+// des_run for the global array queue: replay the captured window in batches (16, 32, ...
+// up to 256 windows) between host checks of the device window state.
 gpq_status gaq_engine_run(GaqEngine* g, const PholdDev& d, uint32_t nsteps, int* done, uint64_t* windows,
                           cudaStream_t st) {
   const gpq_phold_config& c = g->c;
   if (done) *done = 0;
-  const uint32_t pgrid = std::max(1u, std::min<uint32_t>((c.num_lps + (g->block / GaqEngine::G) - 1) /
-                                                             (g->block / GaqEngine::G), 8192));
-  const size_t psmem = (size_t)(g->block / GaqEngine::G) * c.insert_capacity * sizeof(uint64_t);
-  uint32_t executed = 0;
+  gpq_status s = gaq_capture(g, d, st);
+  if (s != GPQ_OK) return s;
+  GPQ_CUDA_TRY(cudaMemcpyAsync(g->h_win, g->win, sizeof(GaqWin), cudaMemcpyDeviceToHost, st));
+  GPQ_CUDA_TRY(cudaStreamSynchronize(st));
+  const uint32_t w0 = g->h_win->windows;
+  uint64_t stop = nsteps ? (uint64_t)w0 + nsteps : 0xffffffffull;
+  if (c.max_steps) stop = std::min<uint64_t>(stop, c.max_steps);
+  g->h_win->stop_at = (uint32_t)std::min<uint64_t>(stop, 0xffffffffull);
+  GPQ_CUDA_TRY(cudaMemcpyAsync(&g->win->stop_at, &g->h_win->stop_at, sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+  uint32_t batch = 16;
   for (;;) {
-    if (nsteps && executed >= nsteps) break;
-    if (c.max_steps && *windows >= c.max_steps) { if (done) *done = 1; break; }
-    // des_run: the window minimum is the array head (src/global_array_queue.cu:299-306)
-    g->h_info[4] = kInfBits;
-    if (g->n) GPQ_CUDA_TRY(cudaMemcpyAsync(&g->h_info[4], &g->arr[g->cur][0].ts, 4, cudaMemcpyDeviceToHost, st));
+    for (uint32_t k = 0; k < batch; ++k) GPQ_CUDA_TRY(cudaGraphLaunch(g->gexec, st));
+    GPQ_CUDA_TRY(cudaMemcpyAsync(g->h_win, g->win, sizeof(GaqWin), cudaMemcpyDeviceToHost, st));
     GPQ_CUDA_TRY(cudaMemcpyAsync(&g->h_info[5], &d.ctrl->err, 4, cudaMemcpyDeviceToHost, st));
     GPQ_CUDA_TRY(cudaStreamSynchronize(st));
-    const float m = gpq_u2f(g->h_info[4]);
-    if (g->h_info[5] != 0) return (gpq_status)g->h_info[5];
-    if (g->n == 0 || !(m < c.end_time)) { if (done) *done = 1; break; }
-    const float bound = GPQ_FADD(m, c.lookahead);
-    gpq_item* a = g->arr[g->cur];
-    gaq_split_kernel<<<1, 32, 0, st>>>(a, g->n, bound, c.end_time, g->info);
-    gaq_stage_kernel<<<std::max(1u, std::min<uint32_t>((g->n + 255) / 256, 8192)), 256, 0, st>>>(
-        a, g->info, g->dev(), c.num_lps, &d.ctrl->err);
-    gaq_process_kernel<GaqEngine::G><<<pgrid, g->block, psmem, st>>>(d, g->dev(), &d.ctrl->err);
-    GPQ_CUDA_TRY(cudaGetLastError());
-    GPQ_CUDA_TRY(cudaMemcpyAsync(g->h_info, g->info, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    GPQ_CUDA_TRY(cudaStreamSynchronize(st));
-    const uint32_t cpre = g->h_info[0], nc = std::min(g->h_info[1], g->cap);
-    gpq_item* sorted = g->ch;
-    gpq_status s = radix_sort_by_ts(g->ch, g->ch_tmp, nc, g->h_info[2], g->h_info[3], g->hist, &sorted, st);
-    if (s != GPQ_OK) return s;
-    if (g->n - cpre + nc > g->cap) {
-      set_last_error("global array queue overflow");
-      return GPQ_ERR_QUEUE_FULL;
+    g->n = g->h_win->n;
+    g->cur = (int)g->h_win->cur;
+    if (g->h_info[5] != 0) {
+      *windows += g->h_win->windows - w0;
+      return (gpq_status)g->h_info[5];
     }
-    s = merge_by_ts(a + cpre, g->n - cpre, sorted, nc, g->arr[g->cur ^ 1], st);
-    if (s != GPQ_OK) return s;
-    g->n = g->n - cpre + nc;
-    g->cur ^= 1;
-    ++*windows;
-    ++executed;
+    if (g->h_win->done) {
+      if (done) *done = 1;
+      break;
+    }
+    if (g->h_win->windows >= g->h_win->stop_at) {
+      if (c.max_steps && g->h_win->windows >= c.max_steps && done) *done = 1;
+      break;
+    }
+    batch = std::min<uint32_t>(batch * 2, 256);
   }
+  *windows += g->h_win->windows - w0;
   return GPQ_OK;
 }
 
