@@ -140,6 +140,8 @@ struct AstarTileSmem {
   uint32_t* gt;   // [ts * ts] g of the tile's cells, local index ly * ts + lx
   uint32_t* blk;  // [ts * ts / 32] blocked bits of the tile
   uint32_t* chg;  // [ts * ts / 32] cells whose g dropped during this visit
+  uint2* ob;      // [8 * ts] moves into other tiles, sent when the visit ends
+  uint32_t ob_n;
   uint32_t n[3];  // frontier fill, rotating by level
   uint32_t ub;    // the instance's best goal cost as of this visit (stale values only prune less)
   uint32_t open_min;
@@ -148,8 +150,11 @@ struct AstarTileSmem {
   uint32_t scan[33];
 };
 
+__host__ __device__ inline uint32_t astar_outbox_cap(uint32_t ts) { return 8u * ts; }
+
 __host__ __device__ inline size_t astar_smem_bytes(uint32_t ts, uint32_t frontier_cap) {
-  return 2ull * frontier_cap * sizeof(uint2) + (size_t)ts * ts * sizeof(uint32_t) + 2ull * (ts * ts / 32) * sizeof(uint32_t);
+  return 2ull * frontier_cap * sizeof(uint2) + (size_t)astar_outbox_cap(ts) * sizeof(uint2) +
+         (size_t)ts * ts * sizeof(uint32_t) + 2ull * (ts * ts / 32) * sizeof(uint32_t);
 }
 
 // Geometry of the tile being processed.
@@ -220,6 +225,20 @@ __device__ __forceinline__ bool astar_cell_blocked(const AstarDev& d, const Asta
   return astar_blocked(d, I, (uint32_t)y * I.g.width + (uint32_t)x);
 }
 
+// A move into another tile: lower the cell's global g (the filter), and when that
+// improves it, send the item to the owning tile's inbox for the next round.
+__device__ __forceinline__ void astar_send(const AstarDev& d, AstarInstDev* Ip, const AstarInstDev& I, uint2 it,
+                                           uint32_t npar) {
+  const int x = (int)(it.x & 0xffffu), y = (int)(it.x >> 16);
+  const uint32_t ng = it.y;
+  if (ng >= atomicMin(&d.gcost[I.cell0 + (uint32_t)y * I.g.width + (uint32_t)x], ng)) return;
+  const uint32_t nf = ng + astar_hxy(I.g.conn, x, y, (int)I.gx, (int)I.gy);
+  if (x == (int)I.gx && y == (int)I.gy) atomicMin(&Ip->ub, ng);
+  if (nf > ldcg_u32(&Ip->ub)) return;
+  const uint32_t nt = I.tile0 + ((uint32_t)y >> d.lts) * I.tiles_x + ((uint32_t)x >> d.lts);
+  astar_inbox_push(d, Ip, nt, npar, it);
+}
+
 // Expand frontier items src[ib .. ib + 32 / M) with one warp, one lane per (item, move):
 // lane = item * M + move, M = 4 or 8 moves (all lanes call; ib is warp-uniform).  A level
 // of few items thus costs the latency of one move, not of M moves in a row.  Children
@@ -235,7 +254,7 @@ __device__ __forceinline__ void astar_expand_warp(const AstarDev& d, AstarInstDe
   const uint32_t M = conn == 4 ? 4u : 8u;
   const uint32_t k = lane & (M - 1u);
   const uint32_t i = ib + lane / M;
-  uint32_t kind = 0;  // 1 frontier, 2 open array, 3 another tile's inbox
+  uint32_t kind = 0;  // 1 frontier, 2 open array, 4 outbox (another tile)
   uint2 child = make_uint2(0, 0);
   uint32_t nf = kAstarInf;
   if (i < n) {
@@ -257,7 +276,9 @@ __device__ __forceinline__ void astar_expand_warp(const AstarDev& d, AstarInstDe
             ok = ng < atomicMin(&sm.gt[l], ng);
             if (ok) atomicOr(&sm.chg[l >> 5], 1u << (l & 31u));
           } else {
-            ok = ng < atomicMin(&d.gcost[I.cell0 + (uint32_t)ny * w + (uint32_t)nx], ng);
+            kind = 4u;  // to the outbox: filtered and sent when the visit ends
+            child = make_uint2(astar_pack(nx, ny), ng);
+            ok = false;
           }
           if (ok) {
             const int gx = (int)I.gx, gy = (int)I.gy;
@@ -268,11 +289,7 @@ __device__ __forceinline__ void astar_expand_warp(const AstarDev& d, AstarInstDe
             }
             if (nf <= sm.ub) {
               child = make_uint2(astar_pack(nx, ny), ng);
-              kind = in ? (nf <= bound ? 1u : 2u) : 3u;
-              if (kind == 3u) {
-                const uint32_t nt = I.tile0 + ((uint32_t)ny >> d.lts) * I.tiles_x + ((uint32_t)nx >> d.lts);
-                astar_inbox_push(d, Ip, nt, npar, child);
-              }
+              kind = nf <= bound ? 1u : 2u;
             }
           }
         }
@@ -289,6 +306,18 @@ __device__ __forceinline__ void astar_expand_warp(const AstarDev& d, AstarInstDe
       const uint32_t pos = base + __popc(mf & lt);
       if (pos < d.frontier_cap) next[pos] = child;
       else astar_inbox_push(d, Ip, t, npar, child);  // full: the tile's own next round
+    }
+  }
+  const uint32_t mx = __ballot_sync(GPQ_FULL_MASK, kind == 4u);
+  if (mx) {
+    const uint32_t leader = (uint32_t)(__ffs(mx) - 1);
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(&sm.ob_n, (uint32_t)__popc(mx));
+    base = __shfl_sync(GPQ_FULL_MASK, base, leader);
+    if (kind == 4u) {
+      const uint32_t pos = base + __popc(mx & lt);
+      if (pos < astar_outbox_cap(tg.ts)) sm.ob[pos] = child;
+      else astar_send(d, Ip, I, child, npar);  // full: send now
     }
   }
   const uint32_t mo = __ballot_sync(GPQ_FULL_MASK, kind == 2u);
@@ -367,6 +396,7 @@ __device__ void astar_process_tile(const AstarDev& d, uint32_t t, uint32_t s, As
     sm.n[0] = 0;
     sm.n[1] = 0;
     sm.n[2] = 0;
+    sm.ob_n = 0;
     sm.pops = 0;
     sm.open_cnt = T->open_cnt;
     sm.open_min = kAstarInf;
@@ -482,7 +512,12 @@ __device__ void astar_process_tile(const AstarDev& d, uint32_t t, uint32_t s, As
       astar_expand_warp(d, Ip, I, sm, tg, src, ib, n, dst, (c3 + 1u) % 3u, t, npar, bound, &pops);
     wk.sync();
   }
-  // 4. merge the tile's g values back
+  // 4. send the moves into other tiles
+  {
+    const uint32_t nob = min(sm.ob_n, astar_outbox_cap(ts));
+    for (uint32_t i = wk.tid; i < nob; i += wk.n) astar_send(d, Ip, I, sm.ob[i], npar);
+  }
+  // 5. merge the tile's g values back
   for (uint32_t l = wk.tid; l < ts * ts; l += wk.n) {
     if ((sm.chg[l >> 5] >> (l & 31u)) & 1u) {
       const uint32_t lx = l % ts, ly = l / ts;
@@ -555,7 +590,8 @@ static __global__ void __launch_bounds__(256) astar_persistent_kernel(AstarDev d
     unsigned char* base = smem_raw + (size_t)wk.id * astar_worker_smem_bytes(d.ts, d.frontier_cap);
     sm.fa = reinterpret_cast<uint2*>(base);
     sm.fb = sm.fa + d.frontier_cap;
-    sm.gt = reinterpret_cast<uint32_t*>(sm.fb + d.frontier_cap);
+    sm.ob = sm.fb + d.frontier_cap;
+    sm.gt = reinterpret_cast<uint32_t*>(sm.ob + astar_outbox_cap(d.ts));
     sm.blk = sm.gt + d.ts * d.ts;
     sm.chg = sm.blk + d.ts * d.ts / 32;
   }
