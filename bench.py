@@ -113,6 +113,21 @@ def dist_env():
     return ws, rank, local
 
 
+def reduce_over_ranks(dist, x, op, device):
+    """One float reduced over all ranks (op "max" or "sum"); x itself without a group."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def replica_seed(rank):
+    """Replica r of the multi-GPU bench runs the workload with seed + r."""
+    return WORKLOAD["seed"] + rank
+
+
 def cpu_reference_run(cfgd, end_time, threads):
     from oracle import oracle as O
     c = O.make_cfg(num_lps=cfgd["num_lps"], events_per_lp=cfgd["events_per_lp"], lookahead=cfgd["lookahead"],
@@ -360,7 +375,7 @@ def main():
     cfgd = dict(WORKLOAD)
     if args.end_time is not None:
         cfgd["end_time"] = args.end_time
-    cfgd["seed"] = WORKLOAD["seed"] + rank
+    cfgd["seed"] = replica_seed(rank)
     shape = {}
     if not args.no_tune:
         from gpupq_b200 import autotune
@@ -377,20 +392,10 @@ def main():
             dist.barrier()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_over_ranks(dist, x, "max", "cuda")
 
     def sum_over_ranks(x):
-        if dist is None:
-            return x
-        import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+        return reduce_over_ranks(dist, x, "sum", "cuda")
 
     # warm-up
     ref_digest = None
