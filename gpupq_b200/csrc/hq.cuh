@@ -32,6 +32,7 @@ struct HqDev {
   gpq_item* nodes;   // [maxnodes][r]
   uint32_t* cnt;     // [maxnodes] items per node
   uint32_t* meta;    // [0] last non-empty node, [1] windows executed
+  gpq_item* ch;      // children of the current window (PHOLD engine; population-sized)
   uint32_t r;
   uint32_t maxnodes;
 };

@@ -30,76 +30,88 @@ __device__ __forceinline__ HqWork hq_work(unsigned char* raw, uint32_t r) {
 }
 
 // One heap, all windows (des_run over the parallel heap).  Per window: insert the
-// previous window's children, take the root's safe prefix S, fold S into the per-LP
-// outputs in key order per LP (ranks from a sort by (lp, position)), make S's children,
-// remove S from the root and refill it.  One CTA; blockDim a multiple of 32.
+// previous window's children (from h.ch, r at a time), fix the window bound from the
+// root's head, then repeatedly take the root's prefix below the bound S, fold S into
+// the per-LP outputs in key order per LP (ranks from a sort by (lp, position)), append
+// S's children to h.ch, remove S from the root and refill it -- until the root's head
+// reaches the bound.  The root always holds the r smallest items, so the batches come
+// in global key order; a child is never safe in its parent's window, so the children
+// wait for the next window.  One CTA; blockDim a multiple of 32.
 static __device__ void hq_phold_run(const PholdDev& d, const HqDev& h, uint32_t max_steps, unsigned char* raw) {
   const uint32_t r = h.r;
   const HqWork w = hq_work(raw, r);
-  __shared__ uint32_t s_last, s_ke, s_c, s_n0, s_stop, s_steps;
+  __shared__ uint32_t s_last, s_nch, s_c, s_n0, s_stop, s_steps, s_lim;
   if (threadIdx.x == 0) {
     s_last = h.meta[0];
-    s_ke = 0;
+    s_nch = 0;
     s_steps = 0;
   }
   __syncthreads();
   for (;;) {
-    if (s_ke) {
-      const bool ok = hq_insert(h, w.sm, w.e, s_ke, &s_last);
-      if (!ok) {
-        if (threadIdx.x == 0) gpq_set_error(&d.ctrl->err, GPQ_ERR_QUEUE_FULL);
-        break;
-      }
+    // the previous window's children
+    const uint32_t nch = s_nch;
+    bool full = false;
+    for (uint32_t off = 0; off < nch && !full; off += r) {
+      const uint32_t k = min(r, nch - off);
+      hq_load(w.e, h.ch + off, k);
+      full = !hq_insert(h, w.sm, w.e, k, &s_last);
+    }
+    if (full) {
+      if (threadIdx.x == 0) gpq_set_error(&d.ctrl->err, GPQ_ERR_QUEUE_FULL);
+      break;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-      s_ke = 0;
+      s_nch = 0;
       const uint32_t n0 = h.cnt[0];
       uint32_t stop = (n0 == 0) || (max_steps != 0 && s_steps >= max_steps);
-      uint32_t c = 0;
       if (!stop) {
         const float m = h.nodes[0].ts;
         stop = !(m < d.p.end_time);
         if (!stop) {
-          const uint32_t lim = min(gpq_f2u(GPQ_FADD(m, d.p.lookahead)), gpq_f2u(d.p.end_time));
-          uint32_t lo = 0, hi = n0;
-          while (lo < hi) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (gpq_f2u(h.nodes[mid].ts) < lim) lo = mid + 1; else hi = mid;
-          }
-          c = lo;
+          s_lim = min(gpq_f2u(GPQ_FADD(m, d.p.lookahead)), gpq_f2u(d.p.end_time));
+          ++s_steps;
         }
       }
       s_stop = stop;
-      s_c = c;
-      s_n0 = n0;
     }
     __syncthreads();
     if (s_stop) break;
-    const uint32_t c = s_c, n0 = s_n0;
-    hq_load(w.sm.a, h.nodes, c);
-    hq_lp_ranks(w.sm.a, c, w.keys, w.seg);
-    for (uint32_t p = threadIdx.x; p < c; p += blockDim.x) {
-      const uint32_t key = w.keys[p];
-      const uint32_t i = key & 0x7ffu, lp = key >> 11;
-      const gpq_item e = w.sm.a[i];
-      const uint64_t hh = gpq_ev_hash(e.id, gpq_f2u(e.ts));
-      atomicAdd(&d.csum[lp], (unsigned long long)hh);
-      atomicAdd(&d.ohash[lp], (unsigned long long)gpq_seq_hash(hh, (uint64_t)d.count[lp] + (p - w.seg[p])));
-      w.e[i] = gpq_phold_child(d.p, e);
+    for (;;) {  // batches of the window
+      if (threadIdx.x == 0) {
+        const uint32_t n0 = h.cnt[0];
+        uint32_t lo = 0, hi = n0;
+        while (lo < hi) {
+          const uint32_t mid = (lo + hi) >> 1;
+          if (gpq_f2u(h.nodes[mid].ts) < s_lim) lo = mid + 1; else hi = mid;
+        }
+        s_c = lo;
+        s_n0 = n0;
+      }
+      __syncthreads();
+      const uint32_t c = s_c, n0 = s_n0, base = s_nch;
+      if (c == 0) break;
+      hq_load(w.sm.a, h.nodes, c);
+      hq_lp_ranks(w.sm.a, c, w.keys, w.seg);
+      for (uint32_t p = threadIdx.x; p < c; p += blockDim.x) {
+        const uint32_t key = w.keys[p];
+        const uint32_t i = key & 0x7ffu, lp = key >> 11;
+        const gpq_item e = w.sm.a[i];
+        const uint64_t hh = gpq_ev_hash(e.id, gpq_f2u(e.ts));
+        atomicAdd(&d.csum[lp], (unsigned long long)hh);
+        atomicAdd(&d.ohash[lp], (unsigned long long)gpq_seq_hash(hh, (uint64_t)d.count[lp] + (p - w.seg[p])));
+        h.ch[base + i] = gpq_phold_child(d.p, e);
+      }
+      __syncthreads();
+      for (uint32_t p = threadIdx.x; p < c; p += blockDim.x) {
+        const uint32_t lp = w.keys[p] >> 11;
+        if (p + 1 == c || (w.keys[p + 1] >> 11) != lp) d.count[lp] += p - w.seg[p] + 1;
+      }
+      hq_load(w.sm.a, h.nodes + c, n0 - c);
+      hq_refill_root(h, w.sm, n0 - c, &s_last);
+      if (threadIdx.x == 0) s_nch = base + c;
+      __syncthreads();
     }
-    __syncthreads();
-    for (uint32_t p = threadIdx.x; p < c; p += blockDim.x) {
-      const uint32_t lp = w.keys[p] >> 11;
-      if (p + 1 == c || (w.keys[p + 1] >> 11) != lp) d.count[lp] += p - w.seg[p] + 1;
-    }
-    hq_load(w.sm.a, h.nodes + c, n0 - c);
-    hq_refill_root(h, w.sm, n0 - c, &s_last);
-    if (threadIdx.x == 0) {
-      s_ke = c;
-      ++s_steps;
-    }
-    __syncthreads();
   }
   if (threadIdx.x == 0) {
     h.meta[0] = s_last;

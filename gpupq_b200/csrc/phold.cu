@@ -176,6 +176,7 @@ gpq_status gpq_phold_create(const gpq_phold_config* cfg_in, gpq_phold** out) {
     TRY(cudaMalloc(&h->hq.meta, 4 * sizeof(uint32_t)));
     TRY(cudaMalloc(&h->hq_sort[0], N * sizeof(gpq_item)));
     TRY(cudaMalloc(&h->hq_sort[1], N * sizeof(gpq_item)));
+    h->hq.ch = h->hq_sort[1];  // after populate: the children of a window
     TRY(cudaMalloc(&h->hq_hist, gpq::radix_hist_words((uint32_t)N) * sizeof(uint32_t)));
     TRY(cudaMalloc(&h->hq_mm, 2 * sizeof(uint32_t)));
     TRY(cudaFuncSetAttribute(hq_phold_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hq_smem_bytes(r)));

@@ -73,7 +73,7 @@ def test_phold_plain_workload_bit_exact(gpu_lib, loop, queue, lanes):
     """1024 LPs x 16 events, lookahead 1.0, end 100, uniform destinations, seed 42."""
     o = _oracle(C1)
     r, s = _run(C1, loop=loop, queue=queue, lanes_per_lp=lanes)
-    _assert_same(r, s, o, check_steps=queue != "hq")
+    _assert_same(r, s, o)
     assert r["committed"] == 820705
 
 
@@ -83,7 +83,7 @@ def test_phold_heap_queue_node_sizes(gpu_lib, node_size):
     cfgd = dict(num_lps=300, events_per_lp=7, lookahead=0.3, end_time=25.0, seed=21, dest_mode=1, ring_width=5)
     o = _oracle(cfgd)
     r, s = _run(cfgd, queue="hq", node_size=node_size)
-    _assert_same(r, s, o, check_steps=False)
+    _assert_same(r, s, o)
 
 
 @pytest.mark.parametrize("queue,loop,lanes,block", [
@@ -97,7 +97,7 @@ def test_phold_large_reduced_bit_exact(gpu_lib, queue, loop, lanes, block):
     o = _oracle_cached(cfgd)
     r, s = _run(cfgd, queue=queue, loop=loop, capacity=256, insert_capacity=64, lanes_per_lp=lanes,
                 block_threads=block)
-    _assert_same(r, s, o, check_steps=queue != "hq")
+    _assert_same(r, s, o)
 
 
 @pytest.mark.parametrize("cfgd,kw", [
@@ -120,7 +120,7 @@ def test_phold_large_reduced_bit_exact(gpu_lib, queue, loop, lanes, block):
 def test_phold_edge_shapes(gpu_lib, cfgd, kw, queue, loop, lanes):
     o = _oracle(cfgd)
     r, s = _run(cfgd, queue=queue, loop=loop, lanes_per_lp=lanes, **kw)
-    _assert_same(r, s, o, check_steps=queue != "hq")
+    _assert_same(r, s, o)
 
 
 def test_host_initial_events_path(gpu_lib):
