@@ -183,7 +183,7 @@ def bench_astar_plain(G, O, args, peak):
     """One 2048 x 2048 grid (Bernoulli(0.2), seed 3, corner to corner, 4-connected, 1024
     shards of 64 x 64): expansions (cells with f <= C*) per second of device time."""
     g = G.astar_grid(2048, 2048, 0.2, 3)
-    with G.AStar(tile=32) as a:
+    with G.AStar(tile=64) as a:  # 1024 shards, as the workload names
         def step():
             r = a.solve(g)
             return r[0], a.stats()
