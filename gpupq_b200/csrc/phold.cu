@@ -208,7 +208,7 @@ gpq_status gpq_phold_create(const gpq_phold_config* cfg_in, gpq_phold** out) {
     *out = h;
     return GPQ_OK;
   }
-  if (!phold_kernel_set(c.queue_kind, c.lanes_per_lp, c.insert_capacity, &h->ks)) return fail(GPQ_ERR_INVALID);
+  if (!phold_kernel_set(c.queue_kind, c.lanes_per_lp, c.insert_capacity, &h->ks, c.laq_mode)) return fail(GPQ_ERR_INVALID);
   if (!gpq::fit_block_to_smem(&h->block, h->ks.group, h->ks.group_smem + 24 * kStageRounds,
                               200 * 1024 - 2048 * 16 - 16)) {
     gpq::set_last_error("insert_capacity %u needs too much shared memory per lane group", c.insert_capacity);

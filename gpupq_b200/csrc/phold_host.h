@@ -33,6 +33,8 @@ inline gpq_status validate_phold_config(const gpq_phold_config* c) {
     GPQ_CHECK_ARG(c->ring_width >= 1 && 2ull * c->ring_width < c->num_lps, "ring_width must satisfy 1 <= 2w < num_lps");
   GPQ_CHECK_ARG(c->loop_mode == GPQ_LOOP_PLAIN || c->loop_mode == GPQ_LOOP_PERSISTENT, "loop_mode");
   GPQ_CHECK_ARG(c->queue_kind <= GPQ_QUEUE_LSQ, "queue_kind");
+  GPQ_CHECK_ARG(c->laq_mode <= 1 && (c->laq_mode == 0 || c->queue_kind == GPQ_QUEUE_LAQ),
+                "laq_mode must be 0, or 1 with the local array queue");
   return GPQ_OK;
 }
 

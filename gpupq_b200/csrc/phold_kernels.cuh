@@ -8,6 +8,7 @@
 #include "laq.cuh"
 #include "lhq.cuh"
 #include "lsq.cuh"
+#include "las.cuh"
 
 // Union of the per-LP queue layouts (host-visible; kernels build the policy's view).
 struct LpQueueDev {
@@ -23,6 +24,10 @@ struct LpQueueDev {
 
 template <int G>
 struct LaqP : LaqPolicy<G> {
+  __device__ static LaqDev dev(const LpQueueDev& l) { return LaqDev{l.items, l.a, l.b, l.cap_log2}; }
+};
+template <int G>
+struct LasP : LasPolicy<G> {
   __device__ static LaqDev dev(const LpQueueDev& l) { return LaqDev{l.items, l.a, l.b, l.cap_log2}; }
 };
 template <int G>
@@ -253,10 +258,17 @@ struct PholdKernelSet {
   size_t group_smem;  // per lane group, for insert capacity ibc
 };
 
-inline bool phold_kernel_set(uint32_t kind, uint32_t group, uint32_t ibc, PholdKernelSet* out) {
+inline bool phold_kernel_set(uint32_t kind, uint32_t group, uint32_t ibc, PholdKernelSet* out, uint32_t laq_mode = 0) {
 #define GPQ_KS(P) *out = {(const void*)phold_window_kernel<P>, (const void*)phold_persistent_kernel<P>, \
                           (uint32_t)P::G, P::group_smem_bytes(ibc)}; return true
-  if (kind == GPQ_QUEUE_LAQ) {
+  if (kind == GPQ_QUEUE_LAQ && laq_mode == 1) {
+    switch (group) {
+      case 4: GPQ_KS(LasP<4>);
+      case 8: GPQ_KS(LasP<8>);
+      case 16: GPQ_KS(LasP<16>);
+      case 32: GPQ_KS(LasP<32>);
+    }
+  } else if (kind == GPQ_QUEUE_LAQ) {
     switch (group) {
       case 4: GPQ_KS(LaqP<4>);
       case 8: GPQ_KS(LaqP<8>);

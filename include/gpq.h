@@ -166,7 +166,9 @@ typedef struct gpq_phold_config {
   uint32_t max_steps;       /* safety cap on windows; 0 = none */
   uint32_t lanes_per_lp;    /* LAQ: lanes that work on one LP (4, 8, 16 or 32); 0 = tuned default */
   uint32_t node_size;       /* HQ: items per heap node r (power of two <= 1024); 0 = 1024 */
-  uint32_t reserved[2];
+  uint32_t laq_mode;        /* LAQ: 0 = sorted runs, children merged each window; 1 = unordered
+                               arrays, each window's safe events selected and ranked */
+  uint32_t reserved[1];
 } gpq_phold_config;
 
 typedef struct gpq_phold_result {

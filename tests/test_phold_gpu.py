@@ -27,6 +27,8 @@ def _oracle_cached(cfgd):
 
 
 def _run(cfgd, **kw):
+    if kw.get("queue") == "laqs":  # the local array queue's selection form
+        kw = dict(kw, queue="laq", laq_mode=1)
     cfg = G.make_phold_config(**cfgd, **kw)
     with G.Phold(cfg) as h:
         h.populate()
@@ -37,8 +39,7 @@ def _run(cfgd, **kw):
 
 
 def _assert_same(r, s, o, check_steps=True):
-    """Bit-exact outputs.  The window count is compared too, except for the parallel heap,
-    whose root takes at most one node (r items) per window and so may need more windows."""
+    """Bit-exact outputs, window count included."""
     assert r["status_code"] == 0, r
     assert np.array_equal(s["count"], o["count"])
     assert np.array_equal(s["csum"], o["csum"])
@@ -63,8 +64,8 @@ def test_children_match_oracle(gpu_lib):
     assert np.array_equal(ch["id"], ev["id"])
 
 
-QUEUE_SHAPES = [("laq", 4), ("laq", 8), ("laq", 16), ("laq", 32), ("lhq", 1), ("lhq", 8), ("lhq", 32), ("lsq", 1),
-                ("gaq", 8), ("hq", 8)]
+QUEUE_SHAPES = [("laq", 4), ("laq", 8), ("laq", 16), ("laq", 32), ("laqs", 4), ("laqs", 8), ("laqs", 32), ("lhq", 1),
+                ("lhq", 8), ("lhq", 32), ("lsq", 1), ("gaq", 8), ("hq", 8)]
 
 
 @pytest.mark.parametrize("loop", ["plain", "persistent"])
@@ -88,8 +89,8 @@ def test_phold_heap_queue_node_sizes(gpu_lib, node_size):
 
 @pytest.mark.parametrize("queue,loop,lanes,block", [
     ("laq", "plain", 8, 256), ("laq", "persistent", 4, 128), ("laq", "persistent", 8, 256),
-    ("laq", "persistent", 16, 512), ("laq", "persistent", 32, 256),
-    ("lhq", "persistent", 8, 128), ("lhq", "plain", 4, 256), ("lsq", "persistent", 1, 128), ("lsq", "plain", 1, 256),
+    ("laq", "persistent", 16, 512), ("laq", "persistent", 32, 256), ("laqs", "persistent", 8, 128),
+    ("laqs", "plain", 16, 256), ("lhq", "persistent", 8, 128), ("lhq", "plain", 4, 256), ("lsq", "persistent", 1, 128), ("lsq", "plain", 1, 256),
     ("gaq", "plain", 8, 256), ("hq", "persistent", 8, 256)])
 def test_phold_large_reduced_bit_exact(gpu_lib, queue, loop, lanes, block):
     """The 65,536-LP ring workload cut to end time 3 (checked by the threaded oracle)."""
@@ -114,7 +115,8 @@ def test_phold_large_reduced_bit_exact(gpu_lib, queue, loop, lanes, block):
      dict(capacity=256, insert_capacity=256)),
 ])
 @pytest.mark.parametrize("queue,loop,lanes", [("laq", "plain", 32), ("laq", "persistent", 4), ("laq", "persistent", 8),
-                                              ("laq", "persistent", 32), ("lhq", "persistent", 8), ("lhq", "plain", 1),
+                                              ("laq", "persistent", 32), ("laqs", "persistent", 8), ("laqs", "plain", 32),
+                                              ("laqs", "persistent", 4), ("lhq", "persistent", 8), ("lhq", "plain", 1),
                                               ("lsq", "persistent", 1), ("lsq", "plain", 1), ("gaq", "plain", 8),
                                               ("hq", "persistent", 8)])
 def test_phold_edge_shapes(gpu_lib, cfgd, kw, queue, loop, lanes):
@@ -152,7 +154,7 @@ def test_step_api_resumes(gpu_lib):
     assert n > 10
 
 
-@pytest.mark.parametrize("queue", ["laq", "lhq", "lsq"])
+@pytest.mark.parametrize("queue", ["laq", "laqs", "lhq", "lsq"])
 def test_queue_overflow_reported(gpu_lib, queue):
     # per-LP capacity 32 with 32 initial events: the first child overflows the queue
     cfgd = dict(num_lps=16, events_per_lp=32, lookahead=0.01, end_time=50.0, seed=3, dest_mode=0)
