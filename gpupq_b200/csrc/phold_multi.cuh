@@ -163,7 +163,7 @@ __device__ __forceinline__ void pm_lp_window(const PmDev& d, uint32_t lp, uint32
 // Windows s0, s0 + 1, ... while some instance is running, at most step_windows of them
 // (0 = no limit).  Dynamic shared memory: laq_group_smem_bytes(ibc, G) per lane group.
 template <int G>
-static __global__ void __launch_bounds__(256) pm_persistent_kernel(PmDev d, uint32_t s0, uint32_t step_windows) {
+static __global__ void __launch_bounds__(256, 4) pm_persistent_kernel(PmDev d, uint32_t s0, uint32_t step_windows) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int s_any;
   const LaneGroup<G> g;
