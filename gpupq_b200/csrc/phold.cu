@@ -15,6 +15,7 @@
 #include "gaq.cuh"
 #include "gaq_engine.h"
 #include "hq_kernels.cuh"
+#include "lab.cuh"
 #include "phold_kernels.cuh"
 
 namespace {
@@ -105,7 +106,13 @@ struct gpq_phold {
   uint32_t* hq_mm = nullptr;
   uint64_t hq_windows = 0;
   bool is_hq = false;
-  size_t window_smem() const { return phold_window_smem_bytes(block, ks.group, ks.group_smem); }
+  // bucketed local array queue (queue_kind == GPQ_QUEUE_LAQ, laq_mode 2)
+  LabDev lab{};
+  LabKernelSet lks{};
+  bool is_lab = false;
+  size_t window_smem() const {
+    return is_lab ? lab_cta_smem_bytes(block) : phold_window_smem_bytes(block, ks.group, ks.group_smem);
+  }
 
   ~gpq_phold() {
     for (void* p : {(void*)items, (void*)qa, (void*)qb, (void*)qc, (void*)links, (void*)freestk, (void*)ibuf,
@@ -114,7 +121,8 @@ struct gpq_phold {
     if (h_ctrl) cudaFreeHost(h_ctrl);
     if (gaq) gpq::gaq_engine_destroy(gaq);
     for (void* p : {(void*)hq.nodes, (void*)hq.cnt, (void*)hq.meta, (void*)hq_sort[0], (void*)hq_sort[1],
-                    (void*)hq_hist, (void*)hq_mm})
+                    (void*)hq_hist, (void*)hq_mm, (void*)lab.keys, (void*)lab.cnt, (void*)lab.spill,
+                    (void*)lab.scnt, (void*)lab.wj})
       if (p) cudaFree(p);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -180,6 +188,22 @@ gpq_status gpq_phold_create(const gpq_phold_config* cfg_in, gpq_phold** out) {
     TRY(cudaMalloc(&h->hq_hist, gpq::radix_hist_words((uint32_t)N) * sizeof(uint32_t)));
     TRY(cudaMalloc(&h->hq_mm, 2 * sizeof(uint32_t)));
     TRY(cudaFuncSetAttribute(hq_phold_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hq_smem_bytes(r)));
+  } else if (c.queue_kind == GPQ_QUEUE_LAQ && c.laq_mode == 2) {
+    gpq::LabGeometry geo{};
+    const gpq_status gs = gpq::lab_geometry(c, &geo);
+    if (gs != GPQ_OK) return fail(gs);
+    if (!lab_kernel_set(c.lanes_per_lp, &h->lks)) return fail(GPQ_ERR_INVALID);
+    h->is_lab = true;
+    LabDev& q = h->lab;
+    q.nb_log2 = geo.nb_log2;
+    q.c_log2 = geo.c_log2;
+    q.F = geo.spill;
+    q.inv_w = geo.inv_w;
+    TRY(cudaMalloc(&q.keys, (L << (q.nb_log2 + q.c_log2)) * sizeof(unsigned long long)));
+    TRY(cudaMalloc(&q.cnt, (L << q.nb_log2) * sizeof(uint32_t)));
+    TRY(cudaMalloc(&q.spill, 2 * L * q.F * sizeof(unsigned long long)));
+    TRY(cudaMalloc(&q.scnt, 2 * L * sizeof(uint32_t)));
+    TRY(cudaMalloc(&q.wj, 4 * sizeof(uint32_t)));
   } else if (c.queue_kind != GPQ_QUEUE_GAQ) {
     TRY(cudaMalloc(&h->items, (L << h->cap_log2) * sizeof(gpq_item)));
     TRY(cudaMalloc(&h->qa, L * sizeof(uint32_t)));
@@ -190,8 +214,10 @@ gpq_status gpq_phold_create(const gpq_phold_config* cfg_in, gpq_phold** out) {
     TRY(cudaMalloc(&h->links, (L << h->cap_log2) * sizeof(uint32_t)));
     TRY(cudaMalloc(&h->freestk, (L << h->cap_log2) * sizeof(uint16_t)));
   }
-  TRY(cudaMalloc(&h->ibuf, 2 * L * c.insert_capacity * sizeof(gpq_item)));
-  TRY(cudaMalloc(&h->icnt, 2 * L * sizeof(uint32_t)));
+  if (!h->is_lab) {
+    TRY(cudaMalloc(&h->ibuf, 2 * L * c.insert_capacity * sizeof(gpq_item)));
+    TRY(cudaMalloc(&h->icnt, 2 * L * sizeof(uint32_t)));
+  }
   TRY(cudaMalloc(&h->count, L * sizeof(uint32_t)));
   TRY(cudaMalloc(&h->csum, L * sizeof(unsigned long long)));
   TRY(cudaMalloc(&h->ohash, L * sizeof(unsigned long long)));
@@ -208,7 +234,14 @@ gpq_status gpq_phold_create(const gpq_phold_config* cfg_in, gpq_phold** out) {
     *out = h;
     return GPQ_OK;
   }
-  if (!phold_kernel_set(c.queue_kind, c.lanes_per_lp, c.insert_capacity, &h->ks, c.laq_mode)) return fail(GPQ_ERR_INVALID);
+  if (h->is_lab) {
+    h->ks.group = c.lanes_per_lp;
+    h->ks.group_smem = lab_group_smem_bytes();
+    h->ks.window = h->lks.window;
+    h->ks.persistent = h->lks.persistent;
+  } else if (!phold_kernel_set(c.queue_kind, c.lanes_per_lp, c.insert_capacity, &h->ks, c.laq_mode)) {
+    return fail(GPQ_ERR_INVALID);
+  }
   if (!gpq::fit_block_to_smem(&h->block, h->ks.group, h->ks.group_smem + 24 * kStageRounds,
                               200 * 1024 - 2048 * 16 - 16)) {
     gpq::set_last_error("insert_capacity %u needs too much shared memory per lane group", c.insert_capacity);
@@ -252,7 +285,7 @@ gpq_status gpq_phold_populate(gpq_phold* h, const gpq_item* initial, uint64_t n,
   for (int i = 0; i < 3; ++i) { init.mins[i] = kInfBits; init.errs[i] = 0; }
   *h->h_ctrl = init;
   GPQ_CUDA_TRY(cudaMemcpyAsync(h->ctrl, h->h_ctrl, sizeof(PholdCtrl), cudaMemcpyHostToDevice, st));
-  GPQ_CUDA_TRY(cudaMemsetAsync(h->icnt, 0, 2 * L * sizeof(uint32_t), st));
+  if (h->icnt) GPQ_CUDA_TRY(cudaMemsetAsync(h->icnt, 0, 2 * L * sizeof(uint32_t), st));
   h->phase = 0;
   h->gaq_windows = 0;
   h->hq_windows = 0;
@@ -295,6 +328,23 @@ gpq_status gpq_phold_populate(gpq_phold* h, const gpq_item* initial, uint64_t n,
     h->elapsed_ms = 0.f;
     return GPQ_OK;
   }
+  if (h->is_lab) {
+    // every key slot starts all ones (never written: not live)
+    const LabDev& q = h->lab;
+    GPQ_CUDA_TRY(cudaMemsetAsync(q.keys, 0xff, (L << (q.nb_log2 + q.c_log2)) * sizeof(unsigned long long), st));
+    GPQ_CUDA_TRY(cudaMemsetAsync(q.cnt, 0, (L << q.nb_log2) * sizeof(uint32_t), st));
+    GPQ_CUDA_TRY(cudaMemsetAsync(q.scnt, 0, 2 * L * sizeof(uint32_t), st));
+    GPQ_CUDA_TRY(cudaMemsetAsync(q.wj, 0, 4 * sizeof(uint32_t), st));
+    const uint64_t n_ev = (uint64_t)L * c.events_per_lp;
+    const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((n_ev + 255) / 256, 8192));
+    lab_populate_kernel<<<grid, 256, 0, st>>>(h->dev(), q, c.events_per_lp, src);
+    GPQ_CUDA_TRY(cudaGetLastError());
+    h->phase = 0;
+    h->populated = true;
+    h->finalized = false;
+    h->elapsed_ms = 0.f;
+    return GPQ_OK;
+  }
   const uint32_t wpb = 4;
   const size_t smem = (size_t)wpb * c.events_per_lp * (sizeof(gpq_item) + sizeof(uint64_t));
   GPQ_CUDA_TRY(cudaFuncSetAttribute(phold_populate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -310,7 +360,7 @@ gpq_status gpq_phold_populate(gpq_phold* h, const gpq_item* initial, uint64_t n,
 
 static gpq_status run_plain(gpq_phold* h, uint32_t nsteps, int* done, cudaStream_t st) {
   const gpq_phold_config& c = h->cfg;
-  const uint32_t gpb = h->block / h->ks.group;
+  const uint32_t gpb = h->is_lab ? lab_plain_lps_per_cta(h->block) : h->block / h->ks.group;  // LPs per CTA
   const uint32_t grid = (uint32_t)((c.num_lps + gpb - 1) / gpb);
   const size_t smem = h->window_smem();
   PholdDev d = h->dev();
@@ -331,7 +381,8 @@ static gpq_status run_plain(gpq_phold* h, uint32_t nsteps, int* done, cudaStream
     }
     uint32_t phase = h->phase;
     void* args[] = {&d, &q, &ib, &phase};
-    GPQ_CUDA_TRY(cudaLaunchKernel(h->ks.window, dim3(grid), dim3(h->block), args, smem, st));
+    void* lab_args[] = {&d, &h->lab, &phase};
+    GPQ_CUDA_TRY(cudaLaunchKernel(h->ks.window, dim3(grid), dim3(h->block), h->is_lab ? lab_args : args, smem, st));
     ++h->phase;
     ++executed;
   }
@@ -361,7 +412,7 @@ static gpq_status run_persistent(gpq_phold* h, cudaStream_t st) {
   }
   if (c.ctas_per_sm) per_sm = std::min<int>(per_sm, (int)c.ctas_per_sm);
   uint32_t grid = (uint32_t)(per_sm * h->num_sms);
-  const uint32_t gpb = h->block / h->ks.group;
+  const uint32_t gpb = h->is_lab ? 1u : h->block / h->ks.group;  // LPs per CTA at least
   const uint32_t need = (uint32_t)((c.num_lps + gpb - 1) / gpb);
   grid = std::min(grid, std::max(need, 1u));
   GPQ_CUDA_TRY(cudaMemsetAsync(&h->ctrl->bar, 0, sizeof(unsigned long long), st));
@@ -372,7 +423,9 @@ static gpq_status run_persistent(gpq_phold* h, cudaStream_t st) {
   uint32_t maxs = c.max_steps ? (c.max_steps > s0 ? c.max_steps - s0 : 0) : 0;
   if (c.max_steps && maxs == 0) return GPQ_OK;
   void* args[] = {&d, &q, &ib, &s0, &maxs};
-  GPQ_CUDA_TRY(cudaLaunchCooperativeKernel(h->ks.persistent, dim3(grid), dim3(h->block), args, smem, st));
+  void* lab_args[] = {&d, &h->lab, &s0, &maxs};
+  GPQ_CUDA_TRY(cudaLaunchCooperativeKernel(h->ks.persistent, dim3(grid), dim3(h->block), h->is_lab ? lab_args : args,
+                                           smem, st));
   h->last_grid = grid;
   return GPQ_OK;
 }
@@ -476,7 +529,8 @@ gpq_status gpq_phold_result_get(gpq_phold* h, gpq_phold_result* out, void* strea
   GPQ_CUDA_TRY(cudaMemcpyAsync(h->acc, &a, sizeof(PholdAcc), cudaMemcpyHostToDevice, st));
   const uint32_t wpb = 8;
   const uint32_t grid = std::max(1u, std::min<uint32_t>((h->cfg.num_lps + wpb - 1) / wpb, 4096u));
-  phold_finalize_kernel<<<grid, wpb * 32, 0, st>>>(h->dev(), h->lq(), h->ins(), h->acc);
+  if (h->is_lab) lab_finalize_kernel<<<grid, wpb * 32, 0, st>>>(h->dev(), h->lab, h->acc);
+  else phold_finalize_kernel<<<grid, wpb * 32, 0, st>>>(h->dev(), h->lq(), h->ins(), h->acc);
   GPQ_CUDA_TRY(cudaGetLastError());
   GPQ_CUDA_TRY(cudaMemcpyAsync(&a, h->acc, sizeof(PholdAcc), cudaMemcpyDeviceToHost, st));
   GPQ_CUDA_TRY(cudaMemcpyAsync(h->h_ctrl, h->ctrl, sizeof(PholdCtrl), cudaMemcpyDeviceToHost, st));

@@ -1,6 +1,9 @@
 // Host-side PHOLD configuration helpers shared by the engine entry points.
 #pragma once
 
+#include <algorithm>
+#include <cmath>
+
 #include "host_common.h"
 
 namespace gpq {
@@ -33,8 +36,49 @@ inline gpq_status validate_phold_config(const gpq_phold_config* c) {
     GPQ_CHECK_ARG(c->ring_width >= 1 && 2ull * c->ring_width < c->num_lps, "ring_width must satisfy 1 <= 2w < num_lps");
   GPQ_CHECK_ARG(c->loop_mode == GPQ_LOOP_PLAIN || c->loop_mode == GPQ_LOOP_PERSISTENT, "loop_mode");
   GPQ_CHECK_ARG(c->queue_kind <= GPQ_QUEUE_LSQ, "queue_kind");
-  GPQ_CHECK_ARG(c->laq_mode <= 1 && (c->laq_mode == 0 || c->queue_kind == GPQ_QUEUE_LAQ),
-                "laq_mode must be 0, or 1 with the local array queue");
+  GPQ_CHECK_ARG(c->laq_mode <= 2 && (c->laq_mode == 0 || c->queue_kind == GPQ_QUEUE_LAQ),
+                "laq_mode must be 0, or 1 or 2 with the local array queue");
+  return GPQ_OK;
+}
+
+// Geometry of the bucketed local array queue (laq_mode 2): bucket width w chosen so that
+// about 6 events sit in the front bucket of an LP (the pending events of an LP spread over
+// about lookahead + 1 time units, the mean increment), but at least lookahead / 2.5 so
+// that a window spans at most 4 buckets; NB buckets (a power of two) covering
+// lookahead + 7 time units ahead of the window minimum (an increment beyond lookahead + 7
+// has probability e^-7) and at least lookahead / w + 4 buckets, so that one window's
+// bucket range never wraps; C slots per bucket, twice the expected front occupancy plus
+// 4; spill lists of max(64, C) events.
+struct LabGeometry {
+  uint32_t nb_log2, c_log2, spill;
+  float inv_w;
+};
+
+inline uint32_t next_pow2(double x) {
+  uint32_t p = 1;
+  while ((double)p < x && p < (1u << 30)) p <<= 1;
+  return p;
+}
+
+inline gpq_status lab_geometry(const gpq_phold_config& c, LabGeometry* g) {
+  const double la = c.lookahead, E = c.events_per_lp;
+  double w = std::max(6.0 * (la + 1.0) / E, la / 2.5);
+  double need = std::max(std::ceil((la + 7.0) / w), std::ceil(la / w) + 4.0);
+  if (need > 1024.0) {
+    w = std::max((la + 7.0) / 1024.0, la / 1020.0);
+    need = 1024.0;
+  }
+  const uint32_t nb = std::max(16u, next_pow2(need));
+  const double occ = E * w / (la + 1.0);
+  const uint32_t cs = std::min(1024u, std::max(16u, next_pow2(std::ceil(2.0 * occ + 4.0))));
+  g->nb_log2 = ilog2_ceil(nb);
+  g->c_log2 = ilog2_ceil(cs);
+  g->spill = std::max(64u, cs);
+  g->inv_w = (float)(1.0 / w);
+  GPQ_CHECK_ARG((double)c.lookahead * g->inv_w + 3.0 <= (double)nb,
+                "bucketed local array queue: lookahead too wide for the bucket ring");
+  GPQ_CHECK_ARG(((double)c.end_time + la + 20.0) * g->inv_w < 2147483648.0,
+                "bucketed local array queue: end_time too large for the bucket width");
   return GPQ_OK;
 }
 

@@ -167,7 +167,10 @@ typedef struct gpq_phold_config {
   uint32_t lanes_per_lp;    /* LAQ: lanes that work on one LP (4, 8, 16 or 32); 0 = tuned default */
   uint32_t node_size;       /* HQ: items per heap node r (power of two <= 1024); 0 = 1024 */
   uint32_t laq_mode;        /* LAQ: 0 = sorted runs, children merged each window; 1 = unordered
-                               arrays, each window's safe events selected and ranked */
+                               arrays, each window's safe events selected and ranked; 2 = time
+                               buckets of 8-byte keys per LP, each window's buckets ranked
+                               (bucket geometry from lookahead and events_per_lp; capacity and
+                               insert_capacity unused) */
   uint32_t reserved[1];
 } gpq_phold_config;
 

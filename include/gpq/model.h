@@ -179,8 +179,10 @@ GPQ_HD uint32_t gpq_phold_dest(const gpq_phold_params p, uint32_t lp, uint64_t r
     uint32_t w = p.ring_width;
     uint32_t k = gpq_uniform_below(r, 2u * w);            /* [0, 2w) */
     int32_t off = (k < w) ? (int32_t)k - (int32_t)w : (int32_t)k - (int32_t)w + 1;
-    int64_t d = ((int64_t)lp + off) % (int64_t)p.num_lps;
+    /* (lp + off) mod num_lps; 2w < num_lps, so one correction step is exact */
+    int64_t d = (int64_t)lp + off;
     if (d < 0) d += p.num_lps;
+    else if (d >= (int64_t)p.num_lps) d -= p.num_lps;
     return (uint32_t)d;
   }
   return gpq_uniform_below(r, p.num_lps);

@@ -29,6 +29,8 @@ def _oracle_cached(cfgd):
 def _run(cfgd, **kw):
     if kw.get("queue") == "laqs":  # the local array queue's selection form
         kw = dict(kw, queue="laq", laq_mode=1)
+    if kw.get("queue") == "laqb":  # the local array queue's bucketed form
+        kw = dict(kw, queue="laq", laq_mode=2)
     cfg = G.make_phold_config(**cfgd, **kw)
     with G.Phold(cfg) as h:
         h.populate()
@@ -64,7 +66,8 @@ def test_children_match_oracle(gpu_lib):
     assert np.array_equal(ch["id"], ev["id"])
 
 
-QUEUE_SHAPES = [("laq", 4), ("laq", 8), ("laq", 16), ("laq", 32), ("laqs", 4), ("laqs", 8), ("laqs", 32), ("lhq", 1),
+QUEUE_SHAPES = [("laq", 4), ("laq", 8), ("laq", 16), ("laq", 32), ("laqs", 4), ("laqs", 8), ("laqs", 32), ("laqb", 4),
+                ("laqb", 8), ("laqb", 16), ("laqb", 32), ("lhq", 1),
                 ("lhq", 8), ("lhq", 32), ("lsq", 1), ("gaq", 8), ("hq", 8)]
 
 
@@ -90,7 +93,8 @@ def test_phold_heap_queue_node_sizes(gpu_lib, node_size):
 @pytest.mark.parametrize("queue,loop,lanes,block", [
     ("laq", "plain", 8, 256), ("laq", "persistent", 4, 128), ("laq", "persistent", 8, 256),
     ("laq", "persistent", 16, 512), ("laq", "persistent", 32, 256), ("laqs", "persistent", 8, 128),
-    ("laqs", "plain", 16, 256), ("lhq", "persistent", 8, 128), ("lhq", "plain", 4, 256), ("lsq", "persistent", 1, 128), ("lsq", "plain", 1, 256),
+    ("laqs", "plain", 16, 256), ("laqb", "persistent", 4, 128), ("laqb", "persistent", 8, 128),
+    ("laqb", "persistent", 16, 256), ("laqb", "plain", 8, 256), ("lhq", "persistent", 8, 128), ("lhq", "plain", 4, 256), ("lsq", "persistent", 1, 128), ("lsq", "plain", 1, 256),
     ("gaq", "plain", 8, 256), ("hq", "persistent", 8, 256)])
 def test_phold_large_reduced_bit_exact(gpu_lib, queue, loop, lanes, block):
     """The 65,536-LP ring workload cut to end time 3 (checked by the threaded oracle)."""
@@ -116,7 +120,9 @@ def test_phold_large_reduced_bit_exact(gpu_lib, queue, loop, lanes, block):
 ])
 @pytest.mark.parametrize("queue,loop,lanes", [("laq", "plain", 32), ("laq", "persistent", 4), ("laq", "persistent", 8),
                                               ("laq", "persistent", 32), ("laqs", "persistent", 8), ("laqs", "plain", 32),
-                                              ("laqs", "persistent", 4), ("lhq", "persistent", 8), ("lhq", "plain", 1),
+                                              ("laqs", "persistent", 4), ("laqb", "persistent", 4),
+                                              ("laqb", "persistent", 8), ("laqb", "plain", 32), ("laqb", "persistent", 32),
+                                              ("lhq", "persistent", 8), ("lhq", "plain", 1),
                                               ("lsq", "persistent", 1), ("lsq", "plain", 1), ("gaq", "plain", 8),
                                               ("hq", "persistent", 8)])
 def test_phold_edge_shapes(gpu_lib, cfgd, kw, queue, loop, lanes):
@@ -125,8 +131,9 @@ def test_phold_edge_shapes(gpu_lib, cfgd, kw, queue, loop, lanes):
     _assert_same(r, s, o)
 
 
-def test_host_initial_events_path(gpu_lib):
-    cfg = G.make_phold_config(**C1)
+@pytest.mark.parametrize("laq_mode", [0, 2])
+def test_host_initial_events_path(gpu_lib, laq_mode):
+    cfg = G.make_phold_config(**C1, laq_mode=laq_mode)
     ev = G.initial_events(cfg)
     with G.Phold(cfg) as h:
         h.populate(ev)
@@ -138,8 +145,9 @@ def test_host_initial_events_path(gpu_lib):
     assert r1["digest"] == r2["digest"] and r1["committed"] == r2["committed"] == 820705
 
 
-def test_step_api_resumes(gpu_lib):
-    cfg = G.make_phold_config(**C1, loop="plain")
+@pytest.mark.parametrize("laq_mode", [0, 2])
+def test_step_api_resumes(gpu_lib, laq_mode):
+    cfg = G.make_phold_config(**C1, loop="plain", laq_mode=laq_mode)
     o = _oracle(C1)
     with G.Phold(cfg) as h:
         h.populate()
@@ -160,3 +168,33 @@ def test_queue_overflow_reported(gpu_lib, queue):
     cfgd = dict(num_lps=16, events_per_lp=32, lookahead=0.01, end_time=50.0, seed=3, dest_mode=0)
     r, _ = _run(cfgd, queue=queue, capacity=32, insert_capacity=64)
     assert r["status_code"] in (3, 4)
+
+
+@pytest.mark.parametrize("shift", ["all", "half", "far"])
+def test_bucketed_form_matches_sorted_form_on_shifted_starts(gpu_lib, shift):
+    """Host-provided initial events with a late start (the minimum jumps over every bucket
+    before window 0), half the LPs starting late, or some events beyond the bucket horizon
+    (they wait in the spill lists): the bucketed form equals the sorted form bit for bit."""
+    cfgd = dict(num_lps=64, events_per_lp=16, lookahead=0.25, end_time=80.0, seed=5, dest_mode=1, ring_width=3)
+    ev = G.initial_events(G.make_phold_config(**cfgd))
+    if shift == "all":
+        ev["ts"] += np.float32(30.0)
+    elif shift == "half":
+        ev["ts"][ev["lp"] >= 32] += np.float32(30.0)
+    else:
+        ev["ts"][ev["id"] % 5 == 0] += np.float32(45.0)
+    out = []
+    for mode, loop in ((0, "persistent"), (2, "persistent"), (2, "plain")):
+        with G.Phold(G.make_phold_config(**cfgd, laq_mode=mode, loop=loop)) as h:
+            h.populate(ev)
+            h.run()
+            r = h.result()
+            s = h.lp_stats()
+        assert r["status_code"] == 0, (mode, loop, r)
+        out.append((r, s))
+    (r0, s0) = out[0]
+    for r, s in out[1:]:
+        for k in ("committed", "pending", "pending_csum", "digest", "steps"):
+            assert r[k] == r0[k], k
+        for k in ("count", "csum", "ohash"):
+            assert np.array_equal(s[k], s0[k]), k
