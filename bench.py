@@ -1,6 +1,10 @@
 #!/usr/bin/env python
 """Benchmark: PHOLD committed events/s on the 65,536-LP ring workload (local array queue).
 
+The local array queue runs in the form the shipped tuned shape names: the bucketed form
+(per-LP time buckets of 8-byte keys, laq_mode 2) on the B200; `--laq-mode 0` selects the
+sorted form (per-LP sorted rings, children merged every window).
+
 Workload (synthetic, seeded): 65,536 LPs x 64 initial events, lookahead 0.1 + Exp(1)
 float32 increments, 90% of destinations uniform within +-16 ring neighbours (self
 excluded) and 10% uniform, end time 1000.0, per-LP capacity 256, seed 7.
@@ -8,7 +12,8 @@ One bench step = one complete run of that workload: populate the queues on the d
 then drain safe windows until the minimum timestamp reaches the end time.
 
   value  committed events / device time of the runs (CUDA events on the launching
-         stream, inputs already resident in HBM; the 268 MB queue array exceeds L2)
+         stream, inputs already resident in HBM; the queue arrays exceed L2: 1.07 GB
+         of buckets in the bucketed form, 268 MB of rings in the sorted form)
   e2e    the same through the public C ABI with host buffers: per step the initial
          events are copied from page-locked host memory, and the per-LP results
          (count, checksum, order hash) are copied back
@@ -349,6 +354,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--queue", default="laq")
     ap.add_argument("--loop", default="persistent", choices=["persistent", "plain"])
+    ap.add_argument("--laq-mode", type=int, default=None, choices=[0, 1, 2],
+                    help="local array queue form (default: the tuned shape's)")
     ap.add_argument("--end-time", type=float, default=None, help="override the workload end time (debug)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -389,6 +396,15 @@ def main():
         from gpupq_b200 import autotune
         shape = autotune.tune_phold(dict(cfgd, capacity=256), queue=args.queue, loop=args.loop,
                                     windows=args.tune_windows, force=args.retune)
+    if args.laq_mode is not None:
+        if shape.get("laq_mode", 0) != args.laq_mode:
+            shape = {"laq_mode": args.laq_mode}
+            if args.laq_mode == 0:
+                shape.update(lanes_per_lp=8, block_threads=128, insert_capacity=32)
+            else:
+                shape.update(block_threads=256)
+    laq_mode = shape.get("laq_mode", 0) if args.queue == "laq" else 0
+    form = {0: "", 1: "s", 2: "b"}[laq_mode]
     cfg = G.make_phold_config(**cfgd, queue=args.queue, capacity=256, loop=args.loop,
                               **dict({"insert_capacity": 64}, **shape))
     h = G.Phold(cfg)
@@ -450,7 +466,7 @@ def main():
     if os.path.exists(tp):
         try:
             t = json.load(open(tp))
-            key = f"{args.queue}_{args.loop}"
+            key = f"{args.queue}{form}_{args.loop}"
             if key in t:
                 traffic = t[key]["dram_bytes_per_event"] * committed / args.steps
         except Exception:
@@ -512,12 +528,15 @@ def main():
             "config": {"workload": WORKLOAD_NAME, "queue": args.queue, "loop": args.loop,
                        "end_time": cfgd["end_time"], "events_per_run": committed / args.steps,
                        "windows_per_run": windows / args.steps,
-                       "l2": "inputs larger than L2 (268 MB queue array)",
+                       "laq_form": {0: "sorted rings", 1: "selection", 2: "time buckets"}[laq_mode]
+                       if args.queue == "laq" else None,
+                       "l2": ("inputs larger than L2 (1.07 GB bucket array)" if laq_mode == 2
+                              else "inputs larger than L2 (268 MB queue array)"),
                        "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU",
                        "launch_shape": dict(shape, block_threads=info["block"], grid=info["grid"])},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "peak_source": f"{peak_kind} hbm_gbs", "kernel": f"phold_laq_{args.loop}",
+                         "peak_source": f"{peak_kind} hbm_gbs", "kernel": ("lab_" if laq_mode == 2 else "phold_laq_") + args.loop,
                          "algorithmic_bytes_per_run": per_run_bytes},
             "cpu_baseline": cpu,
             "e2e": e2e,

@@ -1,7 +1,9 @@
 """Autotuner for the PHOLD engine's launch shape.
 
 For a workload class it times candidate (lanes_per_lp, block_threads, ctas_per_sm,
-insert_capacity) settings on the first `windows` safe windows of the real workload
+insert_capacity) settings -- and, for the local array queue, its sorted and bucketed
+forms (laq_mode 0 and 2; the bucketed form ignores lanes_per_lp and insert_capacity, so
+only its CTA size is varied) -- on the first `windows` safe windows of the real workload
 (same seed, same queues), rejects candidates that overflow or disagree with the others
 (every candidate runs the same windows, so committed count and digest must match), and
 keeps the fastest.  Results are cached in a JSON file keyed by GPU name and workload
@@ -74,14 +76,20 @@ def tune_phold(cfgd, queue="laq", loop="persistent", windows=200, space=None, ca
     shipped = _load(SHIPPED)
     if not force and key in shipped:
         return dict(shipped[key]["best"])
-    space = dict(DEFAULT_SPACE, **(space or {}))
+    space = dict(DEFAULT_SPACE, **({"laq_mode": [0, 2]} if queue == "laq" else {}), **(space or {}))
     names = list(space.keys())
     results = []
     ref = None
+    seen = set()
     for values in itertools.product(*[space[n] for n in names]):
         shape = dict(zip(names, values))
         if shape["block_threads"] < shape["lanes_per_lp"]:
             continue
+        if shape.get("laq_mode") == 2:  # the bucketed form: only the CTA size matters
+            shape.update(lanes_per_lp=8, insert_capacity=64, ctas_per_sm=0)
+            if tuple(sorted(shape.items())) in seen:
+                continue
+            seen.add(tuple(sorted(shape.items())))
         try:
             cfg = make_phold_config(**cfgd, queue=queue, loop=loop, max_steps=windows, **shape)
             with Phold(cfg) as h:
