@@ -24,7 +24,7 @@ SHIPPED = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned_shapes
 
 DEFAULT_SPACE = {
     "lanes_per_lp": [8, 16, 32],
-    "block_threads": [64, 128, 256],
+    "block_threads": [64, 128, 256, 512],
     "ctas_per_sm": [0],
     "insert_capacity": [32, 64],
 }

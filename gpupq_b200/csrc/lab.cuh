@@ -392,13 +392,16 @@ __device__ uint32_t lab_lp_stage(const PholdDev& d, const LabDev& q, uint32_t lp
 static constexpr uint32_t kLabWarpLps = 16;    // LPs per warp chunk
 static constexpr uint32_t kLabSegMax = 5;      // candidate sources per LP on the common path
 static constexpr uint32_t kLabCandCap = 256;   // candidate keys per warp chunk on the common path
-static constexpr uint32_t kLabStageCap = 128;  // staged events per warp chunk
+static constexpr uint32_t kLabStageCap = 128;  // staged events per warp chunk (4-byte entries)
+static constexpr uint32_t kLabSafePerLp = 32;  // safe keys of one LP ranked on the common path
+static constexpr uint32_t kLabItemStageCap = kLabStageCap * 4 / 16;  // staged items on the general path
 
 struct LabWarpSmem {
   unsigned long long* ls_csum;   // [kLabWarpLps] LP checksum
   unsigned long long* ls_ohash;  // [kLabWarpLps] LP order-sensitive hash
   unsigned long long* cand;      // [kLabCandCap] candidate keys (general path: the safe-key list)
-  gpq_item* stage;               // [kLabStageCap]
+  uint32_t* cstage;              // [kLabStageCap] staged events: candidate index | rank << 16
+  gpq_item* stage;               // [kLabItemStageCap] staged items on the general path (same bytes as cstage)
   uint32_t* ls_cnt;              // [kLabWarpLps] LP committed count (before the window: the sequence base)
   uint32_t* seg_raw;             // [kLabWarpLps * kLabSegMax] bucket count / spill count as read
   uint32_t* seg_off;             // [kLabWarpLps * kLabSegMax + 1] candidate offsets
@@ -411,13 +414,13 @@ struct LabWarpSmem {
   uint32_t* nx_cnt;              // [kLabWarpLps * 2] counts of the two buckets above j1
   uint32_t* misc;                // [4] staging count
   uint16_t* cseg;                // [kLabCandCap] source of each candidate: lpi << 3 | r
-  uint16_t* crank;               // [kLabCandCap] rank of each safe candidate
+  uint16_t* sidx;                // [kLabWarpLps * kLabSafePerLp] safe candidates of each LP
 };
 
 __host__ __device__ constexpr size_t lab_warp_smem_bytes() {
-  return ((size_t)kLabWarpLps * 16 + (size_t)kLabCandCap * 8 + (size_t)kLabStageCap * 16 +
+  return ((size_t)kLabWarpLps * 16 + (size_t)kLabCandCap * 8 + (size_t)kLabStageCap * 4 +
           (size_t)(kLabWarpLps + 3 * kLabWarpLps * kLabSegMax + 1 + 7 * kLabWarpLps + 1 + 4) * 4 +
-          (size_t)kLabCandCap * 4 + 15) & ~(size_t)15;
+          (size_t)kLabCandCap * 2 + (size_t)kLabWarpLps * kLabSafePerLp * 2 + 15) & ~(size_t)15;
 }
 
 __host__ __device__ inline size_t lab_cta_smem_bytes(uint32_t block) { return (size_t)(block / 32) * lab_warp_smem_bytes(); }
@@ -427,8 +430,9 @@ __device__ __forceinline__ LabWarpSmem lab_warp_smem(unsigned char* base) {
   s.ls_csum = reinterpret_cast<unsigned long long*>(base);
   s.ls_ohash = s.ls_csum + kLabWarpLps;
   s.cand = s.ls_ohash + kLabWarpLps;
-  s.stage = reinterpret_cast<gpq_item*>(s.cand + kLabCandCap);
-  s.ls_cnt = reinterpret_cast<uint32_t*>(s.stage + kLabStageCap);
+  s.cstage = reinterpret_cast<uint32_t*>(s.cand + kLabCandCap);
+  s.stage = reinterpret_cast<gpq_item*>(s.cstage);
+  s.ls_cnt = s.cstage + kLabStageCap;
   s.seg_raw = s.ls_cnt + kLabWarpLps;
   s.seg_off = s.seg_raw + kLabWarpLps * kLabSegMax;
   s.seg_kept = s.seg_off + kLabWarpLps * kLabSegMax + 1;
@@ -440,7 +444,7 @@ __device__ __forceinline__ LabWarpSmem lab_warp_smem(unsigned char* base) {
   s.nx_cnt = s.lp_nmin + kLabWarpLps;
   s.misc = s.nx_cnt + 2 * kLabWarpLps;
   s.cseg = reinterpret_cast<uint16_t*>(s.misc + 4);
-  s.crank = s.cseg + kLabCandCap;
+  s.sidx = s.cseg + kLabCandCap;
   return s;
 }
 
@@ -515,12 +519,14 @@ __device__ __forceinline__ uint32_t lab_scan_above(const LabDev& q, uint32_t lp,
   return found;
 }
 
-// Events x0, x0 + stride, ... (up to four per thread) of the staging area: hashes into the
-// LP accumulators and the children first, then all bucket reservations (independent
-// atomics in flight together), then the stores.  Returns the children's minimum.
+// Events x0, x0 + stride, ... (up to four per thread) of a staging area (`get(x)` returns
+// staged event x, or one whose aux is kStageHole): hashes into the LP accumulators and the
+// children first, then all bucket reservations (independent atomics in flight together),
+// then the stores.  Returns the children's minimum.
+template <class Get>
 __device__ __forceinline__ uint32_t lab_event_batch(const PholdDev& d, const LabDev& q, const PholdStage& st,
                                                     uint32_t ns, uint32_t x0, uint32_t stride, const LabWin& w,
-                                                    uint32_t* err_slot) {
+                                                    uint32_t* err_slot, Get get) {
   constexpr int U = 4;
   const uint32_t nbm = (1u << q.nb_log2) - 1u, C = 1u << q.c_log2;
   unsigned long long key[U];
@@ -531,7 +537,7 @@ __device__ __forceinline__ uint32_t lab_event_batch(const PholdDev& d, const Lab
     const uint32_t x = x0 + (uint32_t)u * stride;
     lp[u] = ~0u;
     if (x < ns) {
-      const gpq_item e = st.ev[x];
+      const gpq_item e = get(x);
       if (e.aux != kStageHole) {
         const uint32_t slot = e.aux >> 16, idx = e.aux & 0xffffu, tb = gpq_f2u(e.ts);
         const uint64_t h = gpq_ev_hash(e.id, tb);
@@ -682,28 +688,32 @@ __device__ uint32_t lab_warp_window(const PholdDev& d, const LabDev& q, const La
       }
     }
     __syncwarp();
-    // P4
+    // P4a (read-only): safe candidates into their LP's list; the minimum and the "stays at
+    // or below j1" flag of each LP
+    for (uint32_t k = lane; k < K; k += 32u) {
+      const uint32_t sg = sm.cseg[k], lpi = sg >> 3, r = sg & 7u;
+      const uint32_t t = (uint32_t)(sm.cand[k] >> 32);
+      if (!lab_live(t, w)) continue;  // dead, or a slot not written yet
+      if (t < w.safe_lim) {
+        const uint32_t p = atomicAdd(&sm.lp_nsafe[lpi], 1u);
+        if (p < kLabSafePerLp) sm.sidx[lpi * kLabSafePerLp + p] = (uint16_t)k;
+        continue;
+      }
+      atomicMin(&sm.lp_rmin[lpi], t);
+      if (r < nr || lab_bucket(t, q.inv_w) <= w.j1) sm.lp_low[lpi] = 1u;
+    }
+    __syncwarp();
+  }
+  const bool common = K <= kLabCandCap && !__any_sync(GPQ_FULL_MASK, lane < n && sm.lp_nsafe[lane] > kLabSafePerLp);
+  if (common) {
+    // P4b: compaction of the buckets below j1 and re-filing of the spill list
     for (uint32_t k = lane; k < K; k += 32u) {
       const uint32_t sg = sm.cseg[k], lpi = sg >> 3, r = sg & 7u;
       const unsigned long long key = sm.cand[k];
       const uint32_t t = (uint32_t)(key >> 32);
-      if (!lab_live(t, w)) continue;  // dead, or a slot not written yet
-      if (t < w.safe_lim) {
-        const uint32_t a = sm.seg_off[lpi * S], b = sm.seg_off[lpi * S + S];
-        uint32_t rank = 0;
-        for (uint32_t x = a; x < b; ++x) {
-          const unsigned long long k2 = sm.cand[x];
-          const uint32_t t2 = (uint32_t)(k2 >> 32);
-          rank += (t2 >= w.mb && t2 < w.safe_lim && k2 < key) ? 1u : 0u;
-        }
-        sm.crank[k] = (uint16_t)rank;
-        atomicAdd(&sm.lp_nsafe[lpi], 1u);
-        continue;
-      }
-      atomicMin(&sm.lp_rmin[lpi], t);
+      if (!lab_live(t, w) || t < w.safe_lim) continue;
       const uint32_t lp = lp0 + lpi;
       if (r < nr) {
-        sm.lp_low[lpi] = 1u;
         if (r + 1u < nr) {  // a bucket below j1: compact (the staying keys keep their order)
           const uint32_t sgi = lpi * S + r, a = sm.seg_off[sgi];
           uint32_t p = 0;
@@ -715,9 +725,7 @@ __device__ uint32_t lab_warp_window(const PholdDev& d, const LabDev& q, const La
           if (p != k - a) q.keys[((((size_t)lp << q.nb_log2) + ((w.j0 + r) & nbm)) << q.c_log2) + p] = key;
         }
       } else {
-        const uint32_t jb = lab_bucket(t, q.inv_w);
-        if (jb <= w.j1) sm.lp_low[lpi] = 1u;
-        lab_push(d, q, lp, key, jb, w, err_slot);
+        lab_push(d, q, lp, key, lab_bucket(t, q.inv_w), w, err_slot);
       }
     }
     __syncwarp();
@@ -734,20 +742,30 @@ __device__ uint32_t lab_warp_window(const PholdDev& d, const LabDev& q, const La
     __syncwarp();
     const uint32_t nsafe = lab_warp_scan(sm.lp_soff, n);
     if (lane == 0) sm.misc[0] = nsafe;
-    // P6: stage the safe events in (LP, rank) order
-    for (uint32_t k = lane; k < K; k += 32u) {
+    // P6: rank each safe key among its LP's safe keys and stage it at (LP offset + rank)
+    for (uint32_t u = lane; u < nsafe; u += 32u) {
+      uint32_t lo = 0, hi = n;  // LP: lp_soff[lo] <= u < lp_soff[lo + 1]
+      while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (sm.lp_soff[mid] <= u) lo = mid; else hi = mid;
+      }
+      const uint16_t* li = sm.sidx + lo * kLabSafePerLp;
+      const uint32_t ns_lp = sm.lp_nsafe[lo];
+      const uint32_t k = li[u - sm.lp_soff[lo]];
       const unsigned long long key = sm.cand[k];
-      const uint32_t t = (uint32_t)(key >> 32);
-      if (!(t >= w.mb && t < w.safe_lim)) continue;
-      const uint32_t lpi = sm.cseg[k] >> 3, rank = sm.crank[k];
-      const uint32_t pos = sm.lp_soff[lpi] + rank;
-      gpq_item e;
-      e.ts = gpq_u2f(t);
-      e.lp = lp0 + lpi;
-      e.id = (uint32_t)key;
-      e.aux = (lpi << 16) | rank;
-      if (pos < kLabStageCap) sm.stage[pos] = e;
-      else mn = min(mn, lab_process_event(d, q, st, e, w, err_slot));
+      uint32_t rank = 0;
+      for (uint32_t x = 0; x < ns_lp; ++x) rank += (sm.cand[li[x]] < key) ? 1u : 0u;
+      const uint32_t pos = sm.lp_soff[lo] + rank;
+      if (pos < kLabStageCap) {
+        sm.cstage[pos] = k | (rank << 16);
+      } else {
+        gpq_item e;
+        e.ts = gpq_u2f((uint32_t)(key >> 32));
+        e.lp = lp0 + lo;
+        e.id = (uint32_t)key;
+        e.aux = (lo << 16) | rank;
+        mn = min(mn, lab_process_event(d, q, st, e, w, err_slot));
+      }
     }
     // next-minimum scan of the LPs with nothing live at or below j1, when one of the two
     // buckets above j1 holds keys: two lanes per LP issue their loads here and use them
@@ -777,6 +795,9 @@ __device__ uint32_t lab_warp_window(const PholdDev& d, const LabDev& q, const La
   } else {
     // general path: the warp as one lane group per LP
     const LaneGroup<32> g;
+    st.cap = kLabItemStageCap;
+    if (lane < n) sm.lp_nsafe[lane] = 0u;
+    __syncwarp();
     for (uint32_t lpi = 0; lpi < n; ++lpi) {
       const uint32_t lp = lp0 + lpi;
       const LabMeta mt = lab_load_meta(d, q, lp, w, g.gl);
@@ -786,9 +807,25 @@ __device__ uint32_t lab_warp_window(const PholdDev& d, const LabDev& q, const La
   }
 
   // P7: events (four in flight per lane), then the next minimum of each LP
-  const uint32_t ns = min(sm.misc[0], kLabStageCap);
-  for (uint32_t x0 = lane; x0 < ns; x0 += 128u) mn = min(mn, lab_event_batch(d, q, st, ns, x0, 32u, w, err_slot));
-  if (K <= kLabCandCap) {
+  if (common) {
+    const uint32_t ns = min(sm.misc[0], kLabStageCap);
+    auto get = [&](uint32_t x) {
+      const uint32_t c = sm.cstage[x], k = c & 0xffffu;
+      const unsigned long long key = sm.cand[k];
+      gpq_item e;
+      e.ts = gpq_u2f((uint32_t)(key >> 32));
+      e.lp = lp0 + (sm.cseg[k] >> 3);
+      e.id = (uint32_t)key;
+      e.aux = ((uint32_t)(sm.cseg[k] >> 3) << 16) | (c >> 16);
+      return e;
+    };
+    for (uint32_t x0 = lane; x0 < ns; x0 += 128u) mn = min(mn, lab_event_batch(d, q, st, ns, x0, 32u, w, err_slot, get));
+  } else {
+    const uint32_t ns = min(sm.misc[0], kLabItemStageCap);
+    auto get = [&](uint32_t x) { return sm.stage[x]; };
+    for (uint32_t x0 = lane; x0 < ns; x0 += 128u) mn = min(mn, lab_event_batch(d, q, st, ns, x0, 32u, w, err_slot, get));
+  }
+  if (common) {
     if (scan_lpi != ~0u && scan_min != kInfBits) atomicMin(&sm.lp_nmin[scan_lpi], scan_min);
     __syncwarp();
     bool deep = false;
@@ -841,7 +878,7 @@ __device__ __forceinline__ void lab_window_body(const PholdDev& d, const LabDev&
 __host__ __device__ inline uint32_t lab_plain_lps_per_cta(uint32_t block) { return (block / 32u) * kLabWarpLps; }
 
 // Plain form: one launch per window.
-static __global__ void __launch_bounds__(256, 4) lab_window_kernel(PholdDev d, LabDev q, uint32_t s) {
+static __global__ void __launch_bounds__(1024, 1) lab_window_kernel(PholdDev d, LabDev q, uint32_t s) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ uint32_t red[32];
   const uint32_t mb = d.ctrl->mins[s % 3u];
@@ -860,7 +897,7 @@ static __global__ void __launch_bounds__(256, 4) lab_window_kernel(PholdDev d, L
 }
 
 // Persistent form: all windows in one cooperative launch, a bounded grid barrier per window.
-static __global__ void __launch_bounds__(256, 4) lab_persistent_kernel(PholdDev d, LabDev q, uint32_t s0,
+static __global__ void __launch_bounds__(1024, 1) lab_persistent_kernel(PholdDev d, LabDev q, uint32_t s0,
                                                                        uint32_t max_steps) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ uint32_t red[32];
