@@ -246,39 +246,56 @@ def bench_astar_batched(G, O, args, peak):
 
 def bench_phold_batched(G, O, args, peak):
     """The PHOLD runs of the first second of the served stream (LPs log-uniform in
-    [256, 65536], 32 events per LP, lookahead 0.5, end time 200), all in one launch."""
+    [256, 65536], 32 events per LP, lookahead 0.5, end time 200), all in one launch of a
+    session whose LP space holds sorted rings (the default session form); the same batch in
+    a time-bucket session and the plain path (each run alone through its own handle, both
+    queue forms) beside it."""
     reqs, n = G.serve_stream(99, 2000.0, 1.0)
     runs = [reqs[i].phold for i in range(n) if reqs[i].kind == G.REQ_PHOLD]
     lps = sum(r.num_lps for r in runs)
-    with G.PholdSession(max_lps=lps, max_instances=len(runs)) as s:
-        def step():
-            for r in runs:
-                s.admit(r)
+
+    def batch(bucketed, warmup, steps):
+        with G.PholdSession(max_lps=lps, max_instances=len(runs), bucketed=bucketed) as s:
+            def step():
+                for r in runs:
+                    s.admit(r)
+                t0 = time.perf_counter()
+                s.step(0)
+                got = s.collect()
+                return got, time.perf_counter() - t0
+            out, _ = _timed(step, warmup, steps)
+        return sum(r.committed for _, r in out[0][0]), sum(t for _, t in out), out[0][0]
+
+    ev, dt, got = batch(False, args.warmup, args.steps)
+    ev0, dt0, got0 = batch(True, 1, args.steps)
+    same = sorted((r.committed, r.digest) for _, r in got) == sorted((r.committed, r.digest) for _, r in got0)
+    plain = {}
+    for mode in (2, 0):
+        pe, pt, pw = 0, 0.0, 0.0
+        for r in runs[:16]:
+            c = G.make_phold_config(r.num_lps, 32, 0.5, 200.0, r.seed, laq_mode=mode,
+                                    **({"block_threads": 512} if mode == 2 else {}))
             t0 = time.perf_counter()
-            s.step(0)
-            got = s.collect()
-            return got, time.perf_counter() - t0
-        out, _ = _timed(step, args.warmup, args.steps)
-    ev = sum(r.committed for _, r in out[0][0])
-    dt = sum(t for _, t in out)
-    pe, pt, pw = 0, 0.0, 0.0
-    for r in runs[:16]:
-        c = G.make_phold_config(r.num_lps, 32, 0.5, 200.0, r.seed)
-        t0 = time.perf_counter()
-        with G.Phold(c) as h:  # the plain path: a handle per run, populate, run, results
-            h.populate()
-            h.run()
-            rr = h.result()
-        pw += time.perf_counter() - t0
-        pe += rr["committed"]
-        pt += rr["elapsed_ms"] / 1e3
+            with G.Phold(c) as h:  # the plain path: a handle per run, populate, run, results
+                h.populate()
+                h.run()
+                rr = h.result()
+            pw += time.perf_counter() - t0
+            pe += rr["committed"]
+            pt += rr["elapsed_ms"] / 1e3
+        plain[mode] = (pe / pw, pe / pt)
+    pv = max(plain[2][0], plain[0][0])
     achieved = ev * BYTES_PER_EVENT * args.steps / dt / 1e9
     return {"workload": f"phold_batched_{len(runs)}runs_lp256-65536_x32_T200", "metric": "PHOLD events/s (batched)",
             "value": ev * args.steps / dt, "unit": "events/s", "runs": len(runs), "lps": lps,
-            "ms_per_batch": 1e3 * dt / args.steps, "plain_value": pe / pw, "plain_device_value": pe / pt,
-            "plain_sample": "first 16 runs, each alone through its own handle (host wall clock, like the batch); "
-                            "plain_device_value counts their device time only",
-            "batched_over_plain": (ev * args.steps / dt) / (pe / pw),
+            "ms_per_batch": 1e3 * dt / args.steps, "queue_form": "sorted rings",
+            "time_bucket_session_value": ev0 * args.steps / dt0, "same_results_both_forms": same,
+            "plain_value": pv, "plain_bucketed_value": plain[2][0], "plain_sorted_value": plain[0][0],
+            "plain_device_value": max(plain[2][1], plain[0][1]),
+            "plain_sample": "first 16 runs, each alone through its own handle (host wall clock, like the batch), "
+                            "bucketed and sorted queue forms; plain_value is the faster; plain_device_value "
+                            "counts device time only",
+            "batched_over_plain": (ev * args.steps / dt) / pv,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak},
             "timing": "host wall clock around the session step (populate, all windows, collect)"}
 

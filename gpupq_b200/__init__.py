@@ -144,6 +144,8 @@ _SIGS = {
     "gpq_astar_session_bytes": ([_VP, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32], ctypes.c_uint64),
     "gpq_phold_session_create": ([ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                                   ctypes.c_uint32, ctypes.POINTER(_VP)], ctypes.c_int),
+    "gpq_phold_session_create_bucketed": ([ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                           ctypes.POINTER(_VP)], ctypes.c_int),
     "gpq_phold_session_destroy": ([_VP], ctypes.c_int),
     "gpq_phold_session_admit": ([_VP, ctypes.POINTER(PholdConfig), ctypes.POINTER(ctypes.c_uint32)], ctypes.c_int),
     "gpq_phold_session_step": ([_VP, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32), _VP], ctypes.c_int),
@@ -153,6 +155,8 @@ _SIGS = {
                                 ctypes.c_int),
     "gpq_phold_session_bytes": ([ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32],
                                 ctypes.c_uint64),
+    "gpq_phold_session_bytes_bucketed": ([ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32],
+                                         ctypes.c_uint64),
 }
 
 
@@ -571,12 +575,21 @@ class AStarSession:
 
 
 class PholdSession:
-    """Resident PHOLD runs (gpq_phold_session_*): admit, step, collect."""
+    """Resident PHOLD runs (gpq_phold_session_*): admit, step, collect.
 
-    def __init__(self, max_lps, max_instances, capacity=256, insert_capacity=64, lanes_per_lp=8):
+    bucketed=True keeps the LP space as time buckets (gpq_phold_session_create_bucketed,
+    `buckets` x `bucket_slots` keys per LP, 0 = 32 x 16) instead of sorted rings
+    (capacity, insert_capacity, lanes_per_lp)."""
+
+    def __init__(self, max_lps, max_instances, capacity=256, insert_capacity=64, lanes_per_lp=8, bucketed=False,
+                 buckets=0, bucket_slots=0):
         self._h = ctypes.c_void_p()
-        check(lib().gpq_phold_session_create(max_lps, capacity, insert_capacity, max_instances, lanes_per_lp,
-                                             ctypes.byref(self._h)), "gpq_phold_session_create")
+        if bucketed:
+            check(lib().gpq_phold_session_create_bucketed(max_lps, buckets, bucket_slots, max_instances,
+                                                          ctypes.byref(self._h)), "gpq_phold_session_create_bucketed")
+        else:
+            check(lib().gpq_phold_session_create(max_lps, capacity, insert_capacity, max_instances, lanes_per_lp,
+                                                 ctypes.byref(self._h)), "gpq_phold_session_create")
         self.max_instances = max_instances
 
     def close(self):
@@ -652,7 +665,7 @@ class ServeConfig(ctypes.Structure):
                 ("astar_rounds", ctypes.c_uint32), ("phold_windows", ctypes.c_uint32),
                 ("astar_share", ctypes.c_double), ("astar", AstarConfig), ("phold_capacity", ctypes.c_uint32),
                 ("phold_insert_capacity", ctypes.c_uint32), ("phold_lanes_per_lp", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32 * 5)]
+                ("phold_form", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 4)]
 
 
 class ServeStats(ctypes.Structure):
@@ -683,9 +696,11 @@ def serve_stream(seed, rate, duration, astar_fraction=0.8):
 
 
 def serve(reqs, n, mode=SERVE_BATCHED, budget=0, realtime=True, astar_rounds=0, phold_windows=0, astar_share=0.0,
-          **astar_cfg):
-    """Run gpq_serve_run; returns (responses, stats dict)."""
+          phold_form=0, **astar_cfg):
+    """Run gpq_serve_run; returns (responses, stats dict).  phold_form 0 keeps the PHOLD
+    runs in sorted rings, 1 in time buckets."""
     c = ServeConfig()
+    c.phold_form = phold_form
     c.hbm_budget = budget
     c.astar_share = astar_share
     c.mode = mode

@@ -46,6 +46,7 @@ struct LabDev {
   uint32_t* wj;               // [4] j1 of window s in wj[s & 3] (wj[3] = 0 before window 0)
   uint32_t nb_log2, c_log2, F;
   float inv_w;                // 1 / bucket width
+  uint32_t chunk;             // LPs per warp chunk (lab_chunk_lps)
 };
 
 static constexpr uint32_t kLabSafeCap = 32;  // safe keys of one LP per window ranked in shared memory
@@ -78,29 +79,65 @@ struct LabWin {
   uint32_t j0, j1;    // bucket range that holds every safe event
   uint32_t j1p;       // j1 of the previous window: appends reach at most j1p + NB - 1
   uint32_t curb, prevb;
+  float inv_w;        // 1 / bucket width of the run
 };
 
 __device__ __forceinline__ bool lab_live(uint32_t t, const LabWin& w) { return t >= w.mb && t <= kInfBits; }
 
-__device__ __forceinline__ LabWin lab_window(const PholdDev& d, const LabDev& q, uint32_t s, float m) {
+// The run a window belongs to: its model, where its LPs sit in the LP space, and where its
+// errors go.  One PHOLD run per launch uses lp_base 0 and L = its LP count; runs that share
+// an LP space number their LPs from lp_base (events carry LP-space numbers; the model sees
+// numbers local to the run).
+struct LabCtx {
+  gpq_phold_params p;  // the run's model (num_lps = its LP count)
+  uint32_t L;          // LP-space size: stride of the spill lists
+  uint32_t lp_base;    // the run's first LP in the LP space
+  uint32_t* err;       // the run's sticky error word
+  uint32_t* err_slot;  // error slot read by the next window's exit decision
+};
+
+__device__ __forceinline__ void lab_fail(const LabCtx& x, uint32_t code) {
+  gpq_set_error(x.err, code);
+  atomicOr(x.err_slot, 1u);
+}
+
+// Child of staged event e (LP-space numbers in and out).
+__device__ __forceinline__ gpq_item lab_child(const LabCtx& x, const gpq_item e) {
+  gpq_item pe = e;
+  pe.lp = e.lp - x.lp_base;
+  pe.aux = pe.lp;
+  gpq_item ch = gpq_phold_child(x.p, pe);
+  ch.lp += x.lp_base;
+  return ch;
+}
+
+// Window s of a run with minimum m, model p, bucket width 1 / inv_w, and top bucket of its
+// previous window j1p.
+__device__ __forceinline__ LabWin lab_window_of(const gpq_phold_params& p, float inv_w, uint32_t s, float m,
+                                                uint32_t j1p) {
   LabWin w;
-  const float bound = GPQ_FADD(m, d.p.lookahead);
+  const float bound = GPQ_FADD(m, p.lookahead);
   w.mb = gpq_f2u(m);
-  const uint32_t bb = gpq_f2u(bound), tb = gpq_f2u(d.p.end_time);
+  const uint32_t bb = gpq_f2u(bound), tb = gpq_f2u(p.end_time);
   w.safe_lim = bb < tb ? bb : tb;  // timestamps, bound and end time are >= +0: bit order = value order
-  w.j0 = lab_bucket(w.mb, q.inv_w);
-  w.j1 = lab_bucket(bb, q.inv_w);
-  w.j1p = ld_relaxed_u32(&q.wj[(s + 3u) & 3u]);
+  w.j0 = lab_bucket(w.mb, inv_w);
+  w.j1 = lab_bucket(bb, inv_w);
+  w.j1p = j1p;
   w.curb = s & 1u;
   w.prevb = (s + 1u) & 1u;
+  w.inv_w = inv_w;
   return w;
+}
+
+__device__ __forceinline__ LabWin lab_window(const PholdDev& d, const LabDev& q, uint32_t s, float m) {
+  return lab_window_of(d.p, q.inv_w, s, m, ld_relaxed_u32(&q.wj[(s + 3u) & 3u]));
 }
 
 // Files one pending key of LP `lp` (bucket jb) during window w: into its bucket when jb is
 // in [j1, j1p + NB) and the bucket has room, else into the spill list of this window's
 // parity.
-__device__ __forceinline__ void lab_push(const PholdDev& d, const LabDev& q, uint32_t lp, unsigned long long key,
-                                         uint32_t jb, const LabWin& w, uint32_t* err_slot) {
+__device__ __forceinline__ void lab_push(const LabCtx& x, const LabDev& q, uint32_t lp, unsigned long long key,
+                                         uint32_t jb, const LabWin& w) {
   const uint32_t nbm = (1u << q.nb_log2) - 1u;
   if (jb >= w.j1 && jb - w.j1p <= nbm) {
     const size_t b = ((size_t)lp << q.nb_log2) + (jb & nbm);
@@ -110,31 +147,28 @@ __device__ __forceinline__ void lab_push(const PholdDev& d, const LabDev& q, uin
       return;
     }
   }
-  const size_t sl = (size_t)w.curb * d.L + lp;
+  const size_t sl = (size_t)w.curb * x.L + lp;
   const uint32_t pos = atomicAdd(&q.scnt[sl], 1u);
   if (pos < q.F) {
     q.spill[sl * q.F + pos] = key;
   } else {
-    gpq_set_error(&d.ctrl->err, GPQ_ERR_QUEUE_FULL);
-    atomicOr(err_slot, 1u);
+    lab_fail(x, GPQ_ERR_QUEUE_FULL);
   }
 }
 
 // Process one staged event: per-LP hashes into the slot accumulators, the child into its
 // bucket.  Returns the child's timestamp bits.
-__device__ __forceinline__ uint32_t lab_process_event(const PholdDev& d, const LabDev& q, const PholdStage& st,
-                                                      const gpq_item e, const LabWin& w, uint32_t* err_slot) {
+__device__ __forceinline__ uint32_t lab_process_event(const LabCtx& x, const LabDev& q, const PholdStage& st,
+                                                      const gpq_item e, const LabWin& w) {
   const uint32_t slot = e.aux >> 16;
   const uint32_t idx = e.aux & 0xffffu;
   const uint32_t tb = gpq_f2u(e.ts);
   const uint64_t h = gpq_ev_hash(e.id, tb);
   atomicAdd(&st.csum[slot], (unsigned long long)h);
   atomicAdd(&st.ohash[slot], (unsigned long long)gpq_seq_hash(h, (uint64_t)st.seq0[slot] + idx));
-  gpq_item pe = e;
-  pe.aux = e.lp;
-  const gpq_item ch = gpq_phold_child(d.p, pe);
+  const gpq_item ch = lab_child(x, e);
   const uint32_t cb = gpq_f2u(ch.ts);
-  lab_push(d, q, ch.lp, lab_key(cb, ch.id), lab_bucket(cb, q.inv_w), w, err_slot);
+  lab_push(x, q, ch.lp, lab_key(cb, ch.id), lab_bucket(cb, w.inv_w), w);
   return cb;
 }
 
@@ -144,10 +178,10 @@ struct LabMeta {
   uint32_t sc, bc;
 };
 
-__device__ __forceinline__ LabMeta lab_load_meta(const PholdDev& d, const LabDev& q, uint32_t lp, const LabWin& w,
+__device__ __forceinline__ LabMeta lab_load_meta(const LabCtx& x, const LabDev& q, uint32_t lp, const LabWin& w,
                                                  uint32_t gl) {
   LabMeta mt;
-  mt.sc = q.scnt[(size_t)w.prevb * d.L + lp];
+  mt.sc = q.scnt[(size_t)w.prevb * x.L + lp];
   const uint32_t nbm = (1u << q.nb_log2) - 1u;
   mt.bc = ld_relaxed_u32(&q.cnt[((size_t)lp << q.nb_log2) + ((w.j0 + gl) & nbm)]);
   return mt;
@@ -174,10 +208,9 @@ __device__ __forceinline__ unsigned long long lab_cand(const unsigned long long*
 // the LP's next minimum (ts bits) min'ed with any child processed here.  All lanes of the
 // group, convergent.
 template <int G>
-__device__ uint32_t lab_lp_stage(const PholdDev& d, const LabDev& q, uint32_t lp, uint32_t slot, const LabWin& w,
-                                 unsigned long long* skeys, const PholdStage& st, const LaneGroup<G>& g,
-                                 uint32_t* err_slot, const LabMeta& mt, uint32_t* nsafe_out) {
-  const uint32_t L = d.L;
+__device__ uint32_t lab_lp_stage(const LabCtx& x, const LabDev& q, uint32_t lp, uint32_t slot, const LabWin& w,
+                                 unsigned long long* skeys, const PholdStage& st, const LaneGroup<G>& g, const LabMeta& mt, uint32_t* nsafe_out) {
+  const uint32_t L = x.L;
   const uint32_t NB = 1u << q.nb_log2, nbm = NB - 1u, C = 1u << q.c_log2;
   const size_t lpb = (size_t)lp << q.nb_log2;
   unsigned long long* keys = q.keys + (lpb << q.c_log2);
@@ -215,7 +248,7 @@ __device__ uint32_t lab_lp_stage(const PholdDev& d, const LabDev& q, uint32_t lp
     }
   }
   if (nsafe > 0xffffu) {  // ranks are 16-bit in the staged events
-    if (g.gl == 0) { gpq_set_error(&d.ctrl->err, GPQ_ERR_INVALID); atomicOr(err_slot, 1u); }
+    if (g.gl == 0) lab_fail(x, GPQ_ERR_INVALID);
     nsafe = 0;
   }
   g.sync();
@@ -241,7 +274,7 @@ __device__ uint32_t lab_lp_stage(const PholdDev& d, const LabDev& q, uint32_t lp
           hole.aux = kStageHole;
           st.ev[base + rank] = hole;
         }
-        cmin = min(cmin, lab_process_event(d, q, st, e, w, err_slot));
+        cmin = min(cmin, lab_process_event(x, q, st, e, w));
       }
     };
     if (nsafe <= kLabSafeCap) {
@@ -332,10 +365,10 @@ __device__ uint32_t lab_lp_stage(const PholdDev& d, const LabDev& q, uint32_t lp
     const unsigned long long k = sp[i];
     const uint32_t t = (uint32_t)(k >> 32);
     if (t < w.safe_lim) continue;
-    const uint32_t jb = lab_bucket(t, q.inv_w);
+    const uint32_t jb = lab_bucket(t, w.inv_w);
     rmin = min(rmin, t);
     low_lane = low_lane || jb <= w.j1;
-    lab_push(d, q, lp, k, jb, w, err_slot);
+    lab_push(x, q, lp, k, jb, w);
   }
   const bool low = g.ballot(low_lane) != 0u;
   if (g.gl == 0 && mt.sc != 0) q.scnt[(size_t)w.prevb * L + lp] = 0;
@@ -423,6 +456,22 @@ __host__ __device__ constexpr size_t lab_warp_smem_bytes() {
           (size_t)kLabCandCap * 2 + (size_t)kLabWarpLps * kLabSafePerLp * 2 + 15) & ~(size_t)15;
 }
 
+// LPs per warp chunk for a run with lookahead la, bucket width 1 / inv_w and E events per
+// LP: the chunk's candidate keys (its LPs' range buckets, each holding about
+// occ = E / (inv_w * (la + 1)) live keys, plus dead ones) within kLabCandCap and its safe
+// events (about E * la / (la + 1) per LP per window) within kLabStageCap, with a margin,
+// so that windows stay on the common path.
+__host__ __device__ inline uint32_t lab_chunk_lps(float la, float inv_w, uint32_t E) {
+  const float occ = (float)E / (inv_w * (la + 1.0f));
+  const float cand = occ * (la * inv_w + 1.5f) + 1.0f;
+  const float ev = (float)E * la / (la + 1.0f) + 0.5f;
+  float n = 0.9f * (float)kLabCandCap / cand;
+  const float n2 = 0.9f * (float)kLabStageCap / ev;
+  if (n2 < n) n = n2;
+  if (n > (float)kLabWarpLps) n = (float)kLabWarpLps;
+  return n < 1.0f ? 1u : (uint32_t)n;
+}
+
 __host__ __device__ inline size_t lab_cta_smem_bytes(uint32_t block) { return (size_t)(block / 32) * lab_warp_smem_bytes(); }
 
 __device__ __forceinline__ LabWarpSmem lab_warp_smem(unsigned char* base) {
@@ -473,22 +522,33 @@ __device__ __forceinline__ uint32_t lab_warp_scan(uint32_t* a, uint32_t n) {
   return total;
 }
 
-__device__ __forceinline__ void lab_state_load(const PholdDev& d, const LabWarpSmem& sm, uint32_t lp0, uint32_t n) {
+__device__ __forceinline__ void lab_state_load(const uint32_t* count, const unsigned long long* csum,
+                                               const unsigned long long* ohash, const LabWarpSmem& sm, uint32_t lp0,
+                                               uint32_t n) {
   for (uint32_t x = threadIdx.x & 31u; x < n; x += 32u) {
-    sm.ls_cnt[x] = d.count[lp0 + x];
-    sm.ls_csum[x] = d.csum[lp0 + x];
-    sm.ls_ohash[x] = d.ohash[lp0 + x];
+    sm.ls_cnt[x] = count[lp0 + x];
+    sm.ls_csum[x] = csum[lp0 + x];
+    sm.ls_ohash[x] = ohash[lp0 + x];
   }
   __syncwarp();
 }
 
-__device__ __forceinline__ void lab_state_store(const PholdDev& d, const LabWarpSmem& sm, uint32_t lp0, uint32_t n) {
+__device__ __forceinline__ void lab_state_load(const PholdDev& d, const LabWarpSmem& sm, uint32_t lp0, uint32_t n) {
+  lab_state_load(d.count, d.csum, d.ohash, sm, lp0, n);
+}
+
+__device__ __forceinline__ void lab_state_store(uint32_t* count, unsigned long long* csum, unsigned long long* ohash,
+                                                const LabWarpSmem& sm, uint32_t lp0, uint32_t n) {
   __syncwarp();
   for (uint32_t x = threadIdx.x & 31u; x < n; x += 32u) {
-    d.count[lp0 + x] = sm.ls_cnt[x];
-    d.csum[lp0 + x] = sm.ls_csum[x];
-    d.ohash[lp0 + x] = sm.ls_ohash[x];
+    count[lp0 + x] = sm.ls_cnt[x];
+    csum[lp0 + x] = sm.ls_csum[x];
+    ohash[lp0 + x] = sm.ls_ohash[x];
   }
+}
+
+__device__ __forceinline__ void lab_state_store(const PholdDev& d, const LabWarpSmem& sm, uint32_t lp0, uint32_t n) {
+  lab_state_store(d.count, d.csum, d.ohash, sm, lp0, n);
 }
 
 // Next minimum of an LP with nothing live at or below j1: the smallest live key of the
@@ -524,9 +584,8 @@ __device__ __forceinline__ uint32_t lab_scan_above(const LabDev& q, uint32_t lp,
 // children first, then all bucket reservations (independent atomics in flight together),
 // then the stores.  Returns the children's minimum.
 template <class Get>
-__device__ __forceinline__ uint32_t lab_event_batch(const PholdDev& d, const LabDev& q, const PholdStage& st,
-                                                    uint32_t ns, uint32_t x0, uint32_t stride, const LabWin& w,
-                                                    uint32_t* err_slot, Get get) {
+__device__ __forceinline__ uint32_t lab_event_batch(const LabCtx& x, const LabDev& q, const PholdStage& st,
+                                                    uint32_t ns, uint32_t x0, uint32_t stride, const LabWin& w, Get get) {
   constexpr int U = 4;
   const uint32_t nbm = (1u << q.nb_log2) - 1u, C = 1u << q.c_log2;
   unsigned long long key[U];
@@ -534,22 +593,20 @@ __device__ __forceinline__ uint32_t lab_event_batch(const PholdDev& d, const Lab
   uint32_t mn = kInfBits;
 #pragma unroll
   for (int u = 0; u < U; ++u) {
-    const uint32_t x = x0 + (uint32_t)u * stride;
+    const uint32_t xi = x0 + (uint32_t)u * stride;
     lp[u] = ~0u;
-    if (x < ns) {
-      const gpq_item e = get(x);
+    if (xi < ns) {
+      const gpq_item e = get(xi);
       if (e.aux != kStageHole) {
         const uint32_t slot = e.aux >> 16, idx = e.aux & 0xffffu, tb = gpq_f2u(e.ts);
         const uint64_t h = gpq_ev_hash(e.id, tb);
         atomicAdd(&st.csum[slot], (unsigned long long)h);
         atomicAdd(&st.ohash[slot], (unsigned long long)gpq_seq_hash(h, (uint64_t)st.seq0[slot] + idx));
-        gpq_item pe = e;
-        pe.aux = e.lp;
-        const gpq_item ch = gpq_phold_child(d.p, pe);
+        const gpq_item ch = lab_child(x, e);
         const uint32_t cb = gpq_f2u(ch.ts);
         key[u] = lab_key(cb, ch.id);
         lp[u] = ch.lp;
-        jb[u] = lab_bucket(cb, q.inv_w);
+        jb[u] = lab_bucket(cb, w.inv_w);
         mn = min(mn, cb);
       }
     }
@@ -566,13 +623,12 @@ __device__ __forceinline__ uint32_t lab_event_batch(const PholdDev& d, const Lab
     if (pos[u] < C) {
       st_relaxed_u64(q.keys + ((((size_t)lp[u] << q.nb_log2) + (jb[u] & nbm)) << q.c_log2) + pos[u], key[u]);
     } else {
-      const size_t sl = (size_t)w.curb * d.L + lp[u];
+      const size_t sl = (size_t)w.curb * x.L + lp[u];
       const uint32_t sp = atomicAdd(&q.scnt[sl], 1u);
       if (sp < q.F) {
         q.spill[sl * q.F + sp] = key[u];
       } else {
-        gpq_set_error(&d.ctrl->err, GPQ_ERR_QUEUE_FULL);
-        atomicOr(err_slot, 1u);
+        lab_fail(x, GPQ_ERR_QUEUE_FULL);
       }
     }
   }
@@ -581,22 +637,22 @@ __device__ __forceinline__ uint32_t lab_event_batch(const PholdDev& d, const Lab
 
 // Key of candidate source r, slot i, of LP lp (bucket j1 read with relaxed loads: it may be
 // appended to meanwhile).
-__device__ __forceinline__ unsigned long long lab_load_cand(const PholdDev& d, const LabDev& q, const LabWin& w,
+__device__ __forceinline__ unsigned long long lab_load_cand(const LabCtx& x, const LabDev& q, const LabWin& w,
                                                             uint32_t nr, uint32_t lp, uint32_t r, uint32_t i) {
   const uint32_t nbm = (1u << q.nb_log2) - 1u;
   if (r < nr) {
     const unsigned long long* p = q.keys + ((((size_t)lp << q.nb_log2) + ((w.j0 + r) & nbm)) << q.c_log2) + i;
     return (r + 1u == nr) ? ld_relaxed_u64(p) : *p;
   }
-  return q.spill[((size_t)w.prevb * d.L + lp) * q.F + i];
+  return q.spill[((size_t)w.prevb * x.L + lp) * q.F + i];
 }
 
 // One window for the chunk [lp0, lp0 + n) of one warp (outputs in sm.ls_*).  Returns this
 // lane's part of the chunk minimum (LP next minima and children).  All lanes of the warp.
-__device__ uint32_t lab_warp_window(const PholdDev& d, const LabDev& q, const LabWin& w, uint32_t lp0, uint32_t n,
-                                    const LabWarpSmem& sm, uint32_t* err_slot) {
+static __device__ uint32_t lab_warp_window(const LabCtx& x, const LabDev& q, const LabWin& w, uint32_t lp0, uint32_t n,
+                                    const LabWarpSmem& sm) {
   const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t L = d.L, NB = 1u << q.nb_log2, nbm = NB - 1u, C = 1u << q.c_log2;
+  const uint32_t L = x.L, NB = 1u << q.nb_log2, nbm = NB - 1u, C = 1u << q.c_log2;
   const uint32_t nr = w.j1 - w.j0 + 1u, S = nr + 1u;
   uint32_t mn = kInfBits;
   PholdStage st;
@@ -612,8 +668,8 @@ __device__ uint32_t lab_warp_window(const PholdDev& d, const LabDev& q, const La
   // bucket skipped by a jump of m (no append reaches their next use before this window)
   if (w.j0 > w.j1p) {
     const uint32_t nres = min(w.j0, w.j1p + NB) - w.j1p;
-    for (uint32_t x = lane; x < n * nres; x += 32u) {
-      const uint32_t lpi = x / nres, j = w.j1p + (x - lpi * nres);
+    for (uint32_t y = lane; y < n * nres; y += 32u) {
+      const uint32_t lpi = y / nres, j = w.j1p + (y - lpi * nres);
       q.cnt[((size_t)(lp0 + lpi) << q.nb_log2) + (j & nbm)] = 0u;
     }
   }
@@ -628,8 +684,8 @@ __device__ uint32_t lab_warp_window(const PholdDev& d, const LabDev& q, const La
   uint32_t K = 0xffffffffu;
   if (S <= kLabSegMax) {
     // P1: range-bucket and spill counts, and the counts of the two buckets above j1
-    for (uint32_t x = lane; x < n * (S + 2u); x += 32u) {
-      const uint32_t lpi = x / (S + 2u), r = x - lpi * (S + 2u), lp = lp0 + lpi;
+    for (uint32_t y = lane; y < n * (S + 2u); y += 32u) {
+      const uint32_t lpi = y / (S + 2u), r = y - lpi * (S + 2u), lp = lp0 + lpi;
       if (r < S) {
         uint32_t raw, c;
         if (r < nr) {
@@ -675,7 +731,7 @@ __device__ uint32_t lab_warp_window(const PholdDev& d, const LabDev& q, const La
           uint32_t r = 0;
           while (r + 1u < S && sm.seg_off[lo * S + r + 1u] <= k) ++r;
           sg[u] = (lo << 3) | r;
-          v[u] = lab_load_cand(d, q, w, nr, lp0 + lo, r, k - sm.seg_off[lo * S + r]);
+          v[u] = lab_load_cand(x, q, w, nr, lp0 + lo, r, k - sm.seg_off[lo * S + r]);
         }
       }
 #pragma unroll
@@ -700,7 +756,7 @@ __device__ uint32_t lab_warp_window(const PholdDev& d, const LabDev& q, const La
         continue;
       }
       atomicMin(&sm.lp_rmin[lpi], t);
-      if (r < nr || lab_bucket(t, q.inv_w) <= w.j1) sm.lp_low[lpi] = 1u;
+      if (r < nr || lab_bucket(t, w.inv_w) <= w.j1) sm.lp_low[lpi] = 1u;
     }
     __syncwarp();
   }
@@ -717,15 +773,15 @@ __device__ uint32_t lab_warp_window(const PholdDev& d, const LabDev& q, const La
         if (r + 1u < nr) {  // a bucket below j1: compact (the staying keys keep their order)
           const uint32_t sgi = lpi * S + r, a = sm.seg_off[sgi];
           uint32_t p = 0;
-          for (uint32_t x = a; x < k; ++x) {
-            const uint32_t t2 = (uint32_t)(sm.cand[x] >> 32);
+          for (uint32_t y = a; y < k; ++y) {
+            const uint32_t t2 = (uint32_t)(sm.cand[y] >> 32);
             p += (lab_live(t2, w) && t2 >= w.safe_lim) ? 1u : 0u;
           }
           atomicAdd(&sm.seg_kept[sgi], 1u);
           if (p != k - a) q.keys[((((size_t)lp << q.nb_log2) + ((w.j0 + r) & nbm)) << q.c_log2) + p] = key;
         }
       } else {
-        lab_push(d, q, lp, key, lab_bucket(t, q.inv_w), w, err_slot);
+        lab_push(x, q, lp, key, lab_bucket(t, w.inv_w), w);
       }
     }
     __syncwarp();
@@ -733,8 +789,8 @@ __device__ uint32_t lab_warp_window(const PholdDev& d, const LabDev& q, const La
     if (lane < n) {
       const uint32_t lp = lp0 + lane;
       for (uint32_t r = 0; r + 1u < nr; ++r) {
-        const uint32_t x = lane * S + r;
-        if (sm.seg_kept[x] != sm.seg_raw[x]) q.cnt[((size_t)lp << q.nb_log2) + ((w.j0 + r) & nbm)] = sm.seg_kept[x];
+        const uint32_t y = lane * S + r;
+        if (sm.seg_kept[y] != sm.seg_raw[y]) q.cnt[((size_t)lp << q.nb_log2) + ((w.j0 + r) & nbm)] = sm.seg_kept[y];
       }
       if (sm.seg_raw[lane * S + nr] != 0u) q.scnt[(size_t)w.prevb * L + lp] = 0u;
       sm.lp_soff[lane] = sm.lp_nsafe[lane];
@@ -754,7 +810,7 @@ __device__ uint32_t lab_warp_window(const PholdDev& d, const LabDev& q, const La
       const uint32_t k = li[u - sm.lp_soff[lo]];
       const unsigned long long key = sm.cand[k];
       uint32_t rank = 0;
-      for (uint32_t x = 0; x < ns_lp; ++x) rank += (sm.cand[li[x]] < key) ? 1u : 0u;
+      for (uint32_t y = 0; y < ns_lp; ++y) rank += (sm.cand[li[y]] < key) ? 1u : 0u;
       const uint32_t pos = sm.lp_soff[lo] + rank;
       if (pos < kLabStageCap) {
         sm.cstage[pos] = k | (rank << 16);
@@ -764,7 +820,7 @@ __device__ uint32_t lab_warp_window(const PholdDev& d, const LabDev& q, const La
         e.lp = lp0 + lo;
         e.id = (uint32_t)key;
         e.aux = (lo << 16) | rank;
-        mn = min(mn, lab_process_event(d, q, st, e, w, err_slot));
+        mn = min(mn, lab_process_event(x, q, st, e, w));
       }
     }
     // next-minimum scan of the LPs with nothing live at or below j1, when one of the two
@@ -800,8 +856,8 @@ __device__ uint32_t lab_warp_window(const PholdDev& d, const LabDev& q, const La
     __syncwarp();
     for (uint32_t lpi = 0; lpi < n; ++lpi) {
       const uint32_t lp = lp0 + lpi;
-      const LabMeta mt = lab_load_meta(d, q, lp, w, g.gl);
-      mn = min(mn, lab_lp_stage<32>(d, q, lp, lpi, w, sm.cand, st, g, err_slot, mt, sm.lp_nsafe));
+      const LabMeta mt = lab_load_meta(x, q, lp, w, g.gl);
+      mn = min(mn, lab_lp_stage<32>(x, q, lp, lpi, w, sm.cand, st, g, mt, sm.lp_nsafe));
     }
     __syncwarp();
   }
@@ -809,8 +865,8 @@ __device__ uint32_t lab_warp_window(const PholdDev& d, const LabDev& q, const La
   // P7: events (four in flight per lane), then the next minimum of each LP
   if (common) {
     const uint32_t ns = min(sm.misc[0], kLabStageCap);
-    auto get = [&](uint32_t x) {
-      const uint32_t c = sm.cstage[x], k = c & 0xffffu;
+    auto get = [&](uint32_t y) {
+      const uint32_t c = sm.cstage[y], k = c & 0xffffu;
       const unsigned long long key = sm.cand[k];
       gpq_item e;
       e.ts = gpq_u2f((uint32_t)(key >> 32));
@@ -819,11 +875,11 @@ __device__ uint32_t lab_warp_window(const PholdDev& d, const LabDev& q, const La
       e.aux = ((uint32_t)(sm.cseg[k] >> 3) << 16) | (c >> 16);
       return e;
     };
-    for (uint32_t x0 = lane; x0 < ns; x0 += 128u) mn = min(mn, lab_event_batch(d, q, st, ns, x0, 32u, w, err_slot, get));
+    for (uint32_t x0 = lane; x0 < ns; x0 += 128u) mn = min(mn, lab_event_batch(x, q, st, ns, x0, 32u, w, get));
   } else {
     const uint32_t ns = min(sm.misc[0], kLabItemStageCap);
-    auto get = [&](uint32_t x) { return sm.stage[x]; };
-    for (uint32_t x0 = lane; x0 < ns; x0 += 128u) mn = min(mn, lab_event_batch(d, q, st, ns, x0, 32u, w, err_slot, get));
+    auto get = [&](uint32_t y) { return sm.stage[y]; };
+    for (uint32_t x0 = lane; x0 < ns; x0 += 128u) mn = min(mn, lab_event_batch(x, q, st, ns, x0, 32u, w, get));
   }
   if (common) {
     if (scan_lpi != ~0u && scan_min != kInfBits) atomicMin(&sm.lp_nmin[scan_lpi], scan_min);
@@ -858,16 +914,16 @@ __device__ __forceinline__ void lab_window_body(const PholdDev& d, const LabDev&
                                                 unsigned char* smem_raw, uint32_t* red, uint32_t lp_lo,
                                                 uint32_t lp_hi, bool resident) {
   const LabWin w = lab_window(d, q, s, m);
-  uint32_t* err_slot = &d.ctrl->errs[(s + 1u) % 3u];
+  const LabCtx x{d.p, d.L, 0u, &d.ctrl->err, &d.ctrl->errs[(s + 1u) % 3u]};
   const uint32_t warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const LabWarpSmem sm = lab_warp_smem(smem_raw + (size_t)warp * lab_warp_smem_bytes());
   const uint32_t pw = (lp_hi - lp_lo + nw - 1u) / nw;
   const uint32_t wlo = min(lp_hi, lp_lo + warp * pw), whi = min(lp_hi, wlo + pw);
   uint32_t mn = kInfBits;
-  for (uint32_t c0 = wlo; c0 < whi; c0 += kLabWarpLps) {
-    const uint32_t n = min(kLabWarpLps, whi - c0);
+  for (uint32_t c0 = wlo; c0 < whi; c0 += q.chunk) {
+    const uint32_t n = min(q.chunk, whi - c0);
     if (!resident) lab_state_load(d, sm, c0, n);
-    mn = min(mn, lab_warp_window(d, q, w, c0, n, sm, err_slot));
+    mn = min(mn, lab_warp_window(x, q, w, c0, n, sm));
     if (!resident) lab_state_store(d, sm, c0, n);
   }
   mn = block_min_u32(mn, red);
@@ -875,7 +931,7 @@ __device__ __forceinline__ void lab_window_body(const PholdDev& d, const LabDev&
 }
 
 // LPs a CTA of `block` threads covers in one launch of the plain form.
-__host__ __device__ inline uint32_t lab_plain_lps_per_cta(uint32_t block) { return (block / 32u) * kLabWarpLps; }
+__host__ __device__ inline uint32_t lab_plain_lps_per_cta(uint32_t block, uint32_t chunk) { return (block / 32u) * chunk; }
 
 // Plain form: one launch per window.
 static __global__ void __launch_bounds__(1024, 1) lab_window_kernel(PholdDev d, LabDev q, uint32_t s) {
@@ -891,7 +947,7 @@ static __global__ void __launch_bounds__(1024, 1) lab_window_kernel(PholdDev d, 
     d.ctrl->phase = s + 1u;
     q.wj[s & 3u] = lab_bucket(gpq_f2u(GPQ_FADD(m, d.p.lookahead)), q.inv_w);
   }
-  const uint32_t per = lab_plain_lps_per_cta(blockDim.x);
+  const uint32_t per = (blockDim.x / 32u) * q.chunk;
   const uint32_t lp_lo = min(d.L, blockIdx.x * per), lp_hi = min(d.L, lp_lo + per);
   lab_window_body(d, q, s, m, smem_raw, red, lp_lo, lp_hi, false);
 }
@@ -906,7 +962,7 @@ static __global__ void __launch_bounds__(1024, 1) lab_persistent_kernel(PholdDev
   const uint32_t warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const uint32_t pw = (lp_hi - lp_lo + nw - 1u) / nw;
   const uint32_t wlo = min(lp_hi, lp_lo + warp * pw), whi = min(lp_hi, wlo + pw);
-  const bool resident = (per + nw - 1u) / nw <= kLabWarpLps;
+  const bool resident = (per + nw - 1u) / nw <= q.chunk;
   const LabWarpSmem sm = lab_warp_smem(smem_raw + (size_t)warp * lab_warp_smem_bytes());
   if (resident) lab_state_load(d, sm, wlo, whi - wlo);
   unsigned long long target = 0;

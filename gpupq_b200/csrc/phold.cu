@@ -199,6 +199,7 @@ gpq_status gpq_phold_create(const gpq_phold_config* cfg_in, gpq_phold** out) {
     q.c_log2 = geo.c_log2;
     q.F = geo.spill;
     q.inv_w = geo.inv_w;
+    q.chunk = lab_chunk_lps(c.lookahead, q.inv_w, c.events_per_lp);
     TRY(cudaMalloc(&q.keys, (L << (q.nb_log2 + q.c_log2)) * sizeof(unsigned long long)));
     TRY(cudaMalloc(&q.cnt, (L << q.nb_log2) * sizeof(uint32_t)));
     TRY(cudaMalloc(&q.spill, 2 * L * q.F * sizeof(unsigned long long)));
@@ -360,7 +361,7 @@ gpq_status gpq_phold_populate(gpq_phold* h, const gpq_item* initial, uint64_t n,
 
 static gpq_status run_plain(gpq_phold* h, uint32_t nsteps, int* done, cudaStream_t st) {
   const gpq_phold_config& c = h->cfg;
-  const uint32_t gpb = h->is_lab ? lab_plain_lps_per_cta(h->block) : h->block / h->ks.group;  // LPs per CTA
+  const uint32_t gpb = h->is_lab ? lab_plain_lps_per_cta(h->block, h->lab.chunk) : h->block / h->ks.group;  // LPs per CTA
   const uint32_t grid = (uint32_t)((c.num_lps + gpb - 1) / gpb);
   const size_t smem = h->window_smem();
   PholdDev d = h->dev();

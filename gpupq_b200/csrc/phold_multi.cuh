@@ -23,7 +23,7 @@ struct PmInstDev {
   uint32_t err;
   uint32_t windows;    // windows this instance took part in
   uint32_t w0;         // its first window; it runs windows [w0, w0 + windows)
-  uint32_t pad;
+  uint32_t aux;        // bucketed sessions: 1 / bucket width of the run (float bits)
 };
 
 struct PmCtl {

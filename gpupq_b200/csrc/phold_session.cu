@@ -1,13 +1,16 @@
 // Resident PHOLD instances (gpq_phold_session_*): many runs in one persistent launch for
 // batching and serving.  Instances take free ranges of one LP space reserved up front,
 // advance together one window per grid barrier (each with its own window), and are
-// collected when their minimum reaches their end time.
+// collected when their minimum reaches their end time.  The LP space holds either sorted
+// rings (phold_multi.cuh) or time buckets (phold_multi_lab.cuh, a bucketed session).
 #include <algorithm>
+#include <cstring>
 #include <vector>
 
 #include "host_common.h"
 #include "phold_host.h"
 #include "phold_multi.cuh"
+#include "phold_multi_lab.cuh"
 #include "range_alloc.h"
 
 using gpq::set_last_error;
@@ -45,6 +48,9 @@ struct gpq_phold_session {
   int grid = 0;
   size_t smem = 0;
   const void* kern = nullptr;
+  // bucketed sessions
+  bool bucketed = false;
+  PmbDev b{};
 };
 
 namespace {
@@ -110,6 +116,42 @@ __global__ void pm_retire_kernel(uint8_t* on, const uint32_t* list, uint32_t n, 
   }
 }
 
+// Device arrays and the persistent kernel's launch shape, once the per-LP queue arrays exist.
+gpq_status finish_create(gpq_phold_session* s, uint32_t max_instances) {
+  cudaError_t e = dmalloc(&s->inst, max_instances);
+  if (e == cudaSuccess) e = dmalloc(&s->mins, 3ull * max_instances);
+  if (e == cudaSuccess) e = dmalloc(&s->errs, 3ull * max_instances);
+  if (e == cudaSuccess) e = dmalloc(&s->on, max_instances);
+  if (e == cudaSuccess) e = dmalloc(&s->lp_inst, s->max_lps);
+  if (e == cudaSuccess) e = dmalloc(&s->count, s->max_lps);
+  if (e == cudaSuccess) e = dmalloc(&s->csum, s->max_lps);
+  if (e == cudaSuccess) e = dmalloc(&s->ohash, s->max_lps);
+  if (e == cudaSuccess) e = dmalloc(&s->ctl, 1);
+  if (e == cudaSuccess) e = dmalloc(&s->list, max_instances);
+  if (e == cudaSuccess) e = dmalloc(&s->list_n, 1);
+  if (e == cudaSuccess) e = dmalloc(&s->acc, max_instances);
+  if (e == cudaSuccess) e = dmalloc(&s->staged, max_instances);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s->on, 0, max_instances, s->own);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s->lp_inst, 0xff, (size_t)s->max_lps * 4, s->own);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s->ctl, 0, sizeof(PmCtl), s->own);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->own);
+  if (e != cudaSuccess) {
+    set_last_error("gpq_phold_session_create: %s", cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? GPQ_ERR_NOMEM : GPQ_ERR_CUDA;
+  }
+  int dev = 0, sms = 0, per_sm = 0;
+  GPQ_CUDA_TRY(cudaFuncSetAttribute(s->kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem));
+  GPQ_CUDA_TRY(cudaGetDevice(&dev));
+  GPQ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  GPQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, s->kern, (int)s->block, s->smem));
+  if (per_sm < 1) {
+    set_last_error("phold session: kernel does not fit on an SM");
+    return GPQ_ERR_INVALID;
+  }
+  s->grid = per_sm * sms;
+  return GPQ_OK;
+}
+
 gpq_status flush_pending(gpq_phold_session* s, cudaStream_t st) {
   const uint32_t n = (uint32_t)s->pending.size();
   if (n == 0) return GPQ_OK;
@@ -126,6 +168,17 @@ gpq_status flush_pending(gpq_phold_session* s, cudaStream_t st) {
   GPQ_CUDA_TRY(cudaMemcpyAsync(s->list, s->pending.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
   pm_admit_kernel<<<(n + 127) / 128, 128, 0, st>>>(s->inst, s->mins, s->errs, s->on, dstaged, s->list, n);
   const PmDev d = session_dev(s);
+  if (s->bucketed) {
+    for (uint32_t j0 = 0; j0 < n; j0 += 65535) {
+      const uint32_t nj = std::min<uint32_t>(65535, n - j0);
+      const uint32_t gx = std::min<uint32_t>((max_lps + 7) / 8, 1024);
+      pmb_populate_kernel<<<dim3(gx, nj), 256, 0, st>>>(d, s->b, s->list + j0, s->next_window);
+    }
+    GPQ_CUDA_TRY(cudaGetLastError());
+    GPQ_CUDA_TRY(cudaStreamSynchronize(st));
+    s->pending.clear();
+    return GPQ_OK;
+  }
   const uint32_t block = 256, wpb = block / 32;
   const size_t smem = (size_t)wpb * max_p * (sizeof(gpq_item) + sizeof(uint64_t));
   GPQ_CUDA_TRY(cudaFuncSetAttribute(pm_populate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -167,29 +220,12 @@ gpq_status gpq_phold_session_create(uint32_t max_lps, uint32_t capacity, uint32_
   s->h_inst.assign(max_instances, PmInstDev{});
   for (uint32_t i = max_instances; i-- > 0;) s->free_slots.push_back(i);
   cudaError_t e = cudaStreamCreateWithFlags(&s->own, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = dmalloc(&s->inst, max_instances);
-  if (e == cudaSuccess) e = dmalloc(&s->mins, 3ull * max_instances);
-  if (e == cudaSuccess) e = dmalloc(&s->errs, 3ull * max_instances);
-  if (e == cudaSuccess) e = dmalloc(&s->on, max_instances);
-  if (e == cudaSuccess) e = dmalloc(&s->lp_inst, max_lps);
   if (e == cudaSuccess) e = dmalloc(&s->ring, (uint64_t)max_lps << s->cap_log2);
   if (e == cudaSuccess) e = dmalloc(&s->rd, max_lps);
   if (e == cudaSuccess) e = dmalloc(&s->wr, max_lps);
   if (e == cudaSuccess) e = dmalloc(&s->ibuf, 2ull * max_lps * insert_capacity);
   if (e == cudaSuccess) e = dmalloc(&s->icnt, 2ull * max_lps);
-  if (e == cudaSuccess) e = dmalloc(&s->count, max_lps);
-  if (e == cudaSuccess) e = dmalloc(&s->csum, max_lps);
-  if (e == cudaSuccess) e = dmalloc(&s->ohash, max_lps);
-  if (e == cudaSuccess) e = dmalloc(&s->ctl, 1);
-  if (e == cudaSuccess) e = dmalloc(&s->list, max_instances);
-  if (e == cudaSuccess) e = dmalloc(&s->list_n, 1);
-  if (e == cudaSuccess) e = dmalloc(&s->acc, max_instances);
-  if (e == cudaSuccess) e = dmalloc(&s->staged, max_instances);
-  if (e == cudaSuccess) e = cudaMemsetAsync(s->on, 0, max_instances, s->own);
-  if (e == cudaSuccess) e = cudaMemsetAsync(s->lp_inst, 0xff, (size_t)max_lps * 4, s->own);
   if (e == cudaSuccess) e = cudaMemsetAsync(s->icnt, 0, 2ull * max_lps * 4, s->own);
-  if (e == cudaSuccess) e = cudaMemsetAsync(s->ctl, 0, sizeof(PmCtl), s->own);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s->own);
   if (e != cudaSuccess) {
     set_last_error("gpq_phold_session_create: %s", cudaGetErrorString(e));
     gpq_phold_session_destroy(s);
@@ -197,25 +233,67 @@ gpq_status gpq_phold_session_create(uint32_t max_lps, uint32_t capacity, uint32_
   }
   s->kern = pm_kernel(s->group);
   s->smem = (size_t)(s->block / s->group) * laq_group_smem_bytes(s->ibc, s->group);
-  int dev = 0, sms = 0, per_sm = 0;
-  GPQ_CUDA_TRY(cudaFuncSetAttribute(s->kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem));
-  GPQ_CUDA_TRY(cudaGetDevice(&dev));
-  GPQ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  GPQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, s->kern, (int)s->block, s->smem));
-  if (per_sm < 1) {
-    set_last_error("phold session: kernel does not fit on an SM");
+  const gpq_status fs = finish_create(s, max_instances);
+  if (fs != GPQ_OK) {
     gpq_phold_session_destroy(s);
-    return GPQ_ERR_INVALID;
+    return fs;
   }
-  s->grid = per_sm * sms;
+  *out = s;
+  return GPQ_OK;
+}
+
+gpq_status gpq_phold_session_create_bucketed(uint32_t max_lps, uint32_t buckets, uint32_t bucket_slots,
+                                             uint32_t max_instances, gpq_phold_session** out) {
+  GPQ_CHECK_ARG(out, "out is NULL");
+  *out = nullptr;
+  if (buckets == 0) buckets = 32;
+  if (bucket_slots == 0) bucket_slots = 16;
+  GPQ_CHECK_ARG(max_lps >= 1 && max_instances >= 1 && max_instances <= (1u << 20), "need max_lps >= 1, 1 <= max_instances <= 2^20");
+  GPQ_CHECK_ARG(gpq::is_pow2(buckets) && buckets >= 8 && buckets <= 1024, "buckets must be a power of two in [8, 1024]");
+  GPQ_CHECK_ARG(gpq::is_pow2(bucket_slots) && bucket_slots >= 8 && bucket_slots <= 1024,
+                "bucket_slots must be a power of two in [8, 1024]");
+  gpq_phold_session* s = new (std::nothrow) gpq_phold_session();
+  if (!s) return GPQ_ERR_NOMEM;
+  s->bucketed = true;
+  s->max_lps = max_lps;
+  s->max_inst = max_instances;
+  s->block = 512;
+  s->lps.reset(max_lps);
+  s->h_on.assign(max_instances, 0);
+  s->h_inst.assign(max_instances, PmInstDev{});
+  for (uint32_t i = max_instances; i-- > 0;) s->free_slots.push_back(i);
+  LabDev& q = s->b.q;
+  q.nb_log2 = gpq::ilog2_ceil(buckets);
+  q.c_log2 = gpq::ilog2_ceil(bucket_slots);
+  q.F = std::max(64u, bucket_slots);
+  cudaError_t e = cudaStreamCreateWithFlags(&s->own, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = dmalloc(&q.keys, (uint64_t)max_lps << (q.nb_log2 + q.c_log2));
+  if (e == cudaSuccess) e = dmalloc(&q.cnt, (uint64_t)max_lps << q.nb_log2);
+  if (e == cudaSuccess) e = dmalloc(&q.spill, 2ull * max_lps * q.F);
+  if (e == cudaSuccess) e = dmalloc(&q.scnt, 2ull * max_lps);
+  if (e == cudaSuccess) e = dmalloc(&s->b.wj, 4ull * max_instances);
+  if (e == cudaSuccess) e = dmalloc(&s->b.fin, max_instances);
+  if (e != cudaSuccess) {
+    set_last_error("gpq_phold_session_create_bucketed: %s", cudaGetErrorString(e));
+    gpq_phold_session_destroy(s);
+    return e == cudaErrorMemoryAllocation ? GPQ_ERR_NOMEM : GPQ_ERR_CUDA;
+  }
+  s->kern = (const void*)pmb_persistent_kernel;
+  s->smem = lab_cta_smem_bytes(s->block);
+  const gpq_status fs = finish_create(s, max_instances);
+  if (fs != GPQ_OK) {
+    gpq_phold_session_destroy(s);
+    return fs;
+  }
   *out = s;
   return GPQ_OK;
 }
 
 gpq_status gpq_phold_session_destroy(gpq_phold_session* s) {
   if (!s) return GPQ_OK;
-  void* bufs[] = {s->inst, s->mins,  s->errs, s->on,    s->lp_inst, s->ring,   s->rd,  s->wr,    s->ibuf,
-                  s->icnt, s->count, s->csum, s->ohash, s->ctl,     s->list,   s->list_n, s->acc, s->staged};
+  void* bufs[] = {s->inst,   s->mins,   s->errs,     s->on,       s->lp_inst,   s->ring,     s->rd,    s->wr,
+                  s->ibuf,   s->icnt,   s->count,    s->csum,     s->ohash,     s->ctl,      s->list,  s->list_n,
+                  s->acc,    s->staged, s->b.q.keys, s->b.q.cnt, s->b.q.spill, s->b.q.scnt, s->b.wj, s->b.fin};
   for (void* p : bufs)
     if (p) cudaFree(p);
   if (s->own) cudaStreamDestroy(s->own);
@@ -233,8 +311,20 @@ gpq_status gpq_phold_session_admit(gpq_phold_session* s, const gpq_phold_config*
     const gpq_status v = gpq::validate_phold_config(&c);
     if (v != GPQ_OK) return v;
   }
-  GPQ_CHECK_ARG(c.events_per_lp <= (1u << s->cap_log2), "events_per_lp above the session's queue capacity");
+  if (!s->bucketed)
+    GPQ_CHECK_ARG(c.events_per_lp <= (1u << s->cap_log2), "events_per_lp above the session's queue capacity");
   GPQ_CHECK_ARG(c.events_per_lp <= 1024, "events_per_lp above 1024");
+  uint32_t inv_bits = 0;
+  if (s->bucketed) {
+    // the run's bucket width: about 6 events in an LP's front bucket, a window spanning at
+    // most lookahead / 2.5 buckets, and the session's NB buckets covering lookahead + 7
+    const double la = c.lookahead, E = c.events_per_lp, NB = (double)(1u << s->b.q.nb_log2);
+    const double w = std::max(std::max(6.0 * (la + 1.0) / E, la / 2.5), (la + 7.0) / NB);
+    const float inv = (float)(1.0 / w);
+    GPQ_CHECK_ARG((double)c.lookahead * inv + 3.0 <= NB, "lookahead too wide for the session's buckets");
+    GPQ_CHECK_ARG(((double)c.end_time + la + 20.0) * inv < 2147483648.0, "end_time too large for the bucket width");
+    std::memcpy(&inv_bits, &inv, 4);
+  }
   if (s->free_slots.empty()) return GPQ_ERR_NOMEM;
   uint64_t lp0 = 0;
   if (!s->lps.alloc(c.num_lps, &lp0)) return GPQ_ERR_NOMEM;
@@ -244,6 +334,7 @@ gpq_status gpq_phold_session_admit(gpq_phold_session* s, const gpq_phold_config*
   I.p = gpq::phold_params_of(c);
   I.lp0 = (uint32_t)lp0;
   I.per_lp = c.events_per_lp;
+  I.aux = inv_bits;
   s->h_inst[i] = I;
   s->h_on[i] = 1;
   s->pending.push_back(i);
@@ -262,10 +353,13 @@ gpq_status gpq_phold_session_step(gpq_phold_session* s, uint32_t windows, uint32
   if (running) *running = s->active;
   if (s->active == 0) return GPQ_OK;
   PmDev d = session_dev(s);
+  PmbDev b = s->b;
   uint32_t s0 = s->next_window, sw = windows;
   void* args[] = {&d, &s0, &sw};
+  void* bargs[] = {&d, &b, &s0, &sw};
   GPQ_CUDA_TRY(cudaMemsetAsync(&s->ctl->bar, 0, sizeof(unsigned long long), st));
-  GPQ_CUDA_TRY(cudaLaunchCooperativeKernel(s->kern, dim3(s->grid), dim3(s->block), args, s->smem, st));
+  GPQ_CUDA_TRY(cudaLaunchCooperativeKernel(s->kern, dim3(s->grid), dim3(s->block), s->bucketed ? bargs : args,
+                                           s->smem, st));
   PmCtl ctl{};
   GPQ_CUDA_TRY(cudaMemcpyAsync(&ctl, s->ctl, sizeof(PmCtl), cudaMemcpyDeviceToHost, st));
   GPQ_CUDA_TRY(cudaStreamSynchronize(st));
@@ -300,7 +394,8 @@ gpq_status gpq_phold_session_collect(gpq_phold_session* s, uint32_t* slots, gpq_
   for (uint32_t j0 = 0; j0 < n; j0 += 65535) {
     const uint32_t nj = std::min<uint32_t>(65535, n - j0);
     const uint32_t gx = std::min<uint32_t>((max_lps + 7) / 8, 256);
-    pm_finalize_kernel<<<dim3(gx, nj), 256, 0, st>>>(d, s->list + j0, s->acc + j0);
+    if (s->bucketed) pmb_finalize_kernel<<<dim3(gx, nj), 256, 0, st>>>(d, s->b, s->list + j0, s->acc + j0);
+    else pm_finalize_kernel<<<dim3(gx, nj), 256, 0, st>>>(d, s->list + j0, s->acc + j0);
   }
   std::vector<uint32_t> list(n);
   std::vector<PmAcc> acc(n);
@@ -347,6 +442,15 @@ gpq_status gpq_phold_session_usage(gpq_phold_session* s, uint64_t* lps_used, uin
   if (lps_used) *lps_used = s->lps.used();
   if (instances) *instances = s->active;
   return GPQ_OK;
+}
+
+uint64_t gpq_phold_session_bytes_bucketed(uint32_t max_lps, uint32_t buckets, uint32_t bucket_slots,
+                                          uint32_t max_instances) {
+  if (buckets == 0) buckets = 32;
+  if (bucket_slots == 0) bucket_slots = 16;
+  const uint64_t F = std::max(64u, bucket_slots);
+  const uint64_t per_lp = 8ull * buckets * bucket_slots + 4ull * buckets + 16 * F + 8 + 4 * 2 + 8 * 2;
+  return per_lp * max_lps + (uint64_t)max_instances * (sizeof(PmInstDev) + 24 + 1 + 4 + sizeof(PmAcc) + 20);
 }
 
 uint64_t gpq_phold_session_bytes(uint32_t max_lps, uint32_t capacity, uint32_t insert_capacity,

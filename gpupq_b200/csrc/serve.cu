@@ -61,12 +61,14 @@ gpq_status serve_batched(const gpq_serve_config& c, const gpq_serve_request* req
   const uint32_t cap = c.phold_capacity ? c.phold_capacity : 256;
   const uint32_t ibc = c.phold_insert_capacity ? c.phold_insert_capacity : 64;
   const uint64_t p_bytes = budget - std::min(budget, a_bytes);
-  const uint64_t per_lp = 16ull * cap + 32ull * ibc + 40;
+  const bool buckets = c.phold_form == 1;
+  const uint64_t per_lp = buckets ? gpq_phold_session_bytes_bucketed(1, 0, 0, 0) : 16ull * cap + 32ull * ibc + 40;
   const uint32_t max_lps = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(p_bytes / per_lp, 1024), 1u << 30);
   Sessions ss;
   gpq_status st = gpq_astar_session_create(&ac, max_cells, max_tiles, max_inst, &ss.astar);
   if (st != GPQ_OK) return st;
-  st = gpq_phold_session_create(max_lps, cap, ibc, max_inst, c.phold_lanes_per_lp, &ss.phold);
+  st = buckets ? gpq_phold_session_create_bucketed(max_lps, 0, 0, max_inst, &ss.phold)
+               : gpq_phold_session_create(max_lps, cap, ibc, max_inst, c.phold_lanes_per_lp, &ss.phold);
   if (st != GPQ_OK) return st;
   const uint32_t R = c.astar_rounds ? c.astar_rounds : 32;
   const uint32_t W = c.phold_windows ? c.phold_windows : 32;

@@ -364,6 +364,14 @@ typedef struct gpq_phold_session gpq_phold_session;
 GPQ_API gpq_status gpq_phold_session_create(uint32_t max_lps, uint32_t capacity, uint32_t insert_capacity,
                                             uint32_t max_instances, uint32_t lanes_per_lp,
                                             gpq_phold_session** out);
+/* A session whose LP space holds time buckets instead of sorted rings (the bucketed local
+ * array queue, gpq_phold_config.laq_mode 2): `buckets` buckets of `bucket_slots` keys per
+ * LP (powers of two; 0 = 32 and 16) and spill lists of max(64, bucket_slots) keys.  An
+ * admitted run gets a bucket width from its lookahead and events_per_lp; a run whose
+ * lookahead needs more buckets is refused (GPQ_ERR_INVALID).  Same results as the sorted
+ * form. */
+GPQ_API gpq_status gpq_phold_session_create_bucketed(uint32_t max_lps, uint32_t buckets, uint32_t bucket_slots,
+                                                     uint32_t max_instances, gpq_phold_session** out);
 GPQ_API gpq_status gpq_phold_session_destroy(gpq_phold_session* s);
 
 /* Admit one run (its queue_kind, capacity, insert_capacity and loop fields are ignored:
@@ -381,6 +389,8 @@ GPQ_API gpq_status gpq_phold_session_collect(gpq_phold_session* s, uint32_t* slo
 GPQ_API gpq_status gpq_phold_session_usage(gpq_phold_session* s, uint64_t* lps_used, uint32_t* instances);
 GPQ_API uint64_t gpq_phold_session_bytes(uint32_t max_lps, uint32_t capacity, uint32_t insert_capacity,
                                          uint32_t max_instances);
+GPQ_API uint64_t gpq_phold_session_bytes_bucketed(uint32_t max_lps, uint32_t buckets, uint32_t bucket_slots,
+                                                  uint32_t max_instances);
 
 /* ---------------------------------------------------------------------------------- */
 /* 2c. Serving: a stream of A* queries and PHOLD runs                                  */
@@ -419,8 +429,9 @@ typedef struct gpq_serve_config {
   gpq_astar_config astar;
   uint32_t phold_capacity;        /* per-LP queue capacity; 0 = 256 */
   uint32_t phold_insert_capacity; /* per-LP children per window; 0 = 64 */
-  uint32_t phold_lanes_per_lp;    /* 0 = 8 */
-  uint32_t reserved[5];
+  uint32_t phold_lanes_per_lp;    /* sorted form: lanes per LP; 0 = 8 */
+  uint32_t phold_form;            /* 0 = sorted rings, 1 = time buckets (gpq_phold_session_create_bucketed) */
+  uint32_t reserved[4];
 } gpq_serve_config;
 
 typedef struct gpq_serve_stats {

@@ -47,9 +47,10 @@ def _same(a, b):
     assert a["status"] == 0 and b["status"] == 0
 
 
-def test_batch_equals_alone(gpu_lib):
+@pytest.mark.parametrize("bucketed", [False, True])
+def test_batch_equals_alone(gpu_lib, bucketed):
     runs = _runs(1, 24)
-    with G.PholdSession(max_lps=sum(c.num_lps for c in runs), max_instances=64) as s:
+    with G.PholdSession(max_lps=sum(c.num_lps for c in runs), max_instances=64, bucketed=bucketed) as s:
         slot_of = {s.admit(c): i for i, c in enumerate(runs)}
         s.step(0)
         got = {slot_of[sl]: r for sl, r in s.collect()}
@@ -59,14 +60,15 @@ def test_batch_equals_alone(gpu_lib):
         _same(got[i], _alone(c))
 
 
+@pytest.mark.parametrize("bucketed", [False, True])
 @pytest.mark.parametrize("windows", [1, 5, 40])
-def test_stream_equals_alone(gpu_lib, windows):
+def test_stream_equals_alone(gpu_lib, windows, bucketed):
     """Runs admitted while others are mid-run, into an LP space that holds only some of
-    them at a time."""
+    them at a time (LPs and slots of finished runs are reused)."""
     runs = _runs(2, 20)
     want = [_alone(c) for c in runs]
     got, slot_of, pending, refused = {}, {}, list(range(len(runs))), 0
-    with G.PholdSession(max_lps=4000, max_instances=8) as s:
+    with G.PholdSession(max_lps=4000, max_instances=8, bucketed=bucketed) as s:
         for _ in range(100000):
             while pending:
                 sl = s.admit(runs[pending[0]])

@@ -47,13 +47,15 @@ def _compare(batched, plain, reqs, n):
                 assert getattr(batched[i].phold, k) == getattr(plain[i].phold, k), (i, k)
 
 
+@pytest.mark.parametrize("phold_form", [0, 1])
 @pytest.mark.parametrize("realtime", [False, True])
-def test_mix_equals_alone(gpu_lib, realtime):
+def test_mix_equals_alone(gpu_lib, realtime, phold_form):
+    """PHOLD runs kept in sorted rings (form 0) or time buckets (form 1) while served."""
     n = 60
     reqs = _mixed(n, 5)
     plain, ps = G.serve(reqs, n, mode=G.SERVE_PLAIN, realtime=realtime, tile=32)
     batched, bs = G.serve(reqs, n, mode=G.SERVE_BATCHED, realtime=realtime, budget=4 << 30, astar_rounds=8,
-                          phold_windows=8, tile=32)
+                          phold_windows=8, tile=32, phold_form=phold_form)
     _compare(batched, plain, reqs, n)
     assert bs["max_resident"] > 1
     for s in (ps, bs):
