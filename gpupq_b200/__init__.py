@@ -100,6 +100,8 @@ _SIGS = {
     "gpq_phold_lp_stats": ([_VP, _VP, _VP, _VP, _VP], ctypes.c_int),
     "gpq_phold_initial_events": ([ctypes.POINTER(PholdConfig), _VP, ctypes.c_uint64], ctypes.c_int),
     "gpq_phold_children": ([ctypes.POINTER(PholdConfig), _VP, _VP, ctypes.c_uint64], ctypes.c_int),
+    "gpq_phold_snapshot": ([_VP, _VP, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64), _VP], ctypes.c_int),
+    "gpq_phold_restore": ([_VP, _VP, ctypes.c_uint64, _VP], ctypes.c_int),
     "gpq_phold_launch_info": ([_VP, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32),
                                ctypes.POINTER(ctypes.c_uint32)], ctypes.c_int),
     "gpq_phold_run_static": ([ctypes.POINTER(PholdConfig), _VP, _VP, _VP, _VP, ctypes.POINTER(PholdResult), _VP],
@@ -130,6 +132,7 @@ _SIGS = {
     "gpq_astar_path": ([_VP, ctypes.c_uint32, _VP, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32), _VP],
                        ctypes.c_int),
     "gpq_astar_gcost": ([_VP, ctypes.c_uint32, _VP, ctypes.c_uint64, _VP], ctypes.c_int),
+    "gpq_astar_write_ppm": ([_VP, ctypes.c_uint32, ctypes.c_char_p, _VP], ctypes.c_int),
     "gpq_astar_query": ([ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                          ctypes.c_double, ctypes.c_double, _VP], ctypes.c_int),
     "gpq_astar_session_create": ([_VP, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(_VP)],
@@ -292,6 +295,18 @@ class Phold:
         d = r.as_dict()
         d["status_code"] = st
         return d
+
+    def snapshot(self, stream=None):
+        """The run's whole state between windows (gpq_phold_snapshot) as a uint8 array."""
+        n = ctypes.c_uint64()
+        check(lib().gpq_phold_snapshot(self._h, None, 0, ctypes.byref(n), stream), "gpq_phold_snapshot")
+        buf = np.zeros(n.value, np.uint8)
+        check(lib().gpq_phold_snapshot(self._h, _ptr(buf), n.value, ctypes.byref(n), stream), "gpq_phold_snapshot")
+        return buf
+
+    def restore(self, buf, stream=None):
+        buf = np.ascontiguousarray(buf, dtype=np.uint8)
+        check(lib().gpq_phold_restore(self._h, _ptr(buf), len(buf), stream), "gpq_phold_restore")
 
     def launch_info(self):
         g, b, n = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
@@ -519,6 +534,10 @@ class AStar:
         out = np.zeros(cells, np.uint32)
         check(lib().gpq_astar_gcost(self._h, index, _ptr(out), cells, None), "gpq_astar_gcost")
         return out
+
+    def write_ppm(self, index, filename):
+        """Binary PPM image of instance `index` of the last solve (gpq_astar_write_ppm)."""
+        check(lib().gpq_astar_write_ppm(self._h, index, os.fsencode(filename), None), "gpq_astar_write_ppm")
 
 
 class AStarSession:

@@ -2,6 +2,7 @@
 // launch and the per-instance results.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <vector>
 
@@ -386,6 +387,65 @@ gpq_status gpq_astar_gcost(gpq_astar* a, uint32_t index, uint32_t* g, uint64_t c
   const cudaStream_t st = gpq::as_stream(stream, a->own);
   GPQ_CUDA_TRY(cudaMemcpyAsync(g, a->gcost + I.cell0, cells * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
   GPQ_CUDA_TRY(cudaStreamSynchronize(st));
+  return GPQ_OK;
+}
+
+// Headless image of instance `index` (the reference's dumpResult, src/a_star.cu:596-690,
+// writes a P6 image of its agents' map; here one search is drawn): binary PPM, one pixel
+// per cell, row 0 at the top.  Colours: free cell not reached black (0,0,0); blocked grey
+// (90,90,90); reached but beyond the optimal cost dark blue (0,0,110); expanded
+// (g + h <= C*) light blue (60,140,255); the canonical path red (255,40,40); start green
+// (0,220,0); goal yellow (255,230,0).
+gpq_status gpq_astar_write_ppm(gpq_astar* a, uint32_t index, const char* filename, void* stream) {
+  GPQ_CHECK_ARG(a && filename, "NULL argument");
+  if (!a->solved) return GPQ_ERR_NOT_READY;
+  GPQ_CHECK_ARG(index < a->n_inst, "index out of range");
+  const gpq_astar_grid G = a->h_inst[index].g;
+  const uint64_t cells = (uint64_t)G.width * G.height;
+  GPQ_CHECK_ARG(cells <= (1ull << 28), "grid above 2^28 cells");
+  std::vector<uint32_t> g(cells);
+  gpq_status st = gpq_astar_gcost(a, index, g.data(), cells, stream);
+  if (st != GPQ_OK) return st;
+  uint32_t len = 0;
+  st = gpq_astar_path(a, index, nullptr, 0, &len, stream);
+  if (st != GPQ_OK && st != GPQ_ERR_INVALID) return st;
+  std::vector<uint32_t> path(len);
+  if (len) {
+    st = gpq_astar_path(a, index, path.data(), len, &len, stream);
+    if (st != GPQ_OK) return st;
+  }
+  const uint32_t cs = g[G.goal];
+  std::vector<unsigned char> px(cells * 3, 0);
+  auto put = [&](uint64_t c, unsigned char r, unsigned char gg, unsigned char b) {
+    px[3 * c] = r;
+    px[3 * c + 1] = gg;
+    px[3 * c + 2] = b;
+  };
+  for (uint64_t c = 0; c < cells; ++c) {
+    const uint32_t cell = (uint32_t)c;
+    if (gpq_astar_blocked(&G, cell)) {
+      put(c, 90, 90, 90);
+    } else if (g[c] != GPQ_ASTAR_INF) {
+      const bool exp = cs == GPQ_ASTAR_INF || (uint64_t)g[c] + gpq_astar_h(G.conn, cell, G.goal, G.width) <= cs;
+      if (exp) put(c, 60, 140, 255);
+      else put(c, 0, 0, 110);
+    }
+  }
+  for (uint32_t i = 0; i < len; ++i) put(path[i], 255, 40, 40);
+  put(G.start, 0, 220, 0);
+  put(G.goal, 255, 230, 0);
+  FILE* f = std::fopen(filename, "wb");
+  if (!f) {
+    set_last_error("gpq_astar_write_ppm: cannot open %s", filename);
+    return GPQ_ERR_INVALID;
+  }
+  const int hn = std::fprintf(f, "P6\n%u %u\n255\n", G.width, G.height);
+  const size_t wn = std::fwrite(px.data(), 1, px.size(), f);
+  const int cl = std::fclose(f);
+  if (hn <= 0 || wn != px.size() || cl != 0) {
+    set_last_error("gpq_astar_write_ppm: writing %s failed", filename);
+    return GPQ_ERR_INVALID;
+  }
   return GPQ_OK;
 }
 

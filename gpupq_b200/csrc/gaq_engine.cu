@@ -133,6 +133,27 @@ gpq_status gaq_engine_create(const gpq_phold_config& c, GaqEngine** out) {
 
 void gaq_engine_destroy(GaqEngine* g) { delete g; }
 
+void gaq_engine_state(GaqEngine* g, std::vector<std::pair<void*, size_t>>* dev,
+                      std::vector<std::pair<void*, size_t>>* host) {
+  const size_t cap = g->cap, L = g->c.num_lps;
+  dev->push_back({g->arr[0], cap * sizeof(gpq_item)});
+  dev->push_back({g->arr[1], cap * sizeof(gpq_item)});
+  dev->push_back({g->ch, cap * sizeof(gpq_item)});
+  dev->push_back({g->ch_tmp, cap * sizeof(gpq_item)});
+  dev->push_back({g->stg, L * g->c.insert_capacity * sizeof(gpq_item)});
+  dev->push_back({g->stg_cnt, L * sizeof(uint32_t)});
+  dev->push_back({g->info, 8 * sizeof(uint32_t)});
+  dev->push_back({g->hist, (size_t)256 * std::max<uint32_t>(1u, (g->cap + kWinRsTile - 1) / kWinRsTile) * sizeof(uint32_t)});
+  dev->push_back({g->acc, 8 * sizeof(unsigned long long)});
+  dev->push_back({g->win, sizeof(GaqWin)});
+  dev->push_back({g->dig, 256 * sizeof(uint32_t)});
+  dev->push_back({g->split, ((g->cap + kMpTile - 1) / kMpTile + 2) * sizeof(uint32_t)});
+  host->push_back({&g->cur, sizeof(g->cur)});
+  host->push_back({&g->n, sizeof(g->n)});
+  host->push_back({g->h_info, 8 * sizeof(uint32_t)});
+  host->push_back({g->h_win, sizeof(GaqWin)});
+}
+
 gpq_status gaq_engine_populate(GaqEngine* g, const PholdDev& d, const gpq_item* dev_src, cudaStream_t st) {
   const gpq_phold_config& c = g->c;
   gaq_zero_stats_kernel<<<std::max(1u, std::min<uint32_t>((c.num_lps + 255) / 256, 4096)), 256, 0, st>>>(d);

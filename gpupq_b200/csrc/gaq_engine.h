@@ -4,6 +4,9 @@
 
 #include <cuda_runtime.h>
 
+#include <utility>
+#include <vector>
+
 #include "gpq.h"
 
 struct PholdDev;
@@ -33,5 +36,8 @@ gpq_status gaq_engine_run(GaqEngine* g, const PholdDev& d, uint32_t nsteps, int*
 // committed, pending, pending_csum, digest, pending_min (as float bits)
 gpq_status gaq_engine_finalize(GaqEngine* g, const PholdDev& d, uint64_t out[4], uint32_t* pmin, cudaStream_t st);
 uint32_t gaq_engine_launches_per_window();
+// The engine's state for snapshots: its device buffers and host words (pointer, bytes).
+void gaq_engine_state(GaqEngine* g, std::vector<std::pair<void*, size_t>>* dev,
+                      std::vector<std::pair<void*, size_t>>* host);
 
 }  // namespace gpq

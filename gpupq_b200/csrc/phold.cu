@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cstring>
 #include <new>
+#include <utility>
 #include <vector>
 
 #include "host_common.h"
@@ -568,6 +569,143 @@ gpq_status gpq_phold_launch_info(gpq_phold* h, uint32_t* grid, uint32_t* block, 
     *launches_per_run = h->is_hq ? 1u
                       : h->gaq ? (uint32_t)(h->gaq_windows * gpq::gaq_engine_launches_per_window())
                                : (h->cfg.loop_mode == GPQ_LOOP_PERSISTENT) ? 1u : h->phase;
+  return GPQ_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Every device buffer the handle owns (pointer, bytes) and its host-side state words: the
+// whole state of a run between windows.
+void phold_state(gpq_phold* h, std::vector<std::pair<void*, size_t>>* dev,
+                 std::vector<std::pair<void*, size_t>>* host) {
+  const gpq_phold_config& c = h->cfg;
+  const size_t L = c.num_lps;
+  auto add = [&](void* p, size_t n) {
+    if (p && n) dev->push_back({p, n});
+  };
+  add(h->items, (L << h->cap_log2) * sizeof(gpq_item));
+  add(h->qa, L * sizeof(uint32_t));
+  add(h->qb, L * sizeof(uint32_t));
+  add(h->qc, L * sizeof(uint32_t));
+  add(h->links, (L << h->cap_log2) * sizeof(uint32_t));
+  add(h->freestk, (L << h->cap_log2) * sizeof(uint16_t));
+  add(h->ibuf, 2 * L * c.insert_capacity * sizeof(gpq_item));
+  add(h->icnt, 2 * L * sizeof(uint32_t));
+  add(h->count, L * sizeof(uint32_t));
+  add(h->csum, L * sizeof(unsigned long long));
+  add(h->ohash, L * sizeof(unsigned long long));
+  add(h->ctrl, sizeof(PholdCtrl));
+  if (h->is_lab) {
+    const LabDev& q = h->lab;
+    add(q.keys, (L << (q.nb_log2 + q.c_log2)) * sizeof(unsigned long long));
+    add(q.cnt, (L << q.nb_log2) * sizeof(uint32_t));
+    add(q.spill, 2 * L * q.F * sizeof(unsigned long long));
+    add(q.scnt, 2 * L * sizeof(uint32_t));
+    add(q.wj, 4 * sizeof(uint32_t));
+  }
+  if (h->is_hq) {
+    const uint64_t N = (uint64_t)c.num_lps * c.events_per_lp;
+    add(h->hq.nodes, (size_t)h->hq.maxnodes * h->hq.r * sizeof(gpq_item));
+    add(h->hq.cnt, (size_t)h->hq.maxnodes * sizeof(uint32_t));
+    add(h->hq.meta, 4 * sizeof(uint32_t));
+    add(h->hq_sort[0], N * sizeof(gpq_item));
+    add(h->hq_sort[1], N * sizeof(gpq_item));
+    add(h->hq_mm, 2 * sizeof(uint32_t));
+  }
+  if (h->gaq) gpq::gaq_engine_state(h->gaq, dev, host);
+  host->push_back({&h->phase, sizeof(h->phase)});
+  host->push_back({&h->gaq_windows, sizeof(h->gaq_windows)});
+  host->push_back({&h->hq_windows, sizeof(h->hq_windows)});
+  host->push_back({&h->populated, sizeof(h->populated)});
+}
+
+constexpr uint64_t kSnapMagic = 0x3150414e53515047ull;  // "GPQSNAP1"
+
+}  // namespace
+
+extern "C" {
+
+gpq_status gpq_phold_snapshot(gpq_phold* h, void* buf, uint64_t capacity, uint64_t* size, void* stream) {
+  GPQ_CHECK_ARG(h && size, "NULL argument");
+  std::vector<std::pair<void*, size_t>> dev, host;
+  phold_state(h, &dev, &host);
+  uint64_t need = 8 + sizeof(gpq_phold_config) + 8;
+  for (auto& r : dev) need += 8 + r.second;
+  for (auto& r : host) need += 8 + r.second;
+  *size = need;
+  if (!buf) return GPQ_OK;
+  GPQ_CHECK_ARG(capacity >= need, "capacity below the snapshot size");
+  GPQ_CHECK_ARG(h->populated, "gpq_phold_snapshot before gpq_phold_populate");
+  const cudaStream_t st = gpq::as_stream(stream, h->own);
+  unsigned char* p = static_cast<unsigned char*>(buf);
+  auto put = [&](const void* src, size_t n) {
+    std::memcpy(p, src, n);
+    p += n;
+  };
+  put(&kSnapMagic, 8);
+  put(&h->cfg, sizeof(gpq_phold_config));
+  const uint32_t counts[2] = {(uint32_t)dev.size(), (uint32_t)host.size()};
+  put(counts, 8);
+  GPQ_CUDA_TRY(cudaStreamSynchronize(st));
+  for (auto& r : dev) {
+    const uint64_t n = r.second;
+    put(&n, 8);
+    GPQ_CUDA_TRY(cudaMemcpyAsync(p, r.first, n, cudaMemcpyDeviceToHost, st));
+    p += n;
+  }
+  for (auto& r : host) {
+    const uint64_t n = r.second;
+    put(&n, 8);
+    put(r.first, n);
+  }
+  GPQ_CUDA_TRY(cudaStreamSynchronize(st));
+  return GPQ_OK;
+}
+
+gpq_status gpq_phold_restore(gpq_phold* h, const void* buf, uint64_t size, void* stream) {
+  GPQ_CHECK_ARG(h && buf, "NULL argument");
+  std::vector<std::pair<void*, size_t>> dev, host;
+  phold_state(h, &dev, &host);
+  const unsigned char* p = static_cast<const unsigned char*>(buf);
+  const unsigned char* end = p + size;
+  auto take = [&](void* dst, size_t n) -> bool {
+    if ((uint64_t)(end - p) < n) return false;
+    if (dst) std::memcpy(dst, p, n);
+    p += n;
+    return true;
+  };
+  uint64_t magic = 0;
+  gpq_phold_config cfg{};
+  uint32_t counts[2] = {0, 0};
+  GPQ_CHECK_ARG(take(&magic, 8) && magic == kSnapMagic, "not a PHOLD snapshot");
+  GPQ_CHECK_ARG(take(&cfg, sizeof(cfg)) && std::memcmp(&cfg, &h->cfg, sizeof(cfg)) == 0,
+                "snapshot of a run with another configuration");
+  GPQ_CHECK_ARG(take(counts, 8) && counts[0] == dev.size() && counts[1] == host.size(), "snapshot layout differs");
+  // check every region's size before anything is overwritten
+  const unsigned char* scan = p;
+  for (size_t i = 0; i < dev.size() + host.size(); ++i) {
+    const size_t want = i < dev.size() ? dev[i].second : host[i - dev.size()].second;
+    uint64_t n = 0;
+    GPQ_CHECK_ARG((uint64_t)(end - scan) >= 8, "snapshot truncated");
+    std::memcpy(&n, scan, 8);
+    GPQ_CHECK_ARG(n == want && (uint64_t)(end - scan - 8) >= n, "snapshot region differs or is truncated");
+    scan += 8 + n;
+  }
+  const cudaStream_t st = gpq::as_stream(stream, h->own);
+  GPQ_CUDA_TRY(cudaStreamSynchronize(st));
+  for (auto& r : dev) {
+    p += 8;
+    GPQ_CUDA_TRY(cudaMemcpyAsync(r.first, p, r.second, cudaMemcpyHostToDevice, st));
+    p += r.second;
+  }
+  for (auto& r : host) {
+    p += 8;
+    take(r.first, r.second);
+  }
+  GPQ_CUDA_TRY(cudaStreamSynchronize(st));
+  h->finalized = false;
   return GPQ_OK;
 }
 

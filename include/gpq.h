@@ -218,6 +218,15 @@ GPQ_API gpq_status gpq_phold_initial_events(const gpq_phold_config* cfg, gpq_ite
 GPQ_API gpq_status gpq_phold_children(const gpq_phold_config* cfg, const gpq_item* events, gpq_item* children,
                               uint64_t n);
 
+/* Snapshot of a run's whole state between windows (its queues, per-LP outputs, window
+ * slots and window count) into a HOST buffer, and its restore into a handle created with
+ * the same configuration; the restored run continues exactly as the original would.  The
+ * reference has no checkpoint; this lets a caller stop a long run and resume it later, or
+ * run one prefix and branch several continuations from it.  With buf == NULL,
+ * gpq_phold_snapshot only reports the size.  Both block on the stream. */
+GPQ_API gpq_status gpq_phold_snapshot(gpq_phold* h, void* buf, uint64_t capacity, uint64_t* size, void* stream);
+GPQ_API gpq_status gpq_phold_restore(gpq_phold* h, const void* buf, uint64_t size, void* stream);
+
 /* Launch geometry of the last gpq_phold_run: persistent grid (CTAs), CTA size, and the
  * number of kernel launches the run made (1 for the persistent loop, one per window
  * for the plain loop). */
@@ -308,6 +317,14 @@ GPQ_API gpq_status gpq_astar_path(gpq_astar* a, uint32_t index, uint32_t* cells,
 
 /* The g values of instance `index` of the last solve (HOST array of width * height). */
 GPQ_API gpq_status gpq_astar_gcost(gpq_astar* a, uint32_t index, uint32_t* g, uint64_t capacity, void* stream);
+
+/* Headless image of instance `index` of the last solve (the reference's path image,
+ * dumpResult in src/a_star.cu:596-690, without its GL or agent map): a binary PPM file
+ * (P6), one pixel per cell, row 0 at the top, colours: free unreached black, blocked grey
+ * (90,90,90), reached but above the optimal cost dark blue (0,0,110), expanded
+ * (g + h <= C*) light blue (60,140,255), canonical path red (255,40,40), start green
+ * (0,220,0), goal yellow (255,230,0).  Grids up to 2^28 cells.  Blocks on the stream. */
+GPQ_API gpq_status gpq_astar_write_ppm(gpq_astar* a, uint32_t index, const char* filename, void* stream);
 
 /* Resident A* instances for serving.  No counterpart in the reference, whose agents run
  * to completion inside one a_star launch (src/a_star.cu:269-593).  A session reserves a

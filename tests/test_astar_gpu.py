@@ -149,3 +149,39 @@ def test_session_stream_matches_oracle(gpu_lib, rounds):
         assert r["status"] == 0
         for k in FIELDS:
             assert int(r[k]) == want[i][k], (i, k)
+
+
+def _read_ppm(path):
+    data = open(path, "rb").read()
+    parts = data.split(b"\n", 3)
+    assert parts[0] == b"P6" and parts[2] == b"255"
+    w, h = map(int, parts[1].split())
+    px = np.frombuffer(parts[3], np.uint8).reshape(h, w, 3)
+    return w, h, px
+
+
+def test_path_image(gpu_lib, tmp_path):
+    """The headless image: one pixel per cell; the expanded cells (light blue, path, start
+    and goal) number the result's expanded count, the red path the path length minus its
+    two ends, and the grey cells the oracle's blocked cells."""
+    grids = np.concatenate([G.astar_grid(120, 90, 0.25, 4, conn=8, start=5, goal=120 * 90 - 7),
+                            G.astar_grid(64, 64, 0.2, 3)])
+    with G.AStar(tile=16) as a:
+        res = a.solve(grids)
+        for i in range(len(grids)):
+            f = tmp_path / f"img{i}.ppm"
+            a.write_ppm(i, str(f))
+            w, h, px = _read_ppm(f)
+            assert (w, h) == (int(grids[i]["width"]), int(grids[i]["height"]))
+            col = px.reshape(-1, 3)
+            def n(c):
+                return int(np.all(col == np.array(c, np.uint8), axis=1).sum())
+            red, blue, green, yellow = n((255, 40, 40)), n((60, 140, 255)), n((0, 220, 0)), n((255, 230, 0))
+            assert green == 1 and yellow == 1
+            assert red == int(res[i]["path_len"]) - 2
+            assert blue + red + green + yellow == int(res[i]["expanded"])
+            assert n((0, 0, 0)) + n((90, 90, 90)) + n((0, 0, 110)) + int(res[i]["expanded"]) == w * h
+            # reached cells beyond the expanded set depend on the schedule: count them from
+            # this search's own g values
+            gg = a.gcost(i, w * h)
+            assert n((0, 0, 110)) == int((gg != G.ASTAR_INF).sum()) - int(res[i]["expanded"])
