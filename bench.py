@@ -344,7 +344,7 @@ def run_case(name):
             print(a.stats(), int(r["expanded"].sum()), int(r["pops"].sum()), int((r["status"] != 0).sum()))
     elif name == "astar_plain_2048":
         g = G.astar_grid(2048, 2048, 0.2, 3)
-        with G.AStar(tile=32) as a:
+        with G.AStar(tile=64) as a:
             for _ in range(2):
                 r = a.solve(g)
             print(a.stats(), int(r[0]["expanded"]))

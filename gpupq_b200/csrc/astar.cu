@@ -17,6 +17,7 @@ struct gpq_astar {
   cudaEvent_t ev[4] = {};
   // device buffers and their capacities
   uint32_t* gcost = nullptr;
+  uint8_t* pred = nullptr;  // [cap_cells + kAstarPredSlack]
   uint64_t cap_cells = 0;
   uint32_t* blk = nullptr;
   uint64_t* word0 = nullptr;
@@ -108,7 +109,7 @@ gpq_status gpq_astar_create(const gpq_astar_config* cfg, gpq_astar** out) {
 
 gpq_status gpq_astar_destroy(gpq_astar* a) {
   if (!a) return GPQ_OK;
-  void* bufs[] = {a->gcost, a->blk, a->word0, a->inst, a->fin, a->pout, a->tiles, a->inbox, a->open, a->al,
+  void* bufs[] = {a->gcost, a->pred, a->blk, a->word0, a->inst, a->fin, a->pout, a->tiles, a->inbox, a->open, a->al,
                   a->ctl, a->path_buf};
   for (void* p : bufs)
     if (p) cudaFree(p);
@@ -192,6 +193,7 @@ static gpq_status astar_solve_pass(gpq_astar* a, const gpq_astar_grid* grids, ui
   // buffers
   GPQ_TRY(grow(&a->gcost, a->cap_cells, cell0));
   GPQ_TRY(grow(&a->blk, a->cap_cells / 32 + 1, cell0 / 32 + 1));  // +1: tile loads read one word ahead
+  GPQ_TRY(grow(&a->pred, a->cap_cells + kAstarPredSlack, cell0 + kAstarPredSlack));
   a->cap_cells = std::max(a->cap_cells, cell0);
   if (n > a->cap_inst) {
     GPQ_TRY(grow(&a->word0, 0, n));
@@ -212,6 +214,7 @@ static gpq_status astar_solve_pass(gpq_astar* a, const gpq_astar_grid* grids, ui
   d.tiles = a->tiles;
   d.gcost = a->gcost;
   d.blk = a->blk;
+  d.pred = a->pred;
   d.inbox = a->inbox;
   d.open = a->open;
   d.al = a->al;
@@ -238,7 +241,16 @@ static gpq_status astar_solve_pass(gpq_astar* a, const gpq_astar_grid* grids, ui
     set_last_error("astar: kernel does not fit on an SM (block %u, smem %zu)", c.block_threads, smem);
     return GPQ_ERR_INVALID;
   }
-  if (c.ctas_per_sm) per_sm = std::min<int>(per_sm, (int)c.ctas_per_sm);
+  if (c.ctas_per_sm) {
+    per_sm = std::min<int>(per_sm, (int)c.ctas_per_sm);
+  } else {
+    // a search keeps about sqrt(tiles) tiles of an instance active at a time (its
+    // frontier); tile workers beyond the active tiles only add grid-barrier work
+    double active = 0.0;
+    for (uint32_t i = 0; i < n; ++i) active += std::sqrt((double)a->h_inst[i].tiles_x * a->h_inst[i].tiles_y);
+    const double workers = (double)sms * (c.tile_worker ? c.block_threads / 32 : 1);
+    per_sm = std::min<int>(per_sm, std::max<int>(1, (int)std::ceil(active / workers)));
+  }
   const uint32_t grid = (uint32_t)(per_sm * sms);
   a->grid = grid;
   a->block = c.block_threads;
@@ -260,9 +272,11 @@ static gpq_status astar_solve_pass(gpq_astar* a, const gpq_astar_grid* grids, ui
   GPQ_CUDA_TRY(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(c.block_threads), args, smem, st));
   GPQ_CUDA_TRY(cudaEventRecord(a->ev[2], st));
   GPQ_CUDA_TRY(cudaMemsetAsync(a->fin, 0, 2ull * n * sizeof(unsigned long long), st));
-  const uint32_t fx = (uint32_t)std::min<uint64_t>((max_cells + 255) / 256, 64);
+  // about 16 blocks per SM over all instances, at least 64 per instance
+  const uint32_t fx = (uint32_t)std::min<uint64_t>((max_cells + 255) / 256, std::max<uint64_t>(64, 16ull * sms / n));
   astar_finalize_kernel<<<dim3(fx, n), 256, 0, st>>>(d, nullptr, a->fin);
-  astar_path_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>(d, nullptr, n, a->pout, 0xFFFFFFFFu, nullptr, 0);
+  if (max_cells >= kAstarPredBytesCells) astar_pred_kernel<<<dim3(fx, n), 256, 0, st>>>(d, nullptr);
+  astar_path_kernel<<<n, kPathThreads, 0, st>>>(d, nullptr, n, a->pout, 0xFFFFFFFFu, nullptr, 0);
   GPQ_CUDA_TRY(cudaGetLastError());
   GPQ_CUDA_TRY(cudaEventRecord(a->ev[3], st));
   std::vector<unsigned long long> fin(2ull * n), pout(3ull * n);
@@ -361,8 +375,9 @@ gpq_status gpq_astar_path(gpq_astar* a, uint32_t index, uint32_t* cells, uint32_
   d.inst = a->inst;
   d.gcost = a->gcost;
   d.blk = a->blk;
+  d.pred = a->pred;
   d.n_inst = a->n_inst;
-  astar_path_kernel<<<(a->n_inst * 32 + 255) / 256, 256, 0, st>>>(d, nullptr, a->n_inst, a->pout, index, a->path_buf,
+  astar_path_kernel<<<a->n_inst, kPathThreads, 0, st>>>(d, nullptr, a->n_inst, a->pout, index, a->path_buf,
                                                                    capacity);
   GPQ_CUDA_TRY(cudaGetLastError());
   unsigned long long po[3];

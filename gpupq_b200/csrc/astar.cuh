@@ -78,6 +78,7 @@ struct AstarDev {
   AstarTileDev* tiles;
   uint32_t* gcost;  // [cells]
   const uint32_t* blk;  // blocked bitmap, one bit per cell
+  uint8_t* pred;    // [cells + kAstarPredSlack] move to the canonical predecessor (astar_pred_kernel)
   uint2* inbox;     // [2][n_tiles][in_cap] (cell, g)
   uint2* open;      // [n_tiles][open_cap]
   uint32_t* al;     // [2][n_tiles] active tiles per round parity
@@ -90,6 +91,9 @@ struct AstarDev {
   uint32_t frontier_cap;  // per shared frontier buffer
   uint64_t spin_limit;
 };
+
+// Bytes after the last cell of the predecessor array: path windows read whole words.
+static constexpr uint64_t kAstarPredSlack = 256;
 
 __device__ __forceinline__ uint32_t ldcg_u32(const uint32_t* p) { return __ldcg(p); }
 
@@ -717,6 +721,60 @@ static __global__ void astar_done_list_kernel(const AstarInstDev* inst, const ui
     if (on[i] && inst[i].done) out[atomicAdd(out_n, 1u)] = i;
 }
 
+// Move tested l-th (l = 0..7) when looking for a predecessor, numbered as in
+// gpq_astar_dx/dy: the neighbours NW, N, NE, W, E, SW, S, SE, which is increasing cell id on
+// every grid where two of them exist together.
+__device__ __forceinline__ int astar_pred_order(int l) {
+  return l == 0 ? 7 : l == 1 ? 3 : l == 2 ? 6 : l == 3 ? 1 : l == 4 ? 0 : l == 5 ? 5 : l == 6 ? 2 : 4;
+}
+
+static constexpr uint8_t kAstarNoPred = 0xFF;
+
+// Instances of at least this many cells get predecessor moves from astar_pred_kernel and
+// walk their path over them (long walks, few such instances at a time).
+static constexpr uint64_t kAstarPredBytesCells = 1ull << 20;
+
+__device__ __forceinline__ bool astar_pred_bytes(const AstarInstDev& I) {
+  return (uint64_t)I.g.width * I.g.height >= kAstarPredBytesCells;
+}
+
+// The canonical predecessor of cell c (g = g[c], on an optimal path when g + h(c) <= C*):
+// the neighbour p with the smallest id that is free (both orthogonal cells free for a
+// diagonal), g[p] + c(p, c) == g and g[p] + h(p) <= C*.  Encoded as (dy + 1) << 2 | (dx + 1)
+// for the move from c to p; kAstarNoPred when there is none.  Lanes without a cell that
+// needs it pass cand = false; the blocked bits and g values of all eight neighbours are
+// loaded in one batch and the choice is made in registers, without divergent branches.
+__device__ __forceinline__ uint8_t astar_pred_move(const AstarDev& d, const AstarInstDev& I, const uint32_t* G,
+                                                   bool cand, uint32_t c, uint32_t g, uint32_t cs) {
+  const uint32_t w = I.g.width, h = I.g.height, conn = I.g.conn;
+  const int x = (int)(c % w), y = (int)(c / w);
+  bool fr[8];
+  uint32_t gp[8];
+#pragma unroll
+  for (int l = 0; l < 8; ++l) {
+    const int k = astar_pred_order(l);
+    const int nx = x + gpq_astar_dx(k), ny = y + gpq_astar_dy(k);
+    const bool in = cand && (conn == 8u || k < 4) && nx >= 0 && ny >= 0 && nx < (int)w && ny < (int)h;
+    const uint32_t p = (uint32_t)ny * w + (uint32_t)nx;
+    fr[l] = in && !astar_blocked(d, I, p);
+    gp[l] = in ? __ldg(&G[p]) : kAstarInf;
+  }
+  // diagonals (lanes 0 NW, 2 NE, 5 SW, 7 SE) also need their two orthogonal cells free
+  const bool diag = conn == 8u;
+  const bool ok[8] = {diag && fr[0] && fr[3] && fr[1], fr[1], diag && fr[2] && fr[1] && fr[4], fr[3],
+                      fr[4], diag && fr[5] && fr[3] && fr[6], fr[6], diag && fr[7] && fr[4] && fr[6]};
+  uint8_t best = kAstarNoPred;
+#pragma unroll
+  for (int l = 7; l >= 0; --l) {  // the smallest valid l is assigned last
+    const int k = astar_pred_order(l);
+    const int dx = gpq_astar_dx(k), dy = gpq_astar_dy(k);
+    if (ok[l] && gp[l] != kAstarInf && (uint64_t)gp[l] + gpq_astar_cost(conn, k) == g &&
+        (uint64_t)gp[l] + astar_hxy(conn, x + dx, y + dy, (int)I.gx, (int)I.gy) <= cs)
+      best = (uint8_t)((dy + 1) << 2 | (dx + 1));
+  }
+  return best;
+}
+
 // Per-instance expanded set (g + h <= C*, or every reached cell when the goal is not
 // reachable): count and hash.  Block per (instance, chunk): blockIdx.y = instance.
 static __global__ void astar_finalize_kernel(AstarDev d, const uint32_t* list, unsigned long long* out /* [n][2] */) {
@@ -743,61 +801,244 @@ static __global__ void astar_finalize_kernel(AstarDev d, const uint32_t* list, u
   }
 }
 
-// Canonical path of each instance, one warp per instance: from the goal, step to the
-// smallest-id neighbour p with g[p] + c(p, cell) == g[cell] and g[p] + h(p) <= C*.
-// out[3 * i] = length, out[3 * i + 1] = hash, out[3 * i + 2] = 1 when the walk failed.
-// When path != nullptr the cells of instance `want` are written (goal first, <= cap).
-static __global__ void astar_path_kernel(AstarDev d, const uint32_t* list, uint32_t n, unsigned long long* out,
-                                         uint32_t want, uint32_t* path, uint32_t cap) {
-  const uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+// Predecessor move of every expanded cell (g + h <= C*) of the instances in list[0, n)
+// that reached their goal and have at least kAstarPredBytesCells cells; the others
+// return at once.  Block per (instance, chunk): blockIdx.y = instance.  Whole warps step
+// together (blockDim is a multiple of 32), so a warp without expanded cells skips the
+// neighbour loads.
+static __global__ void astar_pred_kernel(AstarDev d, const uint32_t* list) {
+  const uint32_t i = list ? list[blockIdx.y] : blockIdx.y;
+  const AstarInstDev& I = d.inst[i];
+  const uint32_t cs = I.ub;
+  if (cs == kAstarInf || !astar_pred_bytes(I)) return;
+  const uint64_t cells = (uint64_t)I.g.width * I.g.height;
+  const uint32_t* G = d.gcost + I.cell0;
   const uint32_t lane = threadIdx.x & 31u;
+  for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x + (threadIdx.x - lane); base < cells;
+       base += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t c = base + lane;
+    const uint32_t g = c < cells ? G[c] : kAstarInf;
+    const bool exp = g != kAstarInf && (uint64_t)g + gpq_astar_h(I.g.conn, (uint32_t)c, I.g.goal, I.g.width) <= cs;
+    if (__any_sync(GPQ_FULL_MASK, exp)) {
+      const uint8_t mv = astar_pred_move(d, I, G, exp, (uint32_t)c, g, cs);
+      if (exp) d.pred[I.cell0 + c] = mv;
+    }
+  }
+}
+
+// ---- canonical path ----
+// From the goal, step to the neighbour p with g[p] + c(p, cell) == g[cell] and
+// g[p] + h(p) <= C* that has the smallest id, until the start.  The walk is serial, so
+// one CTA per instance keeps everything else off its critical path: all warps stage a
+// window of the grid in shared memory, one thread (or warp) walks inside it, and all
+// warps hash and store the cells it recorded.  Windows are placed around the current cell
+// with most of their room on the side of the start, where the path is heading.  Two forms:
+//  - instances of at least kAstarPredBytesCells cells (long walks, few of them at a time)
+//    use the predecessor moves that astar_pred_kernel wrote for every expanded cell:
+//    128 x 128 windows of move bytes, one shared-memory byte per step;
+//  - smaller instances (many at a time, where a pass over every expanded cell would
+//    cost more than it saves) stage 64 x 64 windows of g values and blocked
+//    bits, and warp 0 finds each step: lane l tests the l-th neighbour in increasing
+//    cell id, and the first lane whose test passes (one ballot) is the step.
+static constexpr uint32_t kPathThreads = 512;
+static constexpr uint32_t kPathWalkCap = 2048;
+static constexpr int kPathWinB = 128;                  // move-byte window side
+static constexpr int kPathRowWords = kPathWinB / 4 + 1;  // aligned words that cover 128 bytes
+static constexpr int kPathWinC = 64;                   // g-value window side
+static constexpr int kPathHalo = kPathWinC + 2;         // plus the cells its moves reach
+static constexpr int kPathStageBytes = kPathHalo * kPathHalo * 5 > kPathWinB * kPathRowWords * 4
+                                           ? kPathHalo * kPathHalo * 5
+                                           : kPathWinB * kPathRowWords * 4;
+
+// First column (row) of a window of side win around coordinate c on an axis of n cells,
+// with the start at coordinate s: 7/8 of the room towards the start.
+__device__ __forceinline__ int astar_path_origin(int c, int s, int n, int win) {
+  if (n <= win) return 0;
+  const int o = s < c ? c - (win - win / 8) : s > c ? c - (win / 8 - 1) : c - win / 2;
+  return min(max(o, 0), n - win);
+}
+
+struct AstarPathSmem {
+  uint32_t* walk;  // [kPathWalkCap] cells recorded in the current window
+  uint32_t* cur;   // next cell to record
+  uint32_t* nwalk;
+  uint32_t* done;  // 0 walking, 1 reached the start, 2 no predecessor
+};
+
+// One window of the move-byte form: stage, then thread 0 walks.  Ends with a barrier.
+__device__ __forceinline__ void astar_path_window_bytes(const AstarDev& d, const AstarInstDev& I, uint32_t* s_pw,
+                                                        const AstarPathSmem& sm) {
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+  const int w = (int)I.g.width, h = (int)I.g.height;
+  const uint32_t start = I.g.start, cur = *sm.cur;
+  const int cx = (int)(cur % (uint32_t)w), cy = (int)(cur / (uint32_t)w);
+  const int tx0 = astar_path_origin(cx, (int)(start % (uint32_t)w), w, kPathWinB);
+  const int ty0 = astar_path_origin(cy, (int)(start / (uint32_t)w), h, kPathWinB);
+  const uint32_t* PW = reinterpret_cast<const uint32_t*>(d.pred);
+  const int rows = min(kPathWinB, h - ty0);
+  for (int r = (int)warp; r < rows; r += (int)(kPathThreads / 32)) {  // row r: its bytes from (tx0, ty0 + r) on
+    const uint64_t w0 = (I.cell0 + (uint64_t)(ty0 + r) * (uint64_t)w + (uint64_t)tx0) >> 2;
+    const uint32_t a = __ldg(&PW[w0 + lane]);
+    const uint32_t b = lane == 0 ? __ldg(&PW[w0 + 32]) : 0u;
+    s_pw[r * kPathRowWords + (int)lane] = a;
+    if (lane == 0) s_pw[r * kPathRowWords + 32] = b;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    const uint8_t* s_pb = reinterpret_cast<const uint8_t*>(s_pw);
+    uint32_t c = cur, q = 0, done = 0;
+    uint32_t pc = (uint32_t)(I.cell0 + cur);  // its low two bits give each row's offset in its words
+    int lx = cx - tx0, ly = cy - ty0;
+    while (lx >= 0 && ly >= 0 && lx < kPathWinB && ly < kPathWinB && q < kPathWalkCap) {
+      sm.walk[q++] = c;
+      if (c == start) { done = 1; break; }
+      const uint32_t mv = s_pb[ly * (kPathRowWords * 4) + lx + (int)((pc - (uint32_t)lx) & 3u)];
+      if (mv == kAstarNoPred) { done = 2; break; }
+      const int dx = (int)(mv & 3u) - 1, dy = (int)(mv >> 2) - 1;
+      lx += dx;
+      ly += dy;
+      const uint32_t step = (uint32_t)(dy * w + dx);  // modulo 2^32: a step back is a wrapped add
+      c += step;
+      pc += step;
+    }
+    *sm.cur = c;
+    *sm.nwalk = q;
+    *sm.done = done;
+  }
+  __syncthreads();
+}
+
+// One window of the g-value form: stage g values and blocked bits (one grid row per warp
+// and pass), then warp 0 walks.  Ends with a barrier.
+__device__ __forceinline__ void astar_path_window_cells(const AstarDev& d, const AstarInstDev& I, uint32_t* s_g,
+                                                        uint8_t* s_b, const AstarPathSmem& sm) {
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+  const uint32_t* G = d.gcost + I.cell0;
+  const int w = (int)I.g.width, h = (int)I.g.height;
+  const uint32_t conn = I.g.conn, start = I.g.start, cs = I.ub, cur = *sm.cur;
+  const int cx = (int)(cur % (uint32_t)w), cy = (int)(cur / (uint32_t)w);
+  const int tx0 = astar_path_origin(cx, (int)(start % (uint32_t)w), w, kPathWinC);
+  const int ty0 = astar_path_origin(cy, (int)(start / (uint32_t)w), h, kPathWinC);
+  // the window and its halo, clipped to the grid (moves never leave the grid)
+  const int sx0 = max(tx0 - 1, 0), sx1 = min(tx0 + kPathWinC, w - 1);
+  const int sy0 = max(ty0 - 1, 0), sy1 = min(ty0 + kPathWinC, h - 1);
+  for (int y = sy0 + (int)warp; y <= sy1; y += (int)(kPathThreads / 32)) {
+    const uint32_t row = (uint32_t)y * (uint32_t)w;
+    const int hrow = (y - ty0 + 1) * kPathHalo - tx0 + 1;  // + x = halo index of (x, y)
+    uint32_t gv[3];
+    bool bv[3];
+#pragma unroll
+    for (int u = 0; u < 3; ++u) {  // 3 x 32 >= kPathHalo columns
+      const int x = sx0 + (int)lane + 32 * u;
+      if (x <= sx1) {
+        gv[u] = __ldg(&G[row + (uint32_t)x]);
+        bv[u] = astar_blocked(d, I, row + (uint32_t)x);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 3; ++u) {
+      const int x = sx0 + (int)lane + 32 * u;
+      if (x <= sx1) {
+        s_g[hrow + x] = gv[u];
+        s_b[hrow + x] = bv[u] ? 1 : 0;
+      }
+    }
+  }
+  __syncthreads();
+  if (warp == 0) {
+    // this lane's move, offset and cost (lanes 8..31 and the diagonals of 4-conn grids idle)
+    const int lk = astar_pred_order((int)(lane & 7u));
+    const bool lane_on = lane < 8u && (conn == 8u || lk < 4);
+    const int ldx = gpq_astar_dx(lk), ldy = gpq_astar_dy(lk);
+    const int loff = ldy * kPathHalo + ldx;
+    const uint32_t lcost = gpq_astar_cost(conn, lk);
+    uint32_t c = cur, q = 0, done = 0;
+    int x = cx, y = cy, lx = cx - tx0, ly = cy - ty0;
+    while (lx >= 0 && ly >= 0 && lx < kPathWinC && ly < kPathWinC && q < kPathWalkCap) {
+      if (lane == 0) sm.walk[q] = c;
+      ++q;
+      if (c == start) { done = 1; break; }
+      const int hi = (ly + 1) * kPathHalo + (lx + 1);
+      bool ok = false;
+      if (lane_on) {
+        const int nx = x + ldx, ny = y + ldy;
+        if (nx >= 0 && ny >= 0 && nx < w && ny < h && !s_b[hi + loff] &&
+            (ldx == 0 || ldy == 0 || (!s_b[hi + ldx] && !s_b[hi + ldy * kPathHalo]))) {
+          const uint32_t gp = s_g[hi + loff], gc = s_g[hi];
+          ok = gp != kAstarInf && (uint64_t)gp + lcost == gc &&
+               (uint64_t)gp + astar_hxy(conn, nx, ny, (int)I.gx, (int)I.gy) <= cs;
+        }
+      }
+      const uint32_t m = __ballot_sync(GPQ_FULL_MASK, ok);
+      if (m == 0u) { done = 2; break; }
+      const int k = astar_pred_order(__ffs(m) - 1);
+      const int dx = gpq_astar_dx(k), dy = gpq_astar_dy(k);
+      x += dx;
+      y += dy;
+      lx += dx;
+      ly += dy;
+      c += (uint32_t)(dy * w + dx);  // modulo 2^32: a step back is a wrapped add
+    }
+    if (lane == 0) {
+      *sm.cur = c;
+      *sm.nwalk = q;
+      *sm.done = done;
+    }
+  }
+  __syncthreads();
+}
+
+// Canonical path of the instances in list[0, n) (list == NULL: instances 0..n-1), one CTA
+// per instance.  out[3j..3j+2] = path length, path hash, failure flag; the path of
+// instance `want` is written to path[0, cap).
+static __global__ void __launch_bounds__(kPathThreads) astar_path_kernel(AstarDev d, const uint32_t* list, uint32_t n,
+                                                                         unsigned long long* out, uint32_t want,
+                                                                         uint32_t* path, uint32_t cap) {
+  __shared__ __align__(16) uint8_t s_stage[kPathStageBytes];
+  __shared__ uint32_t s_walk[kPathWalkCap];
+  __shared__ uint32_t s_cur, s_len, s_done, s_nwalk;
+  __shared__ unsigned long long s_hs;
+  const uint32_t j = blockIdx.x;
   if (j >= n) return;
   const uint32_t i = list ? list[j] : j;
   const AstarInstDev& I = d.inst[i];
-  const uint32_t cs = I.ub;
-  if (cs == kAstarInf) {
-    if (lane == 0) { out[3 * j] = 0; out[3 * j + 1] = 0; out[3 * j + 2] = 0; }
+  const uint32_t tid = threadIdx.x;
+  if (I.ub == kAstarInf) {
+    if (tid == 0) { out[3 * j] = 0; out[3 * j + 1] = 0; out[3 * j + 2] = 0; }
     return;
   }
-  const uint32_t* G = d.gcost + I.cell0;
-  const uint32_t w = I.g.width, h = I.g.height, conn = I.g.conn;
-  const uint64_t cells = (uint64_t)w * h;
-  uint32_t cur = I.g.goal;
-  unsigned long long hs = 0;
-  uint32_t len = 0, fail = 0;
-  for (uint64_t step = 0; step <= cells; ++step) {
-    if (lane == 0) {
-      hs += gpq_astar_path_hash(len, cur);
-      if (path && i == want && len < cap) path[len] = cur;
-    }
-    ++len;
-    if (cur == I.g.start) break;
-    const uint32_t gc = G[cur];
-    uint32_t cand = kAstarInf;
-    const int k = (int)lane;
-    if (k < (conn == 4 ? 4 : 8)) {
-      const int x = (int)(cur % w), y = (int)(cur / w);
-      const int nx = x + gpq_astar_dx(k), ny = y + gpq_astar_dy(k);
-      if (nx >= 0 && ny >= 0 && nx < (int)w && ny < (int)h) {
-        const uint32_t p = (uint32_t)ny * w + (uint32_t)nx;
-        bool ok = !astar_blocked(d, I, p);
-        if (ok && k >= 4)
-          ok = !astar_blocked(d, I, (uint32_t)y * w + (uint32_t)nx) && !astar_blocked(d, I, (uint32_t)ny * w + (uint32_t)x);
-        if (ok) {
-          const uint32_t gp = G[p];
-          if (gp != kAstarInf && (uint64_t)gp + gpq_astar_cost(conn, k) == gc &&
-              (uint64_t)gp + gpq_astar_h(conn, p, I.g.goal, w) <= cs)
-            cand = p;
-        }
-      }
-    }
-    cand = warp_min_u32(cand);
-    if (cand == kAstarInf) { fail = 1; break; }
-    cur = cand;
+  const bool bytes = astar_pred_bytes(I);
+  const AstarPathSmem sm{s_walk, &s_cur, &s_nwalk, &s_done};
+  const uint64_t cells = (uint64_t)I.g.width * I.g.height;
+  if (tid == 0) {
+    s_cur = I.g.goal;
+    s_len = 0;
+    s_done = 0;
+    s_hs = 0;
   }
-  if (lane == 0) {
-    out[3 * j] = len;
-    out[3 * j + 1] = hs;
-    out[3 * j + 2] = fail;
+  __syncthreads();
+  // every window records at least one cell: at most cells + 1 windows
+  for (uint64_t it = 0; it <= cells && s_done == 0u; ++it) {
+    if (bytes)
+      astar_path_window_bytes(d, I, reinterpret_cast<uint32_t*>(s_stage), sm);
+    else
+      astar_path_window_cells(d, I, reinterpret_cast<uint32_t*>(s_stage), s_stage + kPathHalo * kPathHalo * 4, sm);
+    const uint32_t nw = s_nwalk, len0 = s_len;
+    unsigned long long part = 0;
+    for (uint32_t q = tid; q < nw; q += kPathThreads) {
+      const uint32_t c = s_walk[q];
+      part += gpq_astar_path_hash(len0 + q, c);
+      if (path && i == want && len0 + q < cap) path[len0 + q] = c;
+    }
+    part = warp_sum_u64(part);
+    if ((tid & 31u) == 0 && part) atomicAdd(&s_hs, part);
+    __syncthreads();
+    if (tid == 0) s_len = len0 + nw;  // read again only after the next window's barriers
+  }
+  __syncthreads();
+  if (tid == 0) {
+    out[3 * j] = s_len;
+    out[3 * j + 1] = s_hs;
+    out[3 * j + 2] = s_done == 1u ? 0u : 1u;
   }
 }

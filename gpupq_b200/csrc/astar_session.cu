@@ -21,6 +21,7 @@ struct gpq_astar_session {
   uint32_t max_tiles = 0, max_inst = 0;
   // device state
   uint32_t* gcost = nullptr;
+  uint8_t* pred = nullptr;  // [max_cells + kAstarPredSlack]
   uint32_t* blk = nullptr;
   AstarInstDev* inst = nullptr;
   AstarTileDev* tiles = nullptr;
@@ -89,6 +90,7 @@ AstarDev session_dev(const gpq_astar_session* s) {
   d.tiles = s->tiles;
   d.gcost = s->gcost;
   d.blk = s->blk;
+  d.pred = s->pred;
   d.inbox = s->inbox;
   d.open = s->open;
   d.al = s->al;
@@ -161,6 +163,7 @@ gpq_status gpq_astar_session_create(const gpq_astar_config* cfg, uint64_t max_ce
   cudaError_t e = cudaStreamCreateWithFlags(&s->own, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = dmalloc(&s->gcost, s->max_cells);
   if (e == cudaSuccess) e = dmalloc(&s->blk, s->max_cells / 32 + 1);
+  if (e == cudaSuccess) e = dmalloc(&s->pred, s->max_cells + kAstarPredSlack);
   if (e == cudaSuccess) e = dmalloc(&s->inst, max_instances);
   if (e == cudaSuccess) e = dmalloc(&s->tiles, max_tiles);
   if (e == cudaSuccess) e = dmalloc(&s->inbox, 2ull * max_tiles * c.inbox_capacity);
@@ -204,7 +207,7 @@ gpq_status gpq_astar_session_create(const gpq_astar_config* cfg, uint64_t max_ce
 
 gpq_status gpq_astar_session_destroy(gpq_astar_session* s) {
   if (!s) return GPQ_OK;
-  void* bufs[] = {s->gcost, s->blk,    s->inst,   s->tiles, s->inbox, s->open, s->al,  s->ctl,
+  void* bufs[] = {s->gcost, s->pred, s->blk,    s->inst,   s->tiles, s->inbox, s->open, s->al,  s->ctl,
                   s->on,    s->list,   s->list_n, s->staged, s->fin,  s->pout};
   for (void* p : bufs)
     if (p) cudaFree(p);
@@ -300,10 +303,12 @@ gpq_status gpq_astar_session_collect(gpq_astar_session* s, uint32_t* slots, gpq_
     if (s->h_on[i]) max_cells = std::max<uint64_t>(max_cells, (uint64_t)s->h_grid[i].width * s->h_grid[i].height);
   for (uint32_t j0 = 0; j0 < n; j0 += 65535) {
     const uint32_t nj = std::min<uint32_t>(65535, n - j0);
-    const uint32_t fx = (uint32_t)std::min<uint64_t>((max_cells + 255) / 256, 64);
+    // a few blocks per resident search CTA over all instances, at least 64 per instance
+    const uint32_t fx = (uint32_t)std::min<uint64_t>((max_cells + 255) / 256, std::max<uint64_t>(64, 4ull * s->grid / nj));
     astar_finalize_kernel<<<dim3(fx, nj), 256, 0, st>>>(d, s->list + j0, s->fin + 2ull * j0);
+    if (max_cells >= kAstarPredBytesCells) astar_pred_kernel<<<dim3(fx, nj), 256, 0, st>>>(d, s->list + j0);
   }
-  astar_path_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>(d, s->list, n, s->pout, 0xFFFFFFFFu, nullptr, 0);
+  astar_path_kernel<<<n, kPathThreads, 0, st>>>(d, s->list, n, s->pout, 0xFFFFFFFFu, nullptr, 0);
   astar_gather_kernel<<<(n + 127) / 128, 128, 0, st>>>(s->inst, s->list, n, s->staged, s->on);
   GPQ_CUDA_TRY(cudaGetLastError());
   std::vector<unsigned long long> fin(2ull * n), pout(3ull * n);
@@ -355,7 +360,7 @@ uint64_t gpq_astar_session_bytes(const gpq_astar_config* cfg, uint64_t max_cells
   const uint32_t tile = c.tile ? c.tile : 64;
   const uint64_t in_cap = c.inbox_capacity ? c.inbox_capacity : 8ull * tile;
   const uint64_t open_cap = c.open_capacity ? c.open_capacity : (uint64_t)tile * tile;
-  return max_cells * 4 + max_cells / 8 + (uint64_t)max_tiles * (sizeof(AstarTileDev) + 8 * (2 * in_cap + open_cap) + 8) +
+  return max_cells * 5 + kAstarPredSlack + max_cells / 8 + (uint64_t)max_tiles * (sizeof(AstarTileDev) + 8 * (2 * in_cap + open_cap) + 8) +
          (uint64_t)max_instances * (2 * sizeof(AstarInstDev) + 41);
 }
 

@@ -44,7 +44,7 @@ struct Sessions {
 
 gpq_status serve_batched(const gpq_serve_config& c, const gpq_serve_request* reqs, uint32_t n,
                          gpq_serve_response* out, gpq_serve_stats* stats) {
-  // split the budget: A* cells (4.125 B each) and tiles, PHOLD LPs
+  // split the budget: A* cells (5.125 B each: g, predecessor move, blocked bit) and tiles, PHOLD LPs
   const uint64_t budget = c.hbm_budget;
   const double share = c.astar_share > 0.0 ? c.astar_share : 0.75;
   gpq_astar_config ac = c.astar;
@@ -54,7 +54,7 @@ gpq_status serve_batched(const gpq_serve_config& c, const gpq_serve_request* req
   const uint64_t tile_bytes = 64 + 8 * (2 * in_cap + open_cap) + 8;
   const uint64_t a_bytes = (uint64_t)(budget * share);
   // a tile for every tile*tile cells, plus room for ragged edges
-  const double per_cell = 4.125 + (double)tile_bytes / ((double)tile * tile) * 1.25;
+  const double per_cell = 5.125 + (double)tile_bytes / ((double)tile * tile) * 1.25;
   const uint64_t max_cells = std::max<uint64_t>((uint64_t)(a_bytes / per_cell), 1u << 20);
   const uint32_t max_tiles = (uint32_t)std::min<uint64_t>(max_cells / ((uint64_t)tile * tile) * 5 / 4 + 1024, 1u << 30);
   const uint32_t max_inst = 65536;

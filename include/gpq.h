@@ -274,7 +274,8 @@ typedef struct gpq_astar_config {
   uint32_t open_capacity;     /* items one tile keeps above the window; 0 = tile * tile */
   uint32_t frontier_capacity; /* shared-memory frontier items (two buffers); 0 = 2048 (256 per warp) */
   uint32_t block_threads;     /* 64, 128 or 256; 0 = 256 */
-  uint32_t ctas_per_sm;       /* 0 = as many as fit */
+  uint32_t ctas_per_sm;       /* 0 = one per SM for every SM's worth of tiles expected active at a
+                                 once (sqrt(tiles) per instance), at most as many as fit */
   uint32_t max_rounds;        /* 0 = 2^20; reaching it is GPQ_ERR_TIMEOUT */
   uint32_t tile_worker;       /* who processes one tile visit: 0 = a CTA, 1 = a warp */
   uint32_t reserved[3];
@@ -328,7 +329,7 @@ GPQ_API gpq_status gpq_astar_write_ppm(gpq_astar* a, uint32_t index, const char*
 
 /* Resident A* instances for serving.  No counterpart in the reference, whose agents run
  * to completion inside one a_star launch (src/a_star.cu:269-593).  A session reserves a
- * cell space (max_cells: g values and blocked bits, 4.125 bytes a cell) and a tile space
+ * cell space (max_cells: g values, predecessor moves and blocked bits, 5.125 bytes a cell) and a tile space
  * (max_tiles tile records with their inboxes and open arrays) once; admitted instances
  * take free ranges of both, all running instances advance together, a bounded number of
  * rounds per step (one persistent launch), and finished ones are collected and give

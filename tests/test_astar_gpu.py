@@ -151,6 +151,42 @@ def test_session_stream_matches_oracle(gpu_lib, rounds):
             assert int(r[k]) == want[i][k], (i, k)
 
 
+def _path_form_grids():
+    # 1101 x 1000 and 1024 x 1024 have at least 2^20 cells (paths over predecessor moves),
+    # 1023 x 1023 and 300 x 200 fewer (paths over staged g values); the odd widths start
+    # rows at every byte offset of a word; the first start lies north-east of its goal
+    return np.concatenate([G.astar_grid(1101, 1000, 0.2, 21, conn=8, start=1100, goal=1101 * 999),
+                           G.astar_grid(1024, 1024, 0.25, 22, conn=4, start=0, goal=1024 * 1024 - 1),
+                           G.astar_grid(1023, 1023, 0.2, 23, conn=8, start=5, goal=1023 * 1023 - 7),
+                           G.astar_grid(300, 200, 0.2, 24, conn=4, start=17, goal=300 * 200 - 40)])
+
+
+def test_path_forms(gpu_lib):
+    """Both path forms in one launch, plain and in a session: results and paths exact."""
+    grids = _path_form_grids()
+    want = [O.astar({k: int(g[k]) for k in O.ASTAR_FIELDS}, want_path=True) for g in grids]
+    with G.AStar(tile=64) as a:
+        res = a.solve(grids)
+        _check(res, grids)
+        for i in range(len(grids)):
+            assert np.array_equal(a.path(i), want[i]["path"]), i
+    got = {}
+    with G.AStarSession(max_cells=4 << 20, max_tiles=1024, max_instances=4, tile=64) as s:
+        slot_of = {s.admit(g): i for i, g in enumerate(grids)}
+        assert None not in slot_of
+        for _ in range(100000):
+            s.step(5)
+            slots, res = s.collect()
+            for sl, r in zip(slots, res):
+                got[slot_of[int(sl)]] = r
+            if len(got) == len(grids):
+                break
+    for i, r in got.items():
+        assert r["status"] == 0
+        for k in FIELDS:
+            assert int(r[k]) == want[i][k], (i, k)
+
+
 def _read_ppm(path):
     data = open(path, "rb").read()
     parts = data.split(b"\n", 3)
