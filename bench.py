@@ -184,11 +184,21 @@ def _timed(fn, warmup, steps):
     return out, time.perf_counter() - t0
 
 
+def _astar_shape(grids, args, default, space=None):
+    """The A* configuration for a bench batch: the tuner's (shipped or cached, timed when
+    neither has the workload class) unless --no-tune."""
+    if args.no_tune:
+        return dict(default)
+    from gpupq_b200 import autotune
+    return autotune.tune_astar(grids, space=space, force=args.retune)
+
+
 def bench_astar_plain(G, O, args, peak):
     """One 2048 x 2048 grid (Bernoulli(0.2), seed 3, corner to corner, 4-connected, 1024
     shards of 64 x 64): expansions (cells with f <= C*) per second of device time."""
     g = G.astar_grid(2048, 2048, 0.2, 3)
-    with G.AStar(tile=64) as a:  # 1024 shards, as the workload names
+    shape = _astar_shape(g, args, dict(tile=64), space={"tile": [64]})  # 1024 shards, as the workload names
+    with G.AStar(**shape) as a:
         def step():
             r = a.solve(g)
             return r[0], a.stats()
@@ -200,7 +210,7 @@ def bench_astar_plain(G, O, args, peak):
     achieved = exp * ASTAR_BYTES_PER_EXPANSION[4] * args.steps / dev_s / 1e9
     return {"workload": "astar_plain_2048x2048_p0.2_4conn_1024shards", "metric": "A* expansions/s",
             "value": exp * args.steps / dev_s, "unit": "expansions/s", "cost": int(out[0][0]["cost"]),
-            "expanded": exp, "ms_per_query": 1e3 * dev_s / args.steps, "exact_vs_oracle": exact,
+            "expanded": exp, "ms_per_query": 1e3 * dev_s / args.steps, "exact_vs_oracle": exact, "config": shape,
             "e2e": {"value": exp * args.steps / wall, "unit": "expansions/s", "h2d_bytes_per_step": 32,
                     "d2h_bytes_per_step": 48},
             "roofline": {"bound": "latency (critical path of ~4100 dependent expansions)", "achieved": achieved,
@@ -213,7 +223,8 @@ def bench_astar_batched(G, O, args, peak):
     """10,000 queries in one persistent launch: side log-uniform in [64, 1024], density
     uniform in [0.1, 0.3], 8-connected 10/14, octile, seeds 11 + i."""
     q = G.astar_queries(11, 10000, 8, 64, 1024, 0.1, 0.3)
-    with G.AStar(tile=64, window=100) as a:
+    shape = _astar_shape(q, args, dict(tile=64, window=100))
+    with G.AStar(**shape) as a:
         def step():
             r = a.solve(q)
             return r, a.stats()
@@ -235,6 +246,7 @@ def bench_astar_batched(G, O, args, peak):
     return {"workload": "astar_batched_10000q_side64-1024_8conn", "metric": "A* expansions/s (batched)",
             "value": exp * args.steps / dev_s, "unit": "expansions/s", "queries": len(q),
             "ms_per_batch": 1e3 * dev_s / args.steps, "bad_status": int((out[0][0]["status"] != 0).sum()),
+            "config": shape,
             "plain_value": pe / pt, "plain_sample": "first 200 queries, one launch each",
             "batched_over_plain": (exp * args.steps / dev_s) / (pe / pt), "exact_vs_oracle_first_300": exact,
             "e2e": {"value": exp * args.steps / wall, "unit": "expansions/s",

@@ -187,6 +187,17 @@ def test_path_forms(gpu_lib):
             assert int(r[k]) == want[i][k], (i, k)
 
 
+def test_autotune_astar(gpu_lib, tmp_path):
+    """The A* tuner times its candidates on the batch and returns one whose results are exact."""
+    from gpupq_b200 import autotune
+    grids = G.astar_queries(5, 30, 8, 64, 300, 0.1, 0.3)
+    best = autotune.tune_astar(grids, space={"tile": [32, 64], "window": [4, 10], "ctas_per_sm": [0, 1]},
+                               cache=str(tmp_path / "tune.json"))
+    assert set(best) == {"tile", "window", "ctas_per_sm"} and best["window"] in (40, 100)
+    with G.AStar(**best) as a:
+        _check(a.solve(grids), grids)
+
+
 def _read_ppm(path):
     data = open(path, "rb").read()
     parts = data.split(b"\n", 3)
