@@ -154,6 +154,8 @@ _SIGS = {
     "gpq_phold_session_step": ([_VP, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32), _VP], ctypes.c_int),
     "gpq_phold_session_collect": ([_VP, _VP, ctypes.POINTER(PholdResult), ctypes.c_uint32,
                                    ctypes.POINTER(ctypes.c_uint32), _VP], ctypes.c_int),
+    "gpq_phold_session_snapshot": ([_VP, _VP, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64), _VP], ctypes.c_int),
+    "gpq_phold_session_restore": ([_VP, _VP, ctypes.c_uint64, _VP], ctypes.c_int),
     "gpq_phold_session_usage": ([_VP, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint32)],
                                 ctypes.c_int),
     "gpq_phold_session_bytes": ([ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32],
@@ -647,6 +649,19 @@ class PholdSession:
         a, b = ctypes.c_uint64(), ctypes.c_uint32()
         check(lib().gpq_phold_session_usage(self._h, ctypes.byref(a), ctypes.byref(b)), "gpq_phold_session_usage")
         return a.value, b.value
+
+    def snapshot(self):
+        """The whole session's state between steps (gpq_phold_session_snapshot) as a uint8 array."""
+        n = ctypes.c_uint64()
+        check(lib().gpq_phold_session_snapshot(self._h, None, 0, ctypes.byref(n), None), "gpq_phold_session_snapshot")
+        buf = np.zeros(n.value, np.uint8)
+        check(lib().gpq_phold_session_snapshot(self._h, _ptr(buf), n.value, ctypes.byref(n), None),
+              "gpq_phold_session_snapshot")
+        return buf
+
+    def restore(self, buf):
+        buf = np.ascontiguousarray(buf, dtype=np.uint8)
+        check(lib().gpq_phold_session_restore(self._h, _ptr(buf), len(buf), None), "gpq_phold_session_restore")
 
 
 # ---- serving (gpq_serve_* in include/gpq.h) ----

@@ -193,9 +193,201 @@ gpq_status flush_pending(gpq_phold_session* s, cudaStream_t st) {
   return GPQ_OK;
 }
 
+constexpr uint64_t kSessionSnapMagic = 0x3153534553515047ull;  // "GPQSESS1"
+constexpr uint32_t kSessionSnapHeader = 12;
+
+// Device regions of a session's state for slots [0, high) and LPs [0, lp_high): the
+// scratch buffers (list, acc, staged) are not state.  Parity-major arrays give one
+// region per parity.
+std::vector<std::pair<void*, size_t>> session_regions(const gpq_phold_session* s, uint64_t H, uint64_t L) {
+  std::vector<std::pair<void*, size_t>> r;
+  const uint64_t M = s->max_lps;
+  auto add = [&](void* p, uint64_t n) { r.push_back({p, (size_t)n}); };
+  add(s->inst, H * sizeof(PmInstDev));
+  add(s->mins, 3 * H * sizeof(uint32_t));
+  add(s->errs, 3 * H * sizeof(uint32_t));
+  add(s->on, H);
+  add(s->lp_inst, L * sizeof(uint32_t));
+  add(s->count, L * sizeof(uint32_t));
+  add(s->csum, L * sizeof(unsigned long long));
+  add(s->ohash, L * sizeof(unsigned long long));
+  add(s->ctl, sizeof(PmCtl));
+  if (s->bucketed) {
+    const LabDev& q = s->b.q;
+    add(q.keys, (L << (q.nb_log2 + q.c_log2)) * sizeof(unsigned long long));
+    add(q.cnt, (L << q.nb_log2) * sizeof(uint32_t));
+    for (uint64_t par = 0; par < 2; ++par) {
+      add(q.spill + par * M * q.F, L * q.F * sizeof(unsigned long long));
+      add(q.scnt + par * M, L * sizeof(uint32_t));
+    }
+    add(s->b.wj, 4 * H * sizeof(uint32_t));
+    add(s->b.fin, H * sizeof(uint32_t));
+  } else {
+    add(s->ring, (L << s->cap_log2) * sizeof(gpq_item));
+    add(s->rd, L * sizeof(uint32_t));
+    add(s->wr, L * sizeof(uint32_t));
+    for (uint64_t par = 0; par < 2; ++par) {
+      add(s->ibuf + par * M * s->ibc, L * s->ibc * sizeof(gpq_item));
+      add(s->icnt + par * M, L * sizeof(uint32_t));
+    }
+  }
+  return r;
+}
+
+void session_header(const gpq_phold_session* s, uint32_t h[kSessionSnapHeader]) {
+  const uint32_t v[kSessionSnapHeader] = {s->bucketed ? 1u : 0u, s->max_lps, s->max_inst, s->cap_log2, s->ibc,
+                                          s->group, s->block, s->b.q.nb_log2, s->b.q.c_log2, s->b.q.F,
+                                          (uint32_t)sizeof(PmInstDev), 1u};
+  std::memcpy(h, v, sizeof(v));
+}
+
+// Host state: counters, slot tables, free slots, the LP-range allocator.
+std::vector<unsigned char> session_host_blob(const gpq_phold_session* s) {
+  std::vector<unsigned char> b;
+  auto put = [&](const void* p, size_t n) {
+    const unsigned char* c = static_cast<const unsigned char*>(p);
+    b.insert(b.end(), c, c + n);
+  };
+  const uint32_t k[5] = {s->high, s->lp_high, s->active, s->next_window, s->max_per_lp};
+  put(k, sizeof(k));
+  put(s->h_on.data(), s->h_on.size());
+  put(s->h_inst.data(), s->h_inst.size() * sizeof(PmInstDev));
+  const uint64_t nf = s->free_slots.size();
+  put(&nf, 8);
+  put(s->free_slots.data(), nf * sizeof(uint32_t));
+  const auto ranges = s->lps.free_ranges();
+  const uint64_t a[3] = {s->lps.size(), s->lps.used(), ranges.size()};
+  put(a, sizeof(a));
+  for (const auto& r : ranges) {
+    const uint64_t pr[2] = {r.first, r.second};
+    put(pr, sizeof(pr));
+  }
+  return b;
+}
+
 }  // namespace
 
 extern "C" {
+
+gpq_status gpq_phold_session_snapshot(gpq_phold_session* s, void* buf, uint64_t capacity, uint64_t* size,
+                                      void* stream) {
+  GPQ_CHECK_ARG(s && size, "NULL argument");
+  const cudaStream_t st = gpq::as_stream(stream, s->own);
+  if (buf) {
+    const gpq_status r = flush_pending(s, st);
+    if (r != GPQ_OK) return r;
+  }
+  const std::vector<unsigned char> blob = session_host_blob(s);
+  const auto regions = session_regions(s, s->high, s->lp_high);
+  uint64_t need = 8 + 4 * kSessionSnapHeader + 8 + blob.size() + 4;
+  for (const auto& r : regions) need += 8 + r.second;
+  *size = need;
+  if (!buf) return GPQ_OK;
+  GPQ_CHECK_ARG(capacity >= need, "capacity below the snapshot size");
+  unsigned char* p = static_cast<unsigned char*>(buf);
+  auto put = [&](const void* src, size_t n) {
+    std::memcpy(p, src, n);
+    p += n;
+  };
+  uint32_t hdr[kSessionSnapHeader];
+  session_header(s, hdr);
+  put(&kSessionSnapMagic, 8);
+  put(hdr, sizeof(hdr));
+  const uint64_t nb = blob.size();
+  put(&nb, 8);
+  put(blob.data(), nb);
+  const uint32_t nr = (uint32_t)regions.size();
+  put(&nr, 4);
+  GPQ_CUDA_TRY(cudaStreamSynchronize(st));
+  for (const auto& r : regions) {
+    const uint64_t n = r.second;
+    put(&n, 8);
+    if (n) GPQ_CUDA_TRY(cudaMemcpyAsync(p, r.first, n, cudaMemcpyDeviceToHost, st));
+    p += n;
+  }
+  GPQ_CUDA_TRY(cudaStreamSynchronize(st));
+  return GPQ_OK;
+}
+
+gpq_status gpq_phold_session_restore(gpq_phold_session* s, const void* buf, uint64_t size, void* stream) {
+  GPQ_CHECK_ARG(s && buf, "NULL argument");
+  const unsigned char* p = static_cast<const unsigned char*>(buf);
+  const unsigned char* end = p + size;
+  auto take = [&](void* dst, size_t n) -> bool {
+    if ((uint64_t)(end - p) < n) return false;
+    if (dst) std::memcpy(dst, p, n);
+    p += n;
+    return true;
+  };
+  uint64_t magic = 0;
+  uint32_t hdr[kSessionSnapHeader], mine[kSessionSnapHeader];
+  session_header(s, mine);
+  GPQ_CHECK_ARG(take(&magic, 8) && magic == kSessionSnapMagic, "not a PHOLD session snapshot");
+  GPQ_CHECK_ARG(take(hdr, sizeof(hdr)) && std::memcmp(hdr, mine, sizeof(hdr)) == 0,
+                "snapshot of a session with other parameters");
+  // host state into temporaries; nothing changes until every part has been checked
+  uint64_t nb = 0;
+  GPQ_CHECK_ARG(take(&nb, 8) && (uint64_t)(end - p) >= nb, "snapshot truncated");
+  const unsigned char* hb = p;
+  p += nb;
+  const unsigned char* hend = hb + nb;
+  auto htake = [&](void* dst, size_t n) -> bool {
+    if ((uint64_t)(hend - hb) < n) return false;
+    std::memcpy(dst, hb, n);
+    hb += n;
+    return true;
+  };
+  uint32_t k[5];
+  std::vector<uint8_t> h_on(s->max_inst);
+  std::vector<PmInstDev> h_inst(s->max_inst);
+  uint64_t nf = 0, a[3] = {0, 0, 0};
+  bool ok = htake(k, sizeof(k)) && htake(h_on.data(), h_on.size()) &&
+            htake(h_inst.data(), h_inst.size() * sizeof(PmInstDev)) && htake(&nf, 8) && nf <= s->max_inst;
+  std::vector<uint32_t> free_slots(ok ? nf : 0);
+  ok = ok && htake(free_slots.data(), nf * sizeof(uint32_t)) && htake(a, sizeof(a)) && a[0] == s->max_lps &&
+       a[2] <= s->max_lps;
+  std::vector<std::pair<uint64_t, uint64_t>> ranges(ok ? a[2] : 0);
+  for (auto& r : ranges) {
+    uint64_t pr[2];
+    ok = ok && htake(pr, sizeof(pr)) && pr[0] + pr[1] <= s->max_lps;
+    r = {pr[0], pr[1]};
+  }
+  GPQ_CHECK_ARG(ok && hb == hend && k[0] <= s->max_inst && k[1] <= s->max_lps, "snapshot host state is damaged");
+  const auto regions = session_regions(s, k[0], k[1]);
+  uint32_t nr = 0;
+  GPQ_CHECK_ARG(take(&nr, 4) && nr == regions.size(), "snapshot layout differs");
+  const unsigned char* scan = p;
+  for (const auto& r : regions) {
+    uint64_t n = 0;
+    GPQ_CHECK_ARG((uint64_t)(end - scan) >= 8, "snapshot truncated");
+    std::memcpy(&n, scan, 8);
+    GPQ_CHECK_ARG(n == r.second && (uint64_t)(end - scan - 8) >= n, "snapshot region differs or is truncated");
+    scan += 8 + n;
+  }
+  const cudaStream_t st = gpq::as_stream(stream, s->own);
+  GPQ_CUDA_TRY(cudaStreamSynchronize(st));
+  for (const auto& r : regions) {
+    p += 8;
+    if (r.second) GPQ_CUDA_TRY(cudaMemcpyAsync(r.first, p, r.second, cudaMemcpyHostToDevice, st));
+    p += r.second;
+  }
+  // slots and LPs above the snapshot's highest ones are free
+  if (k[0] < s->max_inst) GPQ_CUDA_TRY(cudaMemsetAsync(s->on + k[0], 0, s->max_inst - k[0], st));
+  if (k[1] < s->max_lps)
+    GPQ_CUDA_TRY(cudaMemsetAsync(s->lp_inst + k[1], 0xff, (size_t)(s->max_lps - k[1]) * sizeof(uint32_t), st));
+  GPQ_CUDA_TRY(cudaStreamSynchronize(st));
+  s->high = k[0];
+  s->lp_high = k[1];
+  s->active = k[2];
+  s->next_window = k[3];
+  s->max_per_lp = k[4];
+  s->h_on.swap(h_on);
+  s->h_inst.swap(h_inst);
+  s->free_slots.swap(free_slots);
+  s->lps.assign(a[0], a[1], ranges);
+  s->pending.clear();
+  return GPQ_OK;
+}
 
 gpq_status gpq_phold_session_create(uint32_t max_lps, uint32_t capacity, uint32_t insert_capacity,
                                     uint32_t max_instances, uint32_t lanes_per_lp, gpq_phold_session** out) {

@@ -6,6 +6,8 @@
 #include <cstdint>
 #include <iterator>
 #include <map>
+#include <utility>
+#include <vector>
 
 namespace gpq {
 
@@ -51,6 +53,14 @@ class RangeAlloc {
   }
   uint64_t used() const { return used_; }
   uint64_t size() const { return size_; }
+  // The free ranges (start, length) in order, and the allocator set back to exactly them.
+  std::vector<std::pair<uint64_t, uint64_t>> free_ranges() const { return {free_.begin(), free_.end()}; }
+  void assign(uint64_t size, uint64_t used, const std::vector<std::pair<uint64_t, uint64_t>>& ranges) {
+    free_.clear();
+    for (const auto& r : ranges) free_[r.first] = r.second;
+    size_ = size;
+    used_ = used;
+  }
 
  private:
   std::map<uint64_t, uint64_t> free_;  // start -> length

@@ -405,6 +405,17 @@ GPQ_API gpq_status gpq_phold_session_step(gpq_phold_session* s, uint32_t windows
 GPQ_API gpq_status gpq_phold_session_collect(gpq_phold_session* s, uint32_t* slots, gpq_phold_result* results,
                                              uint32_t capacity, uint32_t* n, void* stream);
 GPQ_API gpq_status gpq_phold_session_usage(gpq_phold_session* s, uint64_t* lps_used, uint32_t* instances);
+/* Whole-session state between steps: every resident run (queues, per-LP checksums, window
+ * counters, slots, the LP-range allocator), so a serving process can stop and resume, or
+ * branch several continuations from one point.  Admissions not yet started are started
+ * first, at the session's next window, as the next step would start them.  Per-LP arrays
+ * are saved up to the highest LP in use.  A snapshot restores into a session created with
+ * the same parameters, whatever that session holds; it then steps and collects exactly as
+ * the original would have.  With buf == NULL the snapshot only reports its size.  Both
+ * block on the stream. */
+GPQ_API gpq_status gpq_phold_session_snapshot(gpq_phold_session* s, void* buf, uint64_t capacity, uint64_t* size,
+                                              void* stream);
+GPQ_API gpq_status gpq_phold_session_restore(gpq_phold_session* s, const void* buf, uint64_t size, void* stream);
 GPQ_API uint64_t gpq_phold_session_bytes(uint32_t max_lps, uint32_t capacity, uint32_t insert_capacity,
                                          uint32_t max_instances);
 GPQ_API uint64_t gpq_phold_session_bytes_bucketed(uint32_t max_lps, uint32_t buckets, uint32_t bucket_slots,

@@ -84,3 +84,77 @@ def test_stream_equals_alone(gpu_lib, windows, bucketed):
     assert refused > 0 and len(got) == len(runs)
     for i in range(len(runs)):
         _same(got[i], want[i])
+
+
+def _drive(s, runs, slot_of, pending, windows, got):
+    """Admit, step and collect until every run has finished; returns the results by run."""
+    for _ in range(100000):
+        while pending:
+            sl = s.admit(runs[pending[0]])
+            if sl is None:
+                break
+            slot_of[sl] = pending.pop(0)
+        s.step(windows)
+        for sl, r in s.collect():
+            got[slot_of.pop(sl)] = _d(r)
+        if not pending and not slot_of:
+            return got
+    raise AssertionError("runs did not finish")
+
+
+@pytest.mark.parametrize("bucketed", [False, True])
+def test_session_snapshot_resumes_exactly(gpu_lib, bucketed):
+    """Snapshot a session mid-stream (some runs mid-run, one admitted but not started,
+    LP ranges reused), finish it; restore the snapshot into a fresh session and into one
+    that already holds other runs, finish those: every run ends the same three times and
+    as it ends alone."""
+    runs = _runs(3, 14)
+    kw = dict(max_lps=4000, max_instances=8, bucketed=bucketed)
+    with G.PholdSession(**kw) as s:
+        slot_of, pending, got = {}, list(range(len(runs))), {}
+        for _ in range(3):  # a few steps, with collections that free slots and LPs
+            while pending:
+                sl = s.admit(runs[pending[0]])
+                if sl is None:
+                    break
+                slot_of[sl] = pending.pop(0)
+            s.step(4)
+            for sl, r in s.collect():
+                got[slot_of.pop(sl)] = _d(r)
+        if pending:  # one run admitted but not started when the snapshot is taken
+            sl = s.admit(runs[pending[0]])
+            if sl is not None:
+                slot_of[sl] = pending.pop(0)
+        snap = s.snapshot()
+        state = (dict(slot_of), list(pending), dict(got))
+        first = _drive(s, runs, slot_of, pending, 4, got)
+    for target_busy in (False, True):
+        with G.PholdSession(**kw) as t:
+            if target_busy:
+                for c in _runs(9, 3):
+                    t.admit(c)
+                t.step(2)
+            t.restore(snap)
+            slot_of, pending, got = dict(state[0]), list(state[1]), dict(state[2])
+            again = _drive(t, runs, slot_of, pending, 4, got)
+            assert t.usage() == (0, 0)
+        assert sorted(again) == sorted(first) == list(range(len(runs)))
+        for i in range(len(runs)):
+            _same(again[i], first[i])
+    for i, c in enumerate(runs):
+        _same(first[i], _alone(c))
+
+
+def test_session_snapshot_rejects_other_parameters(gpu_lib):
+    with G.PholdSession(max_lps=1000, max_instances=4) as s:
+        s.admit(_runs(4, 1)[0])
+        snap = s.snapshot()
+    with G.PholdSession(max_lps=2000, max_instances=4) as t:
+        with pytest.raises(G.GpqError):
+            t.restore(snap)
+    with G.PholdSession(max_lps=1000, max_instances=4, bucketed=True) as t:
+        with pytest.raises(G.GpqError):
+            t.restore(snap)
+    with G.PholdSession(max_lps=1000, max_instances=4) as t:
+        with pytest.raises(G.GpqError):
+            t.restore(snap[:-5])
