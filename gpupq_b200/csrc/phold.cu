@@ -62,6 +62,14 @@ struct gpq_phold {
   uint32_t cap_log2 = 0;
   uint32_t block = kDefaultBlock;
   uint32_t phase = 0;  // next window (host view; plain loop)
+  // sharded runs (gpq_phold_shard_create): LPs [lp_begin, lp_end) of num_lps, outbox per
+  // destination shard
+  bool sharded = false;
+  uint32_t rank = 0, world = 1, lp_begin = 0, lp_end = 0, shard_lps = 0, out_cap = 0;
+  gpq_item* outbox = nullptr;   // [world][out_cap]
+  uint32_t* out_n = nullptr;    // [world]
+  gpq_item* inject_buf = nullptr;
+  uint64_t inject_cap = 0;
   uint32_t last_grid = 0;  // CTAs of the last persistent launch
   bool populated = false;
   bool finalized = false;
@@ -82,6 +90,12 @@ struct gpq_phold {
     d.ohash = ohash;
     d.ctrl = ctrl;
     d.spin_limit = gpq::spin_limit();
+    d.lp_begin = lp_begin;
+    d.lp_end = sharded ? lp_end : cfg.num_lps;
+    d.shard_lps = shard_lps;
+    d.out_cap = out_cap;
+    d.outbox = sharded ? outbox : nullptr;
+    d.out_n = out_n;
     return d;
   }
   LpQueueDev lq() const {
@@ -117,7 +131,8 @@ struct gpq_phold {
 
   ~gpq_phold() {
     for (void* p : {(void*)items, (void*)qa, (void*)qb, (void*)qc, (void*)links, (void*)freestk, (void*)ibuf,
-                    (void*)icnt, (void*)count, (void*)csum, (void*)ohash, (void*)ctrl, (void*)acc, (void*)staging})
+                    (void*)icnt, (void*)count, (void*)csum, (void*)ohash, (void*)ctrl, (void*)acc, (void*)staging,
+                    (void*)outbox, (void*)out_n, (void*)inject_buf})
       if (p) cudaFree(p);
     if (h_ctrl) cudaFreeHost(h_ctrl);
     if (gaq) gpq::gaq_engine_destroy(gaq);
@@ -706,6 +721,126 @@ gpq_status gpq_phold_restore(gpq_phold* h, const void* buf, uint64_t size, void*
   }
   GPQ_CUDA_TRY(cudaStreamSynchronize(st));
   h->finalized = false;
+  return GPQ_OK;
+}
+
+gpq_status gpq_phold_shard_create(const gpq_phold_config* cfg, uint32_t rank, uint32_t world,
+                                  uint32_t outbox_capacity, gpq_phold** out) {
+  GPQ_CHECK_ARG(cfg && out, "NULL argument");
+  *out = nullptr;
+  GPQ_CHECK_ARG(world >= 1 && rank < world, "need world >= 1 and rank < world");
+  GPQ_CHECK_ARG(cfg->queue_kind == GPQ_QUEUE_LHQ || cfg->queue_kind == GPQ_QUEUE_LSQ ||
+                    (cfg->queue_kind == GPQ_QUEUE_LAQ && cfg->laq_mode != 2),
+                "sharded runs take the per-LP queue kinds (LAQ sorted or selection form, LHQ, LSQ)");
+  GPQ_CHECK_ARG(cfg->num_lps >= world, "need at least one LP per shard");
+  gpq_phold* h = nullptr;
+  gpq_status r = gpq_phold_create(cfg, &h);
+  if (r != GPQ_OK) return r;
+  const uint32_t L = h->cfg.num_lps;
+  h->sharded = true;
+  h->rank = rank;
+  h->world = world;
+  h->shard_lps = (uint32_t)(((uint64_t)L + world - 1) / world);
+  h->lp_begin = std::min<uint32_t>(L, rank * h->shard_lps);
+  h->lp_end = (uint32_t)std::min<uint64_t>(L, (uint64_t)h->lp_begin + h->shard_lps);
+  // default: as many handed-over children per destination as this shard's insert buffers hold
+  h->out_cap = outbox_capacity ? outbox_capacity
+                               : (uint32_t)std::min<uint64_t>((uint64_t)(h->lp_end - h->lp_begin) * h->cfg.insert_capacity,
+                                                              1u << 26);
+  cudaError_t e = cudaMalloc(&h->outbox, std::max<uint64_t>(1, (uint64_t)world * h->out_cap) * sizeof(gpq_item));
+  if (e == cudaSuccess) e = cudaMalloc(&h->out_n, world * sizeof(uint32_t));
+  if (e != cudaSuccess) {
+    gpq::set_last_error("gpq_phold_shard_create: %s", cudaGetErrorString(e));
+    gpq_phold_destroy(h);
+    return e == cudaErrorMemoryAllocation ? GPQ_ERR_NOMEM : GPQ_ERR_CUDA;
+  }
+  *out = h;
+  return GPQ_OK;
+}
+
+gpq_status gpq_phold_shard_range(gpq_phold* h, uint32_t* lp_begin, uint32_t* lp_end, uint32_t* outbox_capacity) {
+  GPQ_CHECK_ARG(h && h->sharded, "not a shard handle");
+  if (lp_begin) *lp_begin = h->lp_begin;
+  if (lp_end) *lp_end = h->lp_end;
+  if (outbox_capacity) *outbox_capacity = h->out_cap;
+  return GPQ_OK;
+}
+
+gpq_status gpq_phold_shard_populate(gpq_phold* h, float* local_min, void* stream) {
+  GPQ_CHECK_ARG(h && h->sharded && local_min, "not a shard handle or NULL argument");
+  gpq_status r = gpq_phold_populate(h, nullptr, 0, stream);
+  if (r != GPQ_OK) return r;
+  const cudaStream_t st = gpq::as_stream(stream, h->own);
+  GPQ_CUDA_TRY(cudaMemcpyAsync(h->h_ctrl, h->ctrl, sizeof(PholdCtrl), cudaMemcpyDeviceToHost, st));
+  GPQ_CUDA_TRY(cudaStreamSynchronize(st));
+  *local_min = gpq_u2f(h->h_ctrl->mins[0]);
+  return GPQ_OK;
+}
+
+gpq_status gpq_phold_shard_window(gpq_phold* h, float global_min, float* local_min, uint32_t* out_counts,
+                                  void* stream) {
+  GPQ_CHECK_ARG(h && h->sharded && local_min && out_counts, "not a shard handle or NULL argument");
+  GPQ_CHECK_ARG(h->populated, "gpq_phold_shard_window before gpq_phold_shard_populate");
+  GPQ_CHECK_ARG(global_min < h->cfg.end_time, "the run has ended: global_min >= end_time");
+  const cudaStream_t st = gpq::as_stream(stream, h->own);
+  const uint32_t s = h->phase;
+  const uint32_t mb = gpq_f2u(global_min);
+  GPQ_CUDA_TRY(cudaMemcpyAsync(&h->ctrl->mins[s % 3], &mb, sizeof(mb), cudaMemcpyHostToDevice, st));
+  GPQ_CUDA_TRY(cudaMemsetAsync(h->out_n, 0, h->world * sizeof(uint32_t), st));
+  const uint32_t gpb = h->block / h->ks.group;  // LPs per CTA and round
+  const uint32_t grid = std::max(1u, (h->lp_end - h->lp_begin + gpb - 1) / gpb);
+  PholdDev d = h->dev();
+  LpQueueDev q = h->lq();
+  InsDev ib = h->ins();
+  uint32_t phase = s;
+  void* args[] = {&d, &q, &ib, &phase};
+  GPQ_CUDA_TRY(cudaLaunchKernel(h->ks.window, dim3(grid), dim3(h->block), args, h->window_smem(), st));
+  ++h->phase;
+  GPQ_CUDA_TRY(cudaMemcpyAsync(h->h_ctrl, h->ctrl, sizeof(PholdCtrl), cudaMemcpyDeviceToHost, st));
+  GPQ_CUDA_TRY(cudaMemcpyAsync(out_counts, h->out_n, h->world * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  GPQ_CUDA_TRY(cudaStreamSynchronize(st));
+  *local_min = gpq_u2f(h->h_ctrl->mins[(s + 1) % 3]);
+  if (h->h_ctrl->err) {
+    gpq::set_last_error("sharded PHOLD: device error %u in window %u", h->h_ctrl->err, s);
+    return (gpq_status)h->h_ctrl->err;
+  }
+  return GPQ_OK;
+}
+
+gpq_status gpq_phold_shard_outbox(gpq_phold* h, gpq_item** items, uint32_t* capacity) {
+  GPQ_CHECK_ARG(h && h->sharded && items, "not a shard handle or NULL argument");
+  *items = h->outbox;
+  if (capacity) *capacity = h->out_cap;
+  return GPQ_OK;
+}
+
+gpq_status gpq_phold_shard_inject(gpq_phold* h, const gpq_item* items, uint64_t n, int on_device, void* stream) {
+  GPQ_CHECK_ARG(h && h->sharded, "not a shard handle");
+  GPQ_CHECK_ARG(h->phase > 0, "gpq_phold_shard_inject before the first window");
+  if (n == 0) return GPQ_OK;
+  GPQ_CHECK_ARG(items, "items is NULL");
+  const cudaStream_t st = gpq::as_stream(stream, h->own);
+  const gpq_item* src = items;
+  if (!on_device) {
+    if (h->inject_cap < n) {
+      if (h->inject_buf) cudaFree(h->inject_buf);
+      h->inject_buf = nullptr;
+      h->inject_cap = 0;
+      GPQ_CUDA_TRY(cudaMalloc(&h->inject_buf, n * sizeof(gpq_item)));
+      h->inject_cap = n;
+    }
+    GPQ_CUDA_TRY(cudaMemcpyAsync(h->inject_buf, items, n * sizeof(gpq_item), cudaMemcpyHostToDevice, st));
+    src = h->inject_buf;
+  }
+  const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, 4096));
+  phold_inject_kernel<<<grid, 256, 0, st>>>(h->dev(), h->ins(), src, n, (h->phase - 1) & 1u);
+  GPQ_CUDA_TRY(cudaGetLastError());
+  GPQ_CUDA_TRY(cudaMemcpyAsync(h->h_ctrl, h->ctrl, sizeof(PholdCtrl), cudaMemcpyDeviceToHost, st));
+  GPQ_CUDA_TRY(cudaStreamSynchronize(st));
+  if (h->h_ctrl->err) {
+    gpq::set_last_error("sharded PHOLD: handed-over items rejected (error %u)", h->h_ctrl->err);
+    return (gpq_status)h->h_ctrl->err;
+  }
   return GPQ_OK;
 }
 

@@ -29,6 +29,15 @@ struct PholdDev {
   unsigned long long* ohash;
   PholdCtrl* ctrl;
   uint64_t spin_limit;
+  // Sharded runs (per-LP queue kinds): this handle processes LPs [lp_begin, lp_end) of the
+  // L-LP arrays; a child for another shard's LP goes to outbox[dest][out_cap] (dest =
+  // lp / shard_lps, count out_n[dest]) for the host to hand over between windows.
+  // Unsharded: [0, L) and outbox == nullptr.
+  uint32_t lp_begin, lp_end;
+  uint32_t shard_lps;
+  uint32_t out_cap;
+  gpq_item* outbox;
+  uint32_t* out_n;
 };
 
 // A group of G consecutive lanes of one warp working on one LP.
@@ -97,6 +106,17 @@ __device__ __forceinline__ uint32_t phold_process_event(const PholdDev& d, const
   gpq_item pe = e;
   pe.aux = e.lp;
   const gpq_item ch = gpq_phold_child(d.p, pe);
+  if (d.outbox && (ch.lp < d.lp_begin || ch.lp >= d.lp_end)) {  // another shard's LP
+    const uint32_t dest = ch.lp / d.shard_lps;
+    const uint32_t pos = atomicAdd(&d.out_n[dest], 1u);
+    if (pos < d.out_cap) {
+      d.outbox[(size_t)dest * d.out_cap + pos] = ch;
+    } else {
+      gpq_set_error(&d.ctrl->err, GPQ_ERR_INSERT_FULL);
+      atomicOr(err_slot, 1u);
+    }
+    return gpq_f2u(ch.ts);
+  }
   const uint32_t pos = atomicAdd(&ib.cnt[(size_t)curb * d.L + ch.lp], 1u);
   if (pos < ib.ibc) {
     ib.buf[((size_t)curb * d.L + ch.lp) * ib.ibc + pos] = ch;

@@ -67,10 +67,10 @@ static __global__ void phold_populate_kernel(PholdDev d, LpQueueDev q, uint32_t 
   gpq_item* s_it = reinterpret_cast<gpq_item*>(smem_raw) + (size_t)wib * per_lp;
   uint64_t* s_key = reinterpret_cast<uint64_t*>(reinterpret_cast<gpq_item*>(smem_raw) + (size_t)wpb * per_lp) +
                     (size_t)wib * per_lp;
-  const uint32_t lp = blockIdx.x * wpb + wib;
+  const uint32_t lp = d.lp_begin + blockIdx.x * wpb + wib;
   const uint32_t cap = 1u << q.cap_log2;
   uint32_t mn = kInfBits;
-  if (lp < d.L) {
+  if (lp < d.lp_end) {
     for (uint32_t j = lane; j < per_lp; j += 32) {
       gpq_item e;
       if (src) {
@@ -166,19 +166,19 @@ __device__ __forceinline__ void phold_window_body(const PholdDev& d, const typen
   uint32_t* err_slot = &d.ctrl->errs[(s + 1u) % 3u];
   const uint32_t prevb = (s + 1u) & 1u, curb = s & 1u;
   const uint32_t ngroups = gridDim.x * gpb;
-  const uint32_t first = blockIdx.x * gpb;
+  const uint32_t first = d.lp_begin + blockIdx.x * gpb;
   uint32_t mn = kInfBits;
-  for (uint32_t r0 = 0; first + r0 * ngroups < d.L; r0 += kStageRounds) {
+  for (uint32_t r0 = 0; first + r0 * ngroups < d.lp_end; r0 += kStageRounds) {
     if (threadIdx.x == 0) *st.cnt = 0;
     for (uint32_t t = threadIdx.x; t < nslots; t += blockDim.x) st.lp[t] = ~0u;
     __syncthreads();
     // A: merge + stage, one LP per lane group per round (metadata prefetched one round ahead)
     uint32_t lp = first + gib + r0 * ngroups;
     typename Q::Meta next;
-    if (lp < d.L) next = Q::load_meta(d, q, ib, lp, prevb);
-    for (uint32_t r = 0; r < kStageRounds && lp < d.L; ++r, lp += ngroups) {
+    if (lp < d.lp_end) next = Q::load_meta(d, q, ib, lp, prevb);
+    for (uint32_t r = 0; r < kStageRounds && lp < d.lp_end; ++r, lp += ngroups) {
       const typename Q::Meta cur = next;
-      if (r + 1 < kStageRounds && lp + ngroups < d.L) next = Q::load_meta(d, q, ib, lp + ngroups, prevb);
+      if (r + 1 < kStageRounds && lp + ngroups < d.lp_end) next = Q::load_meta(d, q, ib, lp + ngroups, prevb);
       mn = min(mn, Q::stage_lp(d, q, ib, lp, r * gpb + gib, s, bound, sm, st, g, err_slot, cur));
     }
     __syncthreads();
@@ -302,7 +302,7 @@ static __global__ void phold_finalize_kernel(PholdDev d, LpQueueDev q, InsDev ib
   const uint32_t cap = 1u << q.cap_log2, mask = cap - 1u;
   uint64_t pend = 0, pcs = 0, dig = 0, com = 0;
   uint32_t pmin = kInfBits;
-  for (uint32_t lp = blockIdx.x * wpb + (threadIdx.x >> 5); lp < d.L; lp += nwarps) {
+  for (uint32_t lp = d.lp_begin + blockIdx.x * wpb + (threadIdx.x >> 5); lp < d.lp_end; lp += nwarps) {
     const gpq_item* items = q.items + ((size_t)lp << q.cap_log2);
     uint32_t first = 0, n = 0;
     if (q.kind == GPQ_QUEUE_LAQ) { first = q.a[lp]; n = q.b[lp] - first; }
@@ -348,4 +348,21 @@ static __global__ void phold_finalize_kernel(PholdDev d, LpQueueDev q, InsDev ib
 static __global__ void phold_children_kernel(gpq_phold_params p, const gpq_item* __restrict__ ev, gpq_item* out, uint64_t n) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
     out[i] = gpq_phold_child(p, ev[i]);
+}
+
+// Sharded runs: items handed over from other shards after window s go into the insert
+// buffers that window s filled (parity curb), so window s + 1 merges them with this
+// shard's own children.  Items for LPs outside the shard are an argument error.
+static __global__ void phold_inject_kernel(PholdDev d, InsDev ib, const gpq_item* __restrict__ items, uint64_t n,
+                                           uint32_t curb) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const gpq_item it = items[i];
+    if (it.lp < d.lp_begin || it.lp >= d.lp_end) {
+      gpq_set_error(&d.ctrl->err, GPQ_ERR_INVALID);
+      continue;
+    }
+    const uint32_t pos = atomicAdd(&ib.cnt[(size_t)curb * d.L + it.lp], 1u);
+    if (pos < ib.ibc) ib.buf[((size_t)curb * d.L + it.lp) * ib.ibc + pos] = it;
+    else gpq_set_error(&d.ctrl->err, GPQ_ERR_INSERT_FULL);
+  }
 }

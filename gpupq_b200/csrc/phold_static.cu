@@ -139,9 +139,10 @@ extern "C" gpq_status gpq_phold_run_static(const gpq_phold_config* cfg_in, const
   GPQ_CUDA_TRY(cudaGetDevice(&dev));
   GPQ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
 
-  PholdDev d;
+  PholdDev d{};  // unsharded: all LPs, no outbox
   d.p = gpq::phold_params_of(c);
   d.L = c.num_lps;
+  d.lp_end = c.num_lps;
   d.count = d_count;
   d.csum = reinterpret_cast<unsigned long long*>(d_csum);
   d.ohash = reinterpret_cast<unsigned long long*>(d_ohash);

@@ -227,6 +227,32 @@ GPQ_API gpq_status gpq_phold_children(const gpq_phold_config* cfg, const gpq_ite
 GPQ_API gpq_status gpq_phold_snapshot(gpq_phold* h, void* buf, uint64_t capacity, uint64_t* size, void* stream);
 GPQ_API gpq_status gpq_phold_restore(gpq_phold* h, const void* buf, uint64_t size, void* stream);
 
+/* Sharded PHOLD: one handle per shard (rank) of a run over cfg->num_lps LPs; shard r
+ * holds LPs [r*P, min((r+1)*P, num_lps)), P = ceil(num_lps / world), and processes
+ * their events.  The reference runs one GPU; this splits the LP space across GPUs with
+ * one exchange per window, driven by the host (gpupq_b200.shard drives it over
+ * torch.distributed):
+ *   populate -> local minimum; the global minimum is the minimum over shards;
+ *   window(global minimum) -> the shard's safe events run; children for other shards'
+ *     LPs wait in the outbox ([world][capacity] device items, counts per destination);
+ *     local minimum (pending events and all children, handed over or not);
+ *   inject(the items other shards handed to this one) -> merged in the next window;
+ *   repeat while the global minimum is below end_time.
+ * A child is never safe in its parent's window, so handing children over between windows
+ * changes no result: the shards' committed counts, pending events and digests add up
+ * (final minimum: the minimum) to those of the unsharded run.  Per-LP queue kinds only
+ * (LAQ sorted or selection form, LHQ, LSQ).  outbox_capacity 0 = the shard's LPs times
+ * insert_capacity per destination.  gpq_phold_result_get gives the shard's part. */
+GPQ_API gpq_status gpq_phold_shard_create(const gpq_phold_config* cfg, uint32_t rank, uint32_t world,
+                                          uint32_t outbox_capacity, gpq_phold** out);
+GPQ_API gpq_status gpq_phold_shard_range(gpq_phold* h, uint32_t* lp_begin, uint32_t* lp_end, uint32_t* outbox_capacity);
+GPQ_API gpq_status gpq_phold_shard_populate(gpq_phold* h, float* local_min, void* stream);
+GPQ_API gpq_status gpq_phold_shard_window(gpq_phold* h, float global_min, float* local_min, uint32_t* out_counts,
+                                          void* stream);
+GPQ_API gpq_status gpq_phold_shard_outbox(gpq_phold* h, gpq_item** items, uint32_t* capacity);
+GPQ_API gpq_status gpq_phold_shard_inject(gpq_phold* h, const gpq_item* items, uint64_t n, int on_device,
+                                          void* stream);
+
 /* Launch geometry of the last gpq_phold_run: persistent grid (CTAs), CTA size, and the
  * number of kernel launches the run made (1 for the persistent loop, one per window
  * for the plain loop). */

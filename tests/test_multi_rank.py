@@ -1,7 +1,8 @@
 """The multi-GPU bench path on CPU: two gloo ranks reduce their device times and event
 counts the way `bench.py --gpus 2` does under torchrun (max of times, sum of events),
-and each rank runs its own replica seed.  PHOLD here shards as replicas only: every rank
-runs a whole instance, so there is no data-path collective to test beyond these."""
+and each rank runs its own replica seed.  The bench runs replicas (every rank a whole
+instance); one run sharded across ranks, with its per-window exchange, is tested in
+test_shard.py."""
 import os
 import socket
 import sys
