@@ -360,6 +360,21 @@ def run_case(name):
             for _ in range(2):
                 r = a.solve(g)
             print(a.stats(), int(r[0]["expanded"]))
+    elif name == "gaq_sort_32m":
+        # the global array queue's post of 32 Mi items: min/max, 4 radix passes, merge
+        import time
+        N, L = 32 << 20, 65536
+        rng = np.random.default_rng(5)
+        items = np.zeros(N, G.ITEM_DTYPE)
+        items["ts"] = rng.uniform(0, 1000, N).astype(np.float32)
+        items["lp"] = rng.integers(0, L, N, dtype=np.uint32)
+        items["id"] = np.arange(N, dtype=np.uint32)
+        for _ in range(2):
+            with G.Queue("gaq", num_lps=L, capacity=N // L + 1, insert_capacity=N // L + 1) as q:
+                q.insert(items)
+                t = time.perf_counter()
+                q.post()
+                print(f"post of {N} items: {(time.perf_counter() - t) * 1e3:.2f} ms (host clock)")
     elif name == "phold_batched_36":
         reqs, n = G.serve_stream(99, 2000.0, 0.1)
         runs = [reqs[i].phold for i in range(n) if reqs[i].kind == G.REQ_PHOLD][:40]
@@ -393,7 +408,8 @@ def main():
     ap.add_argument("--tune-windows", type=int, default=200)
     ap.add_argument("--no-forms", action="store_true", help="skip the A*, batched and served sections")
     ap.add_argument("--served-seconds", type=float, default=1.0, help="length of the served request stream")
-    ap.add_argument("--case", default=None, choices=["astar_batched_1000", "astar_plain_2048", "phold_batched_36"],
+    ap.add_argument("--case", default=None,
+                    choices=["astar_batched_1000", "astar_plain_2048", "phold_batched_36", "gaq_sort_32m"],
                     help="run one small named workload twice and exit (profiling captures)")
     args = ap.parse_args()
     if args.case:

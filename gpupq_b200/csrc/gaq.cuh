@@ -50,17 +50,18 @@ static __global__ void rs_hist_kernel(const gpq_item* __restrict__ in, uint32_t 
   hist[threadIdx.x * ntiles + tile] = cnt[threadIdx.x];
 }
 
-// In-place exclusive scan of `total` counts (one CTA of 1024 threads): each thread owns
-// a contiguous run of ceil(total / 1024) entries, sums it, the CTA scans the 1024 sums
-// (warp shuffles + one round over the warp totals), and each thread writes its run.
-__device__ __forceinline__ uint32_t rs_scan_block(uint32_t* a, uint32_t total) {
+// Exclusive scan of `total` counts from `in` into `out` plus `add` (in == out allowed), by
+// one CTA: each thread owns a contiguous run of ceil(total / blockDim) entries, sums it,
+// the CTA scans the per-thread sums (warp shuffles + one round over the warp totals), and
+// each thread writes its run.  Returns the total (without `add`).
+__device__ __forceinline__ uint32_t rs_scan_into(const uint32_t* in, uint32_t* out, uint32_t total, uint32_t add) {
   __shared__ uint32_t wsum[32];
   __shared__ uint32_t s_all;
   const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
   const uint32_t per = (total + blockDim.x - 1) / blockDim.x;
   const uint32_t b0 = min(t * per, total), b1 = min(b0 + per, total);
   uint32_t sum = 0;
-  for (uint32_t i = b0; i < b1; ++i) sum += a[i];
+  for (uint32_t i = b0; i < b1; ++i) sum += in[i];
   uint32_t incl = sum;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
@@ -82,10 +83,10 @@ __device__ __forceinline__ uint32_t rs_scan_block(uint32_t* a, uint32_t total) {
     if (lane == nw - 1) s_all = wi;
   }
   __syncthreads();
-  uint32_t run = wsum[warp] + incl - sum;
+  uint32_t run = add + wsum[warp] + incl - sum;
   for (uint32_t i = b0; i < b1; ++i) {
-    const uint32_t v = a[i];
-    a[i] = run;
+    const uint32_t v = in[i];
+    out[i] = run;
     run += v;
   }
   const uint32_t all = s_all;
@@ -93,44 +94,114 @@ __device__ __forceinline__ uint32_t rs_scan_block(uint32_t* a, uint32_t total) {
   return all;
 }
 
+__device__ __forceinline__ uint32_t rs_scan_block(uint32_t* a, uint32_t total) { return rs_scan_into(a, a, total, 0u); }
+
 static __global__ void rs_scan_kernel(uint32_t* a, uint32_t total) { rs_scan_block(a, total); }
 
-// Stable scatter of one tile: items are taken in tile order (round j holds items
-// j*256 + t); an item's rank among same-digit items of the tile is the count in earlier
-// rounds + earlier warps of this round + lower lanes of its warp (warp match).
-static __global__ void rs_scatter_kernel(const gpq_item* __restrict__ in, gpq_item* out, uint32_t n, uint32_t kmin,
-                                         uint32_t shift, const uint32_t* __restrict__ off, uint32_t ntiles) {
-  __shared__ uint32_t run[256];
-  __shared__ uint32_t wc[kRsThreads / 32][256];
+// Device-wide exclusive scan in three kernels (gpq::scan_exclusive): chunk sums, one CTA
+// over the sums, then every chunk scanned from its base.
+static constexpr uint32_t kScanChunk = 4096;
+
+static __global__ void __launch_bounds__(1024) rs_chunk_sum_kernel(const uint32_t* __restrict__ in, uint32_t n,
+                                                                   uint32_t* sums) {
+  __shared__ uint32_t wsum[32];
+  const uint64_t c0 = (uint64_t)blockIdx.x * kScanChunk;
+  uint32_t s = 0;
+  for (uint32_t k = threadIdx.x; k < kScanChunk; k += blockDim.x)
+    if (c0 + k < n) s += in[c0 + k];
+  s = __reduce_add_sync(GPQ_FULL_MASK, s);
+  if ((threadIdx.x & 31u) == 0) wsum[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    uint32_t v = threadIdx.x < (blockDim.x >> 5) ? wsum[threadIdx.x] : 0u;
+    v = __reduce_add_sync(GPQ_FULL_MASK, v);
+    if (threadIdx.x == 0) sums[blockIdx.x] = v;
+  }
+}
+
+static __global__ void __launch_bounds__(1024) rs_chunk_scan_kernel(const uint32_t* in, uint32_t* out, uint32_t n,
+                                                                    const uint32_t* __restrict__ base) {
+  const uint64_t c0 = (uint64_t)blockIdx.x * kScanChunk;
+  const uint64_t rest = (uint64_t)n - c0;
+  rs_scan_into(in + c0, out + c0, (uint32_t)(rest < kScanChunk ? rest : kScanChunk), base[blockIdx.x]);
+}
+
+// Stable scatter of one tile through shared memory.  Warp w owns the tile's items
+// [w * 512, (w + 1) * 512), loaded 32 at a time (coalesced, all 16 loads in flight).  It
+// ranks them without block barriers: an item's rank among the same-digit items of its warp
+// is the warp's running count for the digit (warp-private counters, one leader lane per
+// group of equal digits updates it) plus the lower lanes of its round with that digit.
+// After one barrier, a digit's items of warp w start at the tile's start for the digit
+// (exclusive scan of the tile's counts) plus the counts of warps 0..w-1, which keeps the
+// tile order.  The tile is laid out in digit order in shared memory and written so that
+// consecutive threads write consecutive addresses of each digit's run: an item at shared
+// position k with digit d goes to off[d][tile] + k - (start of d in the tile).
+static constexpr uint32_t kRsWarps = kRsThreads / 32;
+static constexpr uint32_t kRsWarpItems = kRsTile / kRsWarps;
+
+static __global__ void __launch_bounds__(kRsThreads) rs_scatter_kernel(const gpq_item* __restrict__ in, gpq_item* out,
+                                                                       uint32_t n, uint32_t kmin, uint32_t shift,
+                                                                       const uint32_t* __restrict__ cnt,
+                                                                       const uint32_t* __restrict__ off, uint32_t ntiles) {
+  extern __shared__ __align__(16) unsigned char rs_smem[];
+  gpq_item* s_it = reinterpret_cast<gpq_item*>(rs_smem);  // [kRsTile]
+  __shared__ uint32_t gpos[256], wtot[kRsWarps];
+  __shared__ uint32_t wc[kRsWarps][256];  // per-warp digit counts, then the warp's start per digit
   const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
   const uint32_t tile = blockIdx.x;
-  run[t] = 0;
-  const uint32_t base = tile * kRsTile;
+  const uint32_t base = tile * kRsTile + warp * kRsWarpItems;
+  gpq_item ev[kRsPer];
+#pragma unroll
   for (uint32_t j = 0; j < kRsPer; ++j) {
-    for (uint32_t x = t; x < (kRsThreads / 32) * 256; x += kRsThreads) (&wc[0][0])[x] = 0;
-    __syncthreads();
-    const uint32_t i = base + j * kRsThreads + t;
-    const bool valid = i < n;
-    gpq_item e;
-    uint32_t dgt = 0;
-    if (valid) {
-      e = in[i];
-      dgt = rs_digit(e, kmin, shift);
-    }
+    const uint32_t i = base + j * 32 + lane;
+    if (i < n) ev[j] = in[i];
+  }
+  for (uint32_t d = lane; d < 256; d += 32) wc[warp][d] = 0;
+  // the tile's digit runs: exclusive scan of its counts (thread t = digit t)
+  const uint32_t c = cnt[(size_t)t * ntiles + tile];
+  uint32_t incl = c;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t u = __shfl_up_sync(GPQ_FULL_MASK, incl, o);
+    if (lane >= (uint32_t)o) incl += u;
+  }
+  if (lane == 31) wtot[warp] = incl;
+  __syncwarp();
+  // warp-private ranks
+  uint32_t rk[kRsPer];
+#pragma unroll
+  for (uint32_t j = 0; j < kRsPer; ++j) {
+    const bool valid = base + j * 32 + lane < n;
+    const uint32_t dgt = valid ? rs_digit(ev[j], kmin, shift) : 0u;
     const uint32_t peers = __match_any_sync(GPQ_FULL_MASK, valid ? dgt : (0x100u + lane));
-    if (valid && lane == (uint32_t)(__ffs(peers) - 1)) wc[warp][dgt] = __popc(peers);
-    __syncthreads();
-    if (valid) {
-      uint32_t pre = 0;
-      for (uint32_t w = 0; w < warp; ++w) pre += wc[w][dgt];
-      const uint32_t below = __popc(peers & ((1u << lane) - 1u));
-      out[off[dgt * ntiles + tile] + run[dgt] + pre + below] = e;
-    }
-    __syncthreads();
-    uint32_t sum = 0;
-    for (uint32_t w = 0; w < kRsThreads / 32; ++w) sum += wc[w][t];
-    run[t] += sum;
-    __syncthreads();
+    const uint32_t before = valid ? wc[warp][dgt] : 0u;
+    rk[j] = before + __popc(peers & ((1u << lane) - 1u));
+    __syncwarp();
+    if (valid && lane == (uint32_t)(__ffs(peers) - 1)) wc[warp][dgt] = before + __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+  // thread t = digit t: the tile's start for t, then each warp's start
+  uint32_t wbase = 0;
+  for (uint32_t w = 0; w < warp; ++w) wbase += wtot[w];
+  uint32_t pos = wbase + incl - c;
+  gpos[t] = off[(size_t)t * ntiles + tile] - pos;  // modulo 2^32; + k gives the output index
+#pragma unroll
+  for (uint32_t w = 0; w < kRsWarps; ++w) {
+    const uint32_t k = wc[w][t];
+    wc[w][t] = pos;
+    pos += k;
+  }
+  __syncthreads();
+#pragma unroll
+  for (uint32_t j = 0; j < kRsPer; ++j)
+    if (base + j * 32 + lane < n) s_it[wc[warp][rs_digit(ev[j], kmin, shift)] + rk[j]] = ev[j];
+  __syncthreads();
+  const uint32_t t0 = tile * kRsTile;
+  const uint32_t tn = min(kRsTile, n - t0);
+  for (uint32_t k = t; k < tn; k += kRsThreads) {
+    const gpq_item e = s_it[k];
+    out[gpos[rs_digit(e, kmin, shift)] + k] = e;
   }
 }
 
@@ -161,16 +232,27 @@ static __global__ void mp_merge_kernel(const gpq_item* __restrict__ A, uint32_t 
   for (uint32_t x = threadIdx.x; x < la; x += kMpThreads) s[x] = A[a0 + x];
   for (uint32_t x = threadIdx.x; x < lb; x += kMpThreads) s[la + x] = B[b0 + x];
   __syncthreads();
-  const uint32_t my0 = threadIdx.x * kMpPer;
-  if (my0 < la + lb) {
+  // each thread merges its kMpPer outputs into registers, the tile goes back to shared
+  // memory in output order, and the CTA writes it with coalesced stores
+  const uint32_t my0 = threadIdx.x * kMpPer, len = la + lb;
+  gpq_item r[kMpPer];
+  if (my0 < len) {
     uint32_t ia = mp_search(s, la, s + la, lb, my0);
     uint32_t ib = my0 - ia;
-    const uint32_t lim = min(my0 + kMpPer, la + lb);
-    for (uint32_t o = my0; o < lim; ++o) {
-      const bool take_a = ib >= lb || (ia < la && gpq_f2u(s[ia].ts) <= gpq_f2u(s[la + ib].ts));
-      out[d0 + o] = take_a ? s[ia++] : s[la + ib++];
+#pragma unroll
+    for (uint32_t k = 0; k < kMpPer; ++k) {
+      if (my0 + k < len) {
+        const bool take_a = ib >= lb || (ia < la && gpq_f2u(s[ia].ts) <= gpq_f2u(s[la + ib].ts));
+        r[k] = take_a ? s[ia++] : s[la + ib++];
+      }
     }
   }
+  __syncthreads();
+#pragma unroll
+  for (uint32_t k = 0; k < kMpPer; ++k)
+    if (my0 + k < len) s[my0 + k] = r[k];
+  __syncthreads();
+  for (uint32_t x = threadIdx.x; x < len; x += kMpThreads) out[d0 + x] = s[x];
 }
 
 // GAQ engine state visible to kernels.

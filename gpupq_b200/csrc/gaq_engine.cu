@@ -11,23 +11,54 @@
 
 namespace gpq {
 
-size_t radix_hist_words(uint32_t n) { return (size_t)256 * std::max<uint32_t>(1u, (n + kRsTile - 1) / kRsTile); }
+size_t scan_scratch_words(uint64_t n) { return (size_t)((n + kScanChunk - 1) / kScanChunk) + 1; }
+
+gpq_status scan_exclusive(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* scratch, cudaStream_t st) {
+  if (n == 0) return GPQ_OK;
+  if (n <= 16 * kScanChunk) {  // one CTA: at most 64 entries a thread
+    if (in != out) GPQ_CUDA_TRY(cudaMemcpyAsync(out, in, (size_t)n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+    rs_scan_kernel<<<1, 1024, 0, st>>>(out, n);
+  } else {
+    const uint32_t chunks = (n + kScanChunk - 1) / kScanChunk;
+    rs_chunk_sum_kernel<<<chunks, 1024, 0, st>>>(in, n, scratch);
+    rs_scan_kernel<<<1, 1024, 0, st>>>(scratch, chunks);
+    rs_chunk_scan_kernel<<<chunks, 1024, 0, st>>>(in, out, n, scratch);
+  }
+  GPQ_CUDA_TRY(cudaGetLastError());
+  return GPQ_OK;
+}
+
+static uint32_t radix_tiles(uint32_t n) { return std::max<uint32_t>(1u, (n + kRsTile - 1) / kRsTile); }
+
+// counts [256][tiles], their exclusive scan [256][tiles], scan scratch
+size_t radix_hist_words(uint32_t n) {
+  const size_t cells = (size_t)256 * radix_tiles(n);
+  return 2 * cells + scan_scratch_words(cells);
+}
 
 gpq_status radix_sort_by_ts(gpq_item* a, gpq_item* b, uint32_t n, uint32_t kmin, uint32_t kmax, uint32_t* hist,
                             gpq_item** sorted, cudaStream_t st) {
   *sorted = a;
   if (n <= 1 || kmax <= kmin) return GPQ_OK;
+  GPQ_CUDA_TRY(cudaFuncSetAttribute(rs_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(kRsTile * sizeof(gpq_item))));
   const uint32_t range = kmax - kmin;
   const uint32_t bits = 32 - __builtin_clz(range);
   const uint32_t passes = (bits + 7) / 8;
-  const uint32_t ntiles = (n + kRsTile - 1) / kRsTile;
+  const uint32_t ntiles = radix_tiles(n);
+  const uint32_t cells = 256 * ntiles;
+  uint32_t* cnt = hist;
+  uint32_t* off = hist + cells;
+  uint32_t* scratch = off + cells;
   gpq_item* src = a;
   gpq_item* dst = b;
   for (uint32_t p = 0; p < passes; ++p) {
     const uint32_t shift = 8 * p;
-    rs_hist_kernel<<<ntiles, kRsThreads, 0, st>>>(src, n, kmin, shift, hist, ntiles);
-    rs_scan_kernel<<<1, 1024, 0, st>>>(hist, 256 * ntiles);
-    rs_scatter_kernel<<<ntiles, kRsThreads, 0, st>>>(src, dst, n, kmin, shift, hist, ntiles);
+    rs_hist_kernel<<<ntiles, kRsThreads, 0, st>>>(src, n, kmin, shift, cnt, ntiles);
+    gpq_status s = scan_exclusive(cnt, off, cells, scratch, st);
+    if (s != GPQ_OK) return s;
+    rs_scatter_kernel<<<ntiles, kRsThreads, kRsTile * sizeof(gpq_item), st>>>(src, dst, n, kmin, shift, cnt, off,
+                                                                              ntiles);
     GPQ_CUDA_TRY(cudaGetLastError());
     std::swap(src, dst);
   }
@@ -43,6 +74,11 @@ gpq_status merge_by_ts(const gpq_item* A, uint32_t na, const gpq_item* B, uint32
   mp_merge_kernel<<<grid, kMpThreads, 0, st>>>(A, na, B, nb, out);
   GPQ_CUDA_TRY(cudaGetLastError());
   return GPQ_OK;
+}
+
+// The engine's hist words serve the bulk sort and the window loop's smaller radix tiles.
+static size_t engine_hist_words(uint32_t cap) {
+  return std::max<size_t>(radix_hist_words(cap), (size_t)256 * std::max<uint32_t>(1u, (cap + kWinRsTile - 1) / kWinRsTile));
 }
 
 struct GaqEngine {
@@ -110,8 +146,7 @@ gpq_status gaq_engine_create(const gpq_phold_config& c, GaqEngine** out) {
   if ((e = cudaMalloc(&g->stg_cnt, (size_t)c.num_lps * sizeof(uint32_t))) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&g->info, 8 * sizeof(uint32_t))) != cudaSuccess) return fail(e);
   // the bulk sort's tiles (kRsTile) and the window loop's smaller ones (kWinRsTile)
-  if ((e = cudaMalloc(&g->hist, (size_t)256 * std::max<uint32_t>(1u, (g->cap + kWinRsTile - 1) / kWinRsTile) *
-                                    sizeof(uint32_t))) != cudaSuccess)
+  if ((e = cudaMalloc(&g->hist, engine_hist_words(g->cap) * sizeof(uint32_t))) != cudaSuccess)
     return fail(e);
   if ((e = cudaFuncSetAttribute(gaq_win_merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)(2 * kMpTile * sizeof(gpq_item)))) != cudaSuccess)
@@ -143,7 +178,7 @@ void gaq_engine_state(GaqEngine* g, std::vector<std::pair<void*, size_t>>* dev,
   dev->push_back({g->stg, L * g->c.insert_capacity * sizeof(gpq_item)});
   dev->push_back({g->stg_cnt, L * sizeof(uint32_t)});
   dev->push_back({g->info, 8 * sizeof(uint32_t)});
-  dev->push_back({g->hist, (size_t)256 * std::max<uint32_t>(1u, (g->cap + kWinRsTile - 1) / kWinRsTile) * sizeof(uint32_t)});
+  dev->push_back({g->hist, engine_hist_words(g->cap) * sizeof(uint32_t)});
   dev->push_back({g->acc, 8 * sizeof(unsigned long long)});
   dev->push_back({g->win, sizeof(GaqWin)});
   dev->push_back({g->dig, 256 * sizeof(uint32_t)});

@@ -16,10 +16,15 @@ namespace gpq {
 // Stable sort of n items by timestamp bits with the project's LSD radix sort.
 // Keys must lie in [kmin, kmax]; only ceil(log2(kmax - kmin + 1) / 8) passes run.  The
 // items start in `a`; `b` is a second buffer of n items; `hist` holds
-// 256 * ceil(n / 4096) words.  *sorted receives a or b, whichever holds the result.
+// radix_hist_words(n) words.  *sorted receives a or b, whichever holds the result.
 gpq_status radix_sort_by_ts(gpq_item* a, gpq_item* b, uint32_t n, uint32_t kmin, uint32_t kmax, uint32_t* hist,
                             gpq_item** sorted, cudaStream_t st);
 size_t radix_hist_words(uint32_t n);
+
+// Exclusive scan of n words from `in` into `out` (in == out allowed) over the whole GPU;
+// `scratch` holds scan_scratch_words(n) words.
+gpq_status scan_exclusive(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* scratch, cudaStream_t st);
+size_t scan_scratch_words(uint64_t n);
 
 // Merge two arrays sorted by timestamp bits into `out` (A first on equal timestamps).
 gpq_status merge_by_ts(const gpq_item* A, uint32_t na, const gpq_item* B, uint32_t nb, gpq_item* out,

@@ -110,7 +110,7 @@ __global__ void gq_count_lp_kernel(const gpq_item* __restrict__ arr, uint32_t n,
 class GaqQueue final : public QueueImpl {
  public:
   ~GaqQueue() override {
-    for (void* p : {(void*)arr_[0], (void*)arr_[1], (void*)pend_, (void*)pend_tmp_, (void*)hist_, (void*)idx_,
+    for (void* p : {(void*)arr_[0], (void*)arr_[1], (void*)pend_, (void*)pend_tmp_, (void*)hist_, (void*)scan_tmp_, (void*)idx_,
                     (void*)cnt_, (void*)out_cnt_, (void*)off_, (void*)tmp_, (void*)taken_, (void*)keep_,
                     (void*)words_, (void*)out_})
       if (p) cudaFree(p);
@@ -133,6 +133,7 @@ class GaqQueue final : public QueueImpl {
     GPQ_CUDA_TRY(cudaMalloc(&pend_, (size_t)pend_cap_ * sizeof(gpq_item)));
     GPQ_CUDA_TRY(cudaMalloc(&pend_tmp_, (size_t)pend_cap_ * sizeof(gpq_item)));
     GPQ_CUDA_TRY(cudaMalloc(&hist_, radix_hist_words(pend_cap_) * sizeof(uint32_t)));
+    GPQ_CUDA_TRY(cudaMalloc(&scan_tmp_, scan_scratch_words((uint64_t)std::max(cap_, L_) + 1) * sizeof(uint32_t)));
     GPQ_CUDA_TRY(cudaMalloc(&idx_, (size_t)L_ * lpcap_ * sizeof(uint32_t)));
     GPQ_CUDA_TRY(cudaMalloc(&tmp_, (size_t)L_ * lpcap_ * sizeof(gpq_item)));
     GPQ_CUDA_TRY(cudaMalloc(&cnt_, (size_t)L_ * sizeof(uint32_t)));
@@ -213,8 +214,7 @@ class GaqQueue final : public QueueImpl {
     gq_take_kernel<<<grid(L_), 256, 0, st>>>(a, L_, idx_, cnt_, lpcap_, max_per_lp, taken_, tmp_, out_cnt_);
     GPQ_CUDA_TRY(cudaMemsetAsync(out_cnt_ + L_, 0, 4, st));
     GPQ_CUDA_TRY(cudaMemcpyAsync(off_, out_cnt_, (size_t)(L_ + 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
-    rs_scan_kernel<<<1, 1024, 0, st>>>(off_, L_ + 1);
-    GPQ_CUDA_TRY(cudaGetLastError());
+    if (gpq_status s_ = scan_exclusive(off_, off_, L_ + 1, scan_tmp_, st)) return s_;
     uint32_t total = 0;
     GPQ_CUDA_TRY(cudaMemcpyAsync(&total, off_ + L_, 4, cudaMemcpyDeviceToHost, st));
     GPQ_CUDA_TRY(cudaMemcpyAsync(&h_words_[8], &words_[8], 4, cudaMemcpyDeviceToHost, st));
@@ -234,7 +234,7 @@ class GaqQueue final : public QueueImpl {
     gq_gather_kernel<<<grid(L_), 256, 0, st>>>(L_, lpcap_, tmp_, out_cnt_, off_, out_);
     // stable compaction of the untaken prefix, followed by the rest of the array
     gq_keep_kernel<<<grid(c + 1), 256, 0, st>>>(taken_, c, keep_);
-    rs_scan_kernel<<<1, 1024, 0, st>>>(keep_, c + 1);
+    if (gpq_status s_ = scan_exclusive(keep_, keep_, c + 1, scan_tmp_, st)) return s_;
     gq_compact_kernel<<<grid(n_), 256, 0, st>>>(a, c, n_, taken_, keep_, arr_[cur_ ^ 1]);
     GPQ_CUDA_TRY(cudaGetLastError());
     if (total) GPQ_CUDA_TRY(cudaMemcpyAsync(out, out_, (size_t)total * sizeof(gpq_item), cudaMemcpyDeviceToHost, st));
@@ -257,7 +257,7 @@ class GaqQueue final : public QueueImpl {
     if (n_ == 0) return GPQ_OK;
     gq_clear_lp_kernel<<<grid(n_ + 1), 256, 0, st>>>(arr_[cur_], n_, lp, keep_);
     GPQ_CUDA_TRY(cudaMemcpyAsync(taken_, keep_, (size_t)(n_ + 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
-    rs_scan_kernel<<<1, 1024, 0, st>>>(keep_, n_ + 1);
+    if (gpq_status s_ = scan_exclusive(keep_, keep_, n_ + 1, scan_tmp_, st)) return s_;
     gq_select_kernel<<<grid(n_), 256, 0, st>>>(arr_[cur_], n_, taken_, keep_, arr_[cur_ ^ 1]);
     GPQ_CUDA_TRY(cudaGetLastError());
     uint32_t kept = 0;
@@ -302,6 +302,7 @@ class GaqQueue final : public QueueImpl {
   gpq_item* pend_ = nullptr;
   gpq_item* pend_tmp_ = nullptr;
   uint32_t* hist_ = nullptr;
+  uint32_t* scan_tmp_ = nullptr;  // scan_exclusive scratch
   uint32_t* idx_ = nullptr;
   uint32_t* cnt_ = nullptr;
   uint32_t* out_cnt_ = nullptr;
