@@ -102,7 +102,8 @@ class LaqQueue final : public LocalQueueBase {
     v->num_lps = L_;
     v->cap_log2 = cap_log2_;
     v->ibc = ibc_;
-    v->reserved = 0;
+    v->kind = GPQ_QUEUE_LAQ;
+    v->size = nullptr;
     return GPQ_OK;
   }
 

@@ -162,12 +162,40 @@ __global__ void lpq_clear_kernel(LpqDev q, uint32_t lp, LocalQueueCounters* ctr)
   }
 }
 
+__global__ void lpq_set_bound_kernel(float* bound, float value) { *bound = value; }
+
 class LpqQueue final : public LocalQueueBase {
  public:
   ~LpqQueue() override {
     for (void* p : {(void*)d_.items, (void*)d_.size, (void*)d_.root, (void*)d_.freetop, (void*)d_.links,
-                    (void*)d_.freestk, (void*)tmp_})
+                    (void*)d_.freestk, (void*)tmp_, (void*)bound_})
       if (p) cudaFree(p);
+  }
+
+  // The local heap queue's device view for model kernels (include/gpq/queue.cuh); the
+  // splay queue has none.
+  gpq_status device_view(gpq_device_queue* v) override {
+    if (d_.kind != GPQ_QUEUE_LHQ) return GPQ_ERR_UNSUPPORTED;
+    *v = gpq_device_queue{};
+    v->ring = d_.items;
+    v->ibuf = ibuf_;
+    v->icnt = icnt_;
+    v->bound = bound_;
+    v->enqueued = &ctr_->enqueued;
+    v->dequeued = &ctr_->dequeued;
+    v->err = &ctr_->err;
+    v->num_lps = L_;
+    v->cap_log2 = d_.cap_log2;
+    v->ibc = ibc_;
+    v->kind = GPQ_QUEUE_LHQ;
+    v->size = d_.size;
+    return GPQ_OK;
+  }
+
+  gpq_status set_bound(float b, cudaStream_t st) override {
+    lpq_set_bound_kernel<<<1, 1, 0, st>>>(bound_, b);
+    GPQ_CUDA_TRY(cudaGetLastError());
+    return GPQ_OK;
   }
 
   gpq_status init(const gpq_queue_config& c) {
@@ -191,6 +219,8 @@ class LpqQueue final : public LocalQueueBase {
       GPQ_CUDA_TRY(cudaMalloc(&d_.freestk, slots * sizeof(uint16_t)));
     }
     lpq_init_kernel<<<grid(), 256, 0, own_>>>(d_, L_);
+    GPQ_CUDA_TRY(cudaMalloc(&bound_, sizeof(float)));
+    lpq_set_bound_kernel<<<1, 1, 0, own_>>>(bound_, gpq_u2f(kInfBits));
     GPQ_CUDA_TRY(cudaGetLastError());
     GPQ_CUDA_TRY(cudaStreamSynchronize(own_));
     return GPQ_OK;
@@ -300,6 +330,7 @@ class LpqQueue final : public LocalQueueBase {
   uint32_t grid() const { return std::max(1u, std::min<uint32_t>((L_ + 255) / 256, 4096)); }
   LpqDev d_{};
   gpq_item* tmp_ = nullptr;
+  float* bound_ = nullptr;  // window bound of the device view
 };
 
 }  // namespace

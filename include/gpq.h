@@ -122,20 +122,23 @@ GPQ_API gpq_status gpq_queue_counts(gpq_queue* q, uint64_t* enqueued, uint64_t* 
  * queue_length, queue_clear, queue_insert_or_update; src/queue.cuh:46-70) are provided
  * as inline __device__ functions over this view by include/gpq/queue.cuh. */
 typedef struct gpq_device_queue {
-  gpq_item* ring;               /* [num_lps << cap_log2] per-LP sorted runs */
-  uint32_t* rd;                 /* per-LP read counter (fel_read); slot = counter & (cap - 1) */
-  uint32_t* wr;                 /* per-LP write counter (fel_write) */
+  gpq_item* ring;               /* [num_lps << cap_log2] per-LP sorted runs (LAQ) or 4-ary heaps (LHQ) */
+  uint32_t* rd;                 /* LAQ: per-LP read counter (fel_read); slot = counter & (cap - 1) */
+  uint32_t* wr;                 /* LAQ: per-LP write counter (fel_write) */
   gpq_item* ibuf;               /* [num_lps][ibc] items inserted since the last post */
   uint32_t* icnt;               /* [num_lps] */
   const float* bound;           /* queue_peek returns the head iff its ts < *bound */
   unsigned long long* enqueued; /* get_enqueue_count */
   unsigned long long* dequeued; /* get_dequeue_count */
   uint32_t* err;                /* sticky error word read by the next gpq_queue_post */
-  uint32_t num_lps, cap_log2, ibc, reserved;
+  uint32_t num_lps, cap_log2, ibc;
+  uint32_t kind;                /* GPQ_QUEUE_LAQ or GPQ_QUEUE_LHQ */
+  uint32_t* size;               /* LHQ: per-LP heap size (root at slot 0, children of i at 4i+1..4i+4) */
 } gpq_device_queue;
 
-/* Fills *out with the device pointers of a local array queue (GPQ_ERR_UNSUPPORTED for
- * the other kinds).  The view stays valid until gpq_queue_destroy. */
+/* Fills *out with the device pointers of a local array queue or a local heap queue
+ * (GPQ_ERR_UNSUPPORTED for the other kinds).  The view stays valid until
+ * gpq_queue_destroy. */
 GPQ_API gpq_status gpq_queue_device_view(gpq_queue* q, gpq_device_queue* out);
 
 /* Sets the window bound queue_peek tests against (the reference's global_min + LOOKAHEAD,

@@ -1,13 +1,15 @@
 /*
  * gpq/queue.cuh -- the reference's device queue functions for model kernels, over a
- * gpupq_b200 local array queue.
+ * gpupq_b200 local array queue or local heap queue.
  *
  * The reference binds queue_insert / queue_peek / queue_set_done / queue_is_empty /
  * queue_length / queue_clear / queue_insert_or_update to one queue implementation by
  * macro (src/queue.cuh:7-70) and model kernels call them per LP (PHOLD:
  * src/phold.cu:81-117).  Including this header in a CUDA translation unit gives those
  * names as inline __device__ functions over the device view of a gpq_queue (local array
- * queue), so a handler written like the reference's compiles against the library:
+ * queue: the head of the LP's sorted run; local heap queue: the root of the LP's 4-ary
+ * heap, src/local_heap_queue.cu), so a handler written like the reference's compiles
+ * against the library:
  *
  *     gpq_item* ev = NULL;
  *     int index = queue_peek(&ev, lp);          // head of lp's run if ts < the window bound
@@ -61,10 +63,41 @@ static __device__ __forceinline__ bool queue_insert(queue_item item) {
   return true;
 }
 
+/* Removes the root of a 4-ary heap of n > 0 items (one thread): the last item sifts
+ * down from the root past every child with a smaller (ts bits, id) key. */
+static __device__ __forceinline__ void gpq_heap4_pop(queue_item* h, uint32_t n) {
+  const uint32_t last = n - 1;
+  if (last == 0) return;
+  const queue_item x = h[last];
+  const uint64_t kx = gpq_lp_key(x);
+  uint32_t pos = 0;
+  for (;;) {
+    const uint32_t fc = pos * 4u + 1u;
+    if (fc >= last) break;
+    uint32_t b = fc;
+    uint64_t kb = gpq_lp_key(h[fc]);
+    for (uint32_t c = fc + 1u; c < fc + 4u && c < last; ++c) {
+      const uint64_t kc = gpq_lp_key(h[c]);
+      if (kc < kb) { kb = kc; b = c; }
+    }
+    if (kb >= kx) break;
+    h[pos] = h[b];
+    pos = b;
+  }
+  h[pos] = x;
+}
+
 /* queue_peek (src/queue.cuh:49-51): the index of lp's earliest item if it lies inside
  * the window (ts < bound), else -1; *item points at it until queue_set_done/post. */
 static __device__ __forceinline__ int queue_peek(queue_item** item, int lp) {
   const gpq_device_queue& q = gpq_bound_queue;
+  if (q.kind == GPQ_QUEUE_LHQ) {
+    if (q.size[lp] == 0u) return -1;
+    queue_item* it = q.ring + ((size_t)lp << q.cap_log2);
+    if (!(it->ts < *q.bound)) return -1;
+    *item = it;
+    return (int)((uint32_t)lp << q.cap_log2);
+  }
   const uint32_t rd = q.rd[lp];
   if (rd == q.wr[lp]) return -1;
   const uint32_t slot = rd & ((1u << q.cap_log2) - 1u);
@@ -78,7 +111,13 @@ static __device__ __forceinline__ int queue_peek(queue_item** item, int lp) {
 static __device__ __forceinline__ void queue_set_done(int index) {
   const gpq_device_queue& q = gpq_bound_queue;
   const uint32_t lp = (uint32_t)index >> q.cap_log2;
-  q.rd[lp] += 1u;
+  if (q.kind == GPQ_QUEUE_LHQ) {
+    const uint32_t n = q.size[lp];
+    gpq_heap4_pop(q.ring + ((size_t)lp << q.cap_log2), n);
+    q.size[lp] = n - 1u;
+  } else {
+    q.rd[lp] += 1u;
+  }
   atomicAdd(q.dequeued, 1ull);
 }
 
@@ -86,20 +125,27 @@ static __device__ __forceinline__ void queue_set_done(int index) {
  * last post (src/local_array_queue.cu:807-810). */
 static __device__ __forceinline__ bool queue_is_empty(int lp) {
   const gpq_device_queue& q = gpq_bound_queue;
-  return q.rd[lp] == q.wr[lp] && q.icnt[lp] == 0u;
+  const bool none = q.kind == GPQ_QUEUE_LHQ ? q.size[lp] == 0u : q.rd[lp] == q.wr[lp];
+  return none && q.icnt[lp] == 0u;
 }
 
-/* queue_length (src/queue.cuh:62-63): items in lp's run. */
+/* queue_length (src/queue.cuh:62-63): items in lp's run or heap. */
 static __device__ __forceinline__ int queue_length(int lp) {
   const gpq_device_queue& q = gpq_bound_queue;
-  return (int)(q.wr[lp] - q.rd[lp]);
+  return q.kind == GPQ_QUEUE_LHQ ? (int)q.size[lp] : (int)(q.wr[lp] - q.rd[lp]);
 }
 
 /* queue_clear (src/queue.cuh:65-66): drop lp's run. */
 static __device__ __forceinline__ void queue_clear(int lp) {
   const gpq_device_queue& q = gpq_bound_queue;
-  const uint32_t n = q.wr[lp] - q.rd[lp];
-  q.rd[lp] = q.wr[lp];
+  uint32_t n;
+  if (q.kind == GPQ_QUEUE_LHQ) {
+    n = q.size[lp];
+    q.size[lp] = 0u;
+  } else {
+    n = q.wr[lp] - q.rd[lp];
+    q.rd[lp] = q.wr[lp];
+  }
   atomicAdd(q.dequeued, (unsigned long long)n);
 }
 

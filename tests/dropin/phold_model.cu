@@ -42,7 +42,7 @@ extern "C" int dropin_phold_run(const gpq_phold_config* cfg, uint32_t* count, un
                                 unsigned long long* committed_out) {
   const uint32_t L = cfg->num_lps;
   gpq_queue_config qc = {};
-  qc.kind = GPQ_QUEUE_LAQ;
+  qc.kind = cfg->queue_kind;  // a local array queue or a local heap queue
   qc.num_lps = L;
   qc.capacity = cfg->capacity ? cfg->capacity : 256;
   qc.insert_capacity = cfg->insert_capacity ? cfg->insert_capacity : 64;

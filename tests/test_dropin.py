@@ -2,7 +2,7 @@
 reference's (a handler kernel calling queue_peek / queue_set_done / queue_insert, a host
 loop of get-min / window / handler / post steps) builds against the header and, on the
 GPU, commits exactly the oracle's per-LP sequences through a gpupq_b200 local array
-queue."""
+queue and through a local heap queue."""
 import ctypes
 import os
 import shutil
@@ -38,12 +38,13 @@ def test_dropin_model_builds():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("queue", ["laq", "lhq"])
 @pytest.mark.parametrize("dest", ["uniform", "ring"])
-def test_dropin_model_matches_oracle(gpu_lib, dest):
+def test_dropin_model_matches_oracle(gpu_lib, dest, queue):
     ring = dest == "ring"
     cfgd = dict(num_lps=700, events_per_lp=8, lookahead=0.5, end_time=15.0, seed=31,
                 dest_mode=1 if ring else 0)
-    cfg = G.make_phold_config(**cfgd, ring_width=16, queue="laq", capacity=256, insert_capacity=64)
+    cfg = G.make_phold_config(**cfgd, ring_width=16, queue=queue, capacity=256, insert_capacity=64)
     L = cfgd["num_lps"]
     count = np.zeros(L, np.uint32)
     csum = np.zeros(L, np.uint64)
