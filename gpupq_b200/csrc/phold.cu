@@ -457,6 +457,7 @@ static gpq_status sync_phase(gpq_phold* h, cudaStream_t st) {
 
 gpq_status gpq_phold_run(gpq_phold* h, void* stream) {
   GPQ_CHECK_ARG(h, "handle is NULL");
+  GPQ_CHECK_ARG(!h->sharded, "a shard handle runs window by window (gpq_phold_shard_window)");
   if (!h->populated) { gpq::set_last_error("gpq_phold_run before gpq_phold_populate"); return GPQ_ERR_NOT_READY; }
   cudaStream_t st = gpq::as_stream(stream, h->own);
   h->finalized = false;
@@ -483,6 +484,7 @@ gpq_status gpq_phold_run(gpq_phold* h, void* stream) {
 
 gpq_status gpq_phold_step(gpq_phold* h, uint32_t nsteps, int* done, void* stream) {
   GPQ_CHECK_ARG(h, "handle is NULL");
+  GPQ_CHECK_ARG(!h->sharded, "a shard handle runs window by window (gpq_phold_shard_window)");
   if (!h->populated) return GPQ_ERR_NOT_READY;
   h->finalized = false;
   if (h->is_hq) {

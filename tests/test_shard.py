@@ -282,6 +282,18 @@ def test_device_shards_over_gloo(gpu_lib):
 
 
 @pytest.mark.gpu
+def test_shard_handle_refuses_whole_runs(gpu_lib):
+    """A shard handle has no exchange of its own: gpq_phold_run / gpq_phold_step refuse it."""
+    import ctypes
+    import gpupq_b200 as G
+    from gpupq_b200 import shard as S
+    with S.PholdShard(_gpu_cfg(GPU_CASES[0], "laq"), 1, 2) as sh:
+        sh.populate()
+        assert G.lib().gpq_phold_run(sh._h, None) == 1
+        assert G.lib().gpq_phold_step(sh._h, 1, ctypes.byref(ctypes.c_int()), None) == 1
+
+
+@pytest.mark.gpu
 def test_outbox_overflow_is_reported(gpu_lib):
     import gpupq_b200 as G
     from gpupq_b200 import shard as S
