@@ -2,6 +2,7 @@
 #include <atomic>
 #include <cstdarg>
 #include <cstdio>
+#include <mutex>
 
 #include "host_common.h"
 
@@ -18,6 +19,16 @@ void set_last_error(const char* fmt, ...) {
 }
 
 uint64_t spin_limit() { return g_spin_limit.load(); }
+
+cudaError_t raise_smem_limit(const void* kernel, size_t bytes) {
+  static std::mutex m;
+  std::lock_guard<std::mutex> lock(m);
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
+  if (e != cudaSuccess) return e;
+  if ((size_t)fa.maxDynamicSharedSizeBytes >= bytes) return cudaSuccess;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
 
 }  // namespace gpq
 

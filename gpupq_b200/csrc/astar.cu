@@ -232,7 +232,7 @@ static gpq_status astar_solve_pass(gpq_astar* a, const gpq_astar_grid* grids, ui
   const void* kern = c.tile_worker ? (const void*)astar_persistent_kernel<true> : (const void*)astar_persistent_kernel<false>;
   const size_t smem = astar_worker_smem_bytes(ts, c.frontier_capacity) * (c.tile_worker ? c.block_threads / 32 : 1);
   GPQ_CHECK_ARG(smem <= 227u * 1024u, "tile, frontier_capacity and workers need more than 227 KB of shared memory");
-  GPQ_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  GPQ_CUDA_TRY(gpq::raise_smem_limit(kern, (int)smem));
   int dev = 0, sms = 0, per_sm = 0;
   GPQ_CUDA_TRY(cudaGetDevice(&dev));
   GPQ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));

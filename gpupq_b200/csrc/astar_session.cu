@@ -195,7 +195,7 @@ gpq_status gpq_astar_session_create(const gpq_astar_config* cfg, uint64_t max_ce
   s->kern = c.tile_worker ? (const void*)astar_persistent_kernel<true> : (const void*)astar_persistent_kernel<false>;
   s->smem = astar_worker_smem_bytes(c.tile, c.frontier_capacity) * (c.tile_worker ? c.block_threads / 32 : 1);
   int dev = 0, sms = 0, per_sm = 0;
-  GPQ_CUDA_TRY(cudaFuncSetAttribute(s->kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem));
+  GPQ_CUDA_TRY(gpq::raise_smem_limit(s->kern, (int)s->smem));
   GPQ_CUDA_TRY(cudaGetDevice(&dev));
   GPQ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   GPQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, s->kern, (int)c.block_threads, s->smem));

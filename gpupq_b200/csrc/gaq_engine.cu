@@ -40,8 +40,7 @@ gpq_status radix_sort_by_ts(gpq_item* a, gpq_item* b, uint32_t n, uint32_t kmin,
                             gpq_item** sorted, cudaStream_t st) {
   *sorted = a;
   if (n <= 1 || kmax <= kmin) return GPQ_OK;
-  GPQ_CUDA_TRY(cudaFuncSetAttribute(rs_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)(kRsTile * sizeof(gpq_item))));
+  GPQ_CUDA_TRY(gpq::raise_smem_limit(rs_scatter_kernel, (int)(kRsTile * sizeof(gpq_item))));
   const uint32_t range = kmax - kmin;
   const uint32_t bits = 32 - __builtin_clz(range);
   const uint32_t passes = (bits + 7) / 8;
@@ -148,8 +147,7 @@ gpq_status gaq_engine_create(const gpq_phold_config& c, GaqEngine** out) {
   // the bulk sort's tiles (kRsTile) and the window loop's smaller ones (kWinRsTile)
   if ((e = cudaMalloc(&g->hist, engine_hist_words(g->cap) * sizeof(uint32_t))) != cudaSuccess)
     return fail(e);
-  if ((e = cudaFuncSetAttribute(gaq_win_merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(2 * kMpTile * sizeof(gpq_item)))) != cudaSuccess)
+  if ((e = gpq::raise_smem_limit(gaq_win_merge_kernel, (int)(2 * kMpTile * sizeof(gpq_item)))) != cudaSuccess)
     return fail(e);
   if ((e = cudaMalloc(&g->acc, 8 * sizeof(unsigned long long))) != cudaSuccess) return fail(e);
   if ((e = cudaMallocHost(&g->h_info, 8 * sizeof(uint32_t))) != cudaSuccess) return fail(e);
@@ -159,8 +157,7 @@ gpq_status gaq_engine_create(const gpq_phold_config& c, GaqEngine** out) {
     return fail(e);
   if ((e = cudaMallocHost(&g->h_win, sizeof(GaqWin))) != cudaSuccess) return fail(e);
   const size_t smem = (size_t)(g->block / GaqEngine::G) * c.insert_capacity * sizeof(uint64_t);
-  if ((e = cudaFuncSetAttribute(gaq_process_kernel<GaqEngine::G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem)) != cudaSuccess)
+  if ((e = gpq::raise_smem_limit(gaq_process_kernel<GaqEngine::G>, (int)smem)) != cudaSuccess)
     return fail(e);
   *out = g;
   return GPQ_OK;

@@ -14,6 +14,18 @@ namespace gpq {
 void set_last_error(const char* fmt, ...);
 uint64_t spin_limit();
 
+// Raises `kernel`'s dynamic shared-memory limit on the current device to at least
+// `bytes`; never lowers it.  Several handles (and the allocation-free run) launch the
+// same kernel instantiations with different shared-memory sizes, so a limit set to one
+// caller's exact size would make another caller's larger launch fail.  Serialized by a
+// process-wide mutex; reads the current limit from the driver, so it holds after a
+// cudaDeviceReset too.
+cudaError_t raise_smem_limit(const void* kernel, size_t bytes);
+template <class K>
+inline cudaError_t raise_smem_limit(K* kernel, size_t bytes) {
+  return raise_smem_limit(reinterpret_cast<const void*>(kernel), bytes);
+}
+
 inline cudaStream_t as_stream(void* s, cudaStream_t fallback) {
   return s ? reinterpret_cast<cudaStream_t>(s) : fallback;
 }

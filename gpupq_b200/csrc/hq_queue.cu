@@ -63,8 +63,8 @@ class HqQueue final : public QueueImpl {
     GPQ_CUDA_TRY(cudaMemsetAsync(h_.meta, 0, 4 * sizeof(uint32_t), own_));
     GPQ_CUDA_TRY(cudaMemsetAsync(words_, 0, 8 * sizeof(uint32_t), own_));
     const int smem = (int)hq_smem_bytes(r);
-    GPQ_CUDA_TRY(cudaFuncSetAttribute(hq_post_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    GPQ_CUDA_TRY(cudaFuncSetAttribute(hq_dequeue_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    GPQ_CUDA_TRY(gpq::raise_smem_limit(hq_post_kernel, smem));
+    GPQ_CUDA_TRY(gpq::raise_smem_limit(hq_dequeue_kernel, smem));
     GPQ_CUDA_TRY(cudaStreamSynchronize(own_));
     return GPQ_OK;
   }

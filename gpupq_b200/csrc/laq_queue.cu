@@ -130,7 +130,7 @@ class LaqQueue final : public LocalQueueBase {
     GPQ_CUDA_TRY(cudaMalloc(&bound_, sizeof(float)));
     laq_set_bound_kernel<<<1, 1, 0, own_>>>(bound_, gpq_u2f(kInfBits));
     const size_t smem = 8 * laq_group_smem_bytes(ibc_, 32);
-    GPQ_CUDA_TRY(cudaFuncSetAttribute(laq_post_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    GPQ_CUDA_TRY(gpq::raise_smem_limit(laq_post_kernel, (int)smem));
     GPQ_CUDA_TRY(cudaStreamSynchronize(own_));
     return GPQ_OK;
   }

@@ -203,7 +203,7 @@ gpq_status gpq_phold_create(const gpq_phold_config* cfg_in, gpq_phold** out) {
     h->hq.ch = h->hq_sort[1];  // after populate: the children of a window
     TRY(cudaMalloc(&h->hq_hist, gpq::radix_hist_words((uint32_t)N) * sizeof(uint32_t)));
     TRY(cudaMalloc(&h->hq_mm, 2 * sizeof(uint32_t)));
-    TRY(cudaFuncSetAttribute(hq_phold_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hq_smem_bytes(r)));
+    TRY(gpq::raise_smem_limit(hq_phold_kernel, (int)hq_smem_bytes(r)));
   } else if (c.queue_kind == GPQ_QUEUE_LAQ && c.laq_mode == 2) {
     gpq::LabGeometry geo{};
     const gpq_status gs = gpq::lab_geometry(c, &geo);
@@ -266,8 +266,8 @@ gpq_status gpq_phold_create(const gpq_phold_config* cfg_in, gpq_phold** out) {
   }
   h->cfg.block_threads = h->block;
   const size_t smem = h->window_smem();
-  TRY(cudaFuncSetAttribute(h->ks.window, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  TRY(cudaFuncSetAttribute(h->ks.persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  TRY(gpq::raise_smem_limit(h->ks.window, (int)smem));
+  TRY(gpq::raise_smem_limit(h->ks.persistent, (int)smem));
 #undef TRY
   *out = h;
   return GPQ_OK;
@@ -364,7 +364,7 @@ gpq_status gpq_phold_populate(gpq_phold* h, const gpq_item* initial, uint64_t n,
   }
   const uint32_t wpb = 4;
   const size_t smem = (size_t)wpb * c.events_per_lp * (sizeof(gpq_item) + sizeof(uint64_t));
-  GPQ_CUDA_TRY(cudaFuncSetAttribute(phold_populate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  GPQ_CUDA_TRY(gpq::raise_smem_limit(phold_populate_kernel, (int)smem));
   const uint32_t grid = (uint32_t)((L + wpb - 1) / wpb);
   phold_populate_kernel<<<grid, wpb * 32, smem, st>>>(h->dev(), h->lq(), c.events_per_lp, src);
   GPQ_CUDA_TRY(cudaGetLastError());

@@ -140,7 +140,7 @@ gpq_status finish_create(gpq_phold_session* s, uint32_t max_instances) {
     return e == cudaErrorMemoryAllocation ? GPQ_ERR_NOMEM : GPQ_ERR_CUDA;
   }
   int dev = 0, sms = 0, per_sm = 0;
-  GPQ_CUDA_TRY(cudaFuncSetAttribute(s->kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem));
+  GPQ_CUDA_TRY(gpq::raise_smem_limit(s->kern, (int)s->smem));
   GPQ_CUDA_TRY(cudaGetDevice(&dev));
   GPQ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   GPQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, s->kern, (int)s->block, s->smem));
@@ -181,7 +181,7 @@ gpq_status flush_pending(gpq_phold_session* s, cudaStream_t st) {
   }
   const uint32_t block = 256, wpb = block / 32;
   const size_t smem = (size_t)wpb * max_p * (sizeof(gpq_item) + sizeof(uint64_t));
-  GPQ_CUDA_TRY(cudaFuncSetAttribute(pm_populate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  GPQ_CUDA_TRY(gpq::raise_smem_limit(pm_populate_kernel, (int)smem));
   for (uint32_t j0 = 0; j0 < n; j0 += 65535) {
     const uint32_t nj = std::min<uint32_t>(65535, n - j0);
     const uint32_t gx = std::min<uint32_t>((max_lps + wpb - 1) / wpb, 1024);

@@ -12,8 +12,12 @@
 //
 // Set-up: the first call on a device, with that device current, looks up the array's
 // device address with cudaGetSymbolAddress (host code only ever sees a host-side
-// stand-in for the symbol, which must not be handed to a kernel) and sets the kernels'
-// shared-memory limits.  Make that first call before any stream capture.
+// stand-in for the symbol, which must not be handed to a kernel) and caches it for that
+// device.  Make that first call before any stream capture.  The cached address does not
+// survive cudaDeviceReset: a process that resets a device must not call this entry point
+// on it afterwards.  Every call raises (never lowers) the shared-memory limits of the
+// kernels it launches to what this configuration needs, so it neither breaks nor is
+// broken by handles created before or after it.
 //
 // Every call shares the one array and leaves its last contents there: each call clears
 // the parts that must start at zero (control block, insert counters) itself.  Calls
@@ -56,7 +60,7 @@ StaticLayout layout_for(const gpq_phold_config& c) {
   return s;
 }
 
-// Once per device: device address of the scratch array and kernel attributes.
+// Once per device: device address of the scratch array.
 gpq_status scratch_for_current_device(unsigned char** out) {
   int dev = 0;
   GPQ_CUDA_TRY(cudaGetDevice(&dev));
@@ -72,12 +76,6 @@ gpq_status scratch_for_current_device(unsigned char** out) {
       gpq::set_last_error("cudaGetSymbolAddress(scratch) -> %s", cudaGetErrorString(e));
       return GPQ_ERR_CUDA;
     }
-    for (uint32_t grp : {4u, 8u, 16u, 32u}) {
-      PholdKernelSet ks;
-      phold_kernel_set(GPQ_QUEUE_LAQ, grp, 64, &ks);
-      GPQ_CUDA_TRY(cudaFuncSetAttribute(ks.persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
-    }
-    GPQ_CUDA_TRY(cudaFuncSetAttribute(phold_populate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     g_scratch_dev[dev] = static_cast<unsigned char*>(p);
   }
   *out = g_scratch_dev[dev];
@@ -111,6 +109,11 @@ extern "C" gpq_status gpq_phold_run_static(const gpq_phold_config* cfg_in, const
     gpq::set_last_error("gpq_phold_run_static supports the local array queue only");
     return GPQ_ERR_UNSUPPORTED;
   }
+  if (c.laq_mode != 0) {
+    gpq::set_last_error("gpq_phold_run_static supports the sorted local array queue only (laq_mode 0, not %u)",
+                        c.laq_mode);
+    return GPQ_ERR_UNSUPPORTED;
+  }
   st = gpq::normalize_laq_config(&c);
   if (st != GPQ_OK) return st;
   const StaticLayout lay = layout_for(c);
@@ -134,6 +137,8 @@ extern "C" gpq_status gpq_phold_run_static(const gpq_phold_config* cfg_in, const
   unsigned char* base = nullptr;
   st = scratch_for_current_device(&base);
   if (st != GPQ_OK) return st;
+  GPQ_CUDA_TRY(gpq::raise_smem_limit(ks.persistent, win_smem));
+  GPQ_CUDA_TRY(gpq::raise_smem_limit(phold_populate_kernel, pop_smem));
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   int dev = 0, sms = 0;
   GPQ_CUDA_TRY(cudaGetDevice(&dev));
@@ -197,5 +202,8 @@ extern "C" gpq_status gpq_phold_run_static(const gpq_phold_config* cfg_in, const
   out->final_min = gpq_u2f(ha.pending_min);
   out->elapsed_ms = 0.f;
   out->status = (int32_t)hc.err;
+  if (hc.err != 0)
+    gpq::set_last_error("gpq_phold_run_static: the device reported %s (status %u) at window %u",
+                        gpq_status_string((gpq_status)hc.err), hc.err, hc.steps);
   return (gpq_status)hc.err;
 }

@@ -278,11 +278,13 @@ GPQ_API gpq_status gpq_phold_launch_info(gpq_phold* h, uint32_t* grid, uint32_t*
  *   d_count, d_csum, d_ohash  DEVICE arrays of num_lps entries, overwritten with the
  *              per-LP results (as gpq_phold_lp_stats);
  *   out        HOST result; elapsed_ms is not measured here (0).
- * Local array queue only.  A configuration whose queues need more than the fixed array
+ * Sorted local array queue only (queue_kind LAQ, laq_mode 0; anything else returns
+ * GPQ_ERR_UNSUPPORTED).  A configuration whose queues need more than the fixed array
  * (about 1024 LPs at capacity 256 and insert capacity 64 use 6.3 MiB) is rejected with
  * GPQ_ERR_INVALID and a message naming the size.  The first call on a device (with that
- * device current) looks up the array's device address; make that first call before any
- * stream capture.  All calls share the array and each call re-initializes what it needs:
+ * device current) looks up the array's device address and caches it; make that first
+ * call before any stream capture, and do not call this entry point on a device after a
+ * cudaDeviceReset of it (the cached address would be stale).  All calls share the array and each call re-initializes what it needs:
  * calls that overlap on the GPU race with each other -- serialize them.  Blocks on
  * `stream` (NULL = the legacy default stream). */
 #define GPQ_STATIC_SCRATCH_BYTES (16u * 1024u * 1024u)

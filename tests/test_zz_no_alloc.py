@@ -74,6 +74,38 @@ def test_static_entry_point_matches_allocating_path(gpu_lib):
     assert want_a[0]["committed"] == 820705
 
 
+@pytest.mark.gpu
+def test_static_entry_point_and_handles_interleaved(gpu_lib):
+    """Handles created before and after a static call keep working, and so does the static
+    call: the shared-memory limits of the kernels they share are only ever raised."""
+    want_a = _reference_path(CFG_A)
+    # a handle with a large window (insert capacity 128) exists across a static call
+    big = dict(CFG_A, insert_capacity=128)
+    with G.Phold(G.make_phold_config(**big, loop="persistent")) as h:
+        h.populate()
+        _same(_static_path(CFG_A), want_a)
+        h.run()
+        r, s = h.result(), h.lp_stats()
+    _same((r, s), want_a)
+    # a handle with a small window and few events per LP, then the static call again
+    small = dict(CFG_B, insert_capacity=8, events_per_lp=2)
+    with G.Phold(G.make_phold_config(**small, loop="persistent")) as h:
+        h.populate()
+        h.run()
+        assert h.result()["status_code"] == 0
+    _same(_static_path(CFG_A), want_a)
+
+
+def test_static_entry_point_rejects_other_queue_forms():
+    for mode in (1, 2):
+        cfg = G.make_phold_config(**CFG_A, laq_mode=mode)
+        res = G.PholdResult()
+        st = G.lib().gpq_phold_run_static(ctypes.byref(cfg), None, ctypes.c_void_p(16), ctypes.c_void_p(16),
+                                          ctypes.c_void_p(16), ctypes.byref(res), None)
+        assert st == 7  # GPQ_ERR_UNSUPPORTED, before any device work
+        assert "laq_mode" in G.last_error()
+
+
 def test_static_entry_point_rejects_oversized_config():
     cfg = G.make_phold_config(num_lps=65536, events_per_lp=64, lookahead=0.1, end_time=10.0, seed=7)
     res = G.PholdResult()
