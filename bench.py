@@ -111,6 +111,35 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def cpu_model():
+    """The host CPU's model name (lscpu / /proc/cpuinfo)."""
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for ln in fh:
+                if ln.lower().startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return None
+
+
+def golden(name):
+    """Oracle results committed by tests/golden/make_phold_golden.py (None if absent)."""
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "phold_golden.json")) as fh:
+            return json.load(fh).get(name)
+    except Exception:
+        return None
+
+
+def matches_golden(O, g, r, s):
+    """A run's result and per-LP outputs equal the committed oracle results, bit for bit."""
+    return (g is not None and r["committed"] == g["committed"] and r["steps"] == g["windows"]
+            and r["pending"] == g["pending"] and r["pending_csum"] == int(g["pending_csum"])
+            and r["digest"] == int(g["digest"])
+            and O.lp_sha256(s["count"], s["csum"], s["ohash"]) == g["lp_sha256"])
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -164,7 +193,8 @@ def run_reference(args):
         "warmup": args.warmup, "ms_per_step": 1e3 * committed / v, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD_NAME, "queue": "per-LP std::priority_queue (CPU)", "sample_end_time": CPU_SAMPLE_END},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
+                         "cpu_model": cpu_model()},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -216,7 +246,8 @@ def bench_astar_plain(G, O, args, peak):
             "roofline": {"bound": "latency (critical path of ~4100 dependent expansions)", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak},
             "cpu_baseline": {"value": want["expanded"] / want["seconds"], "unit": "expansions/s", "cores": 1,
-                             "kind": "port", "sample": "the whole query, sequential std::priority_queue A*"}}
+                             "kind": "port", "sample": "the whole query, sequential std::priority_queue A*",
+                             "cpu_model": cpu_model()}}
 
 
 def bench_astar_batched(G, O, args, peak):
@@ -237,23 +268,101 @@ def bench_astar_batched(G, O, args, peak):
             r = a.solve(q[i:i + 1])
             pe += int(r[0]["expanded"])
             pt += a.stats()["total_ms"] / 1e3
-    sample = [{k: int(q[i][k]) for k in O.ASTAR_FIELDS} for i in range(300)]
+    # every query against the sequential oracle (all host threads, outside the timing)
+    allq = [{k: int(q[i][k]) for k in O.ASTAR_FIELDS} for i in range(len(q))]
     threads = os.cpu_count() or 1
-    sec, res = O.astar_batch(sample, threads)
-    exact = all(int(out[0][0][i][k]) == res[i][k] for i in range(300)
-                for k in ("cost", "expanded", "gsum", "path_len", "path_hash"))
+    sec_all, res_all = O.astar_batch(allq, threads)
+    fields = ("cost", "expanded", "gsum", "path_len", "path_hash")
+    mism = [i for i in range(len(q)) for k in fields if int(out[0][0][i][k]) != res_all[i][k]]
+    exact = all(int(out[j][0][i][k]) == int(out[0][0][i][k]) for j in range(len(out)) for i in range(len(q))
+                for k in fields) and not mism
+    sec, res = O.astar_batch(allq[:300], threads)
     achieved = exp * ASTAR_BYTES_PER_EXPANSION[8] * args.steps / dev_s / 1e9
     return {"workload": "astar_batched_10000q_side64-1024_8conn", "metric": "A* expansions/s (batched)",
             "value": exp * args.steps / dev_s, "unit": "expansions/s", "queries": len(q),
             "ms_per_batch": 1e3 * dev_s / args.steps, "bad_status": int((out[0][0]["status"] != 0).sum()),
             "config": shape,
             "plain_value": pe / pt, "plain_sample": "first 200 queries, one launch each",
-            "batched_over_plain": (exp * args.steps / dev_s) / (pe / pt), "exact_vs_oracle_first_300": exact,
+            "batched_over_plain": (exp * args.steps / dev_s) / (pe / pt), "exact_vs_oracle": exact,
+            "exact_checked": f"all {len(q)} queries of every timed batch against the sequential oracle "
+                             f"({sec_all:.1f} s on {threads} host threads); mismatches {len(set(mism))}",
             "e2e": {"value": exp * args.steps / wall, "unit": "expansions/s",
                     "h2d_bytes_per_step": int(q.nbytes), "d2h_bytes_per_step": int(len(q) * 48)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak},
             "cpu_baseline": {"value": sum(r["expanded"] for r in res) / sec, "unit": "expansions/s", "cores": threads,
-                             "kind": "port", "sample": "first 300 queries, one sequential A* per host thread"}}
+                             "kind": "port", "sample": "first 300 queries, one sequential A* per host thread",
+                             "cpu_model": cpu_model()}}
+
+
+C1 = dict(num_lps=1024, events_per_lp=16, lookahead=1.0, end_time=100.0, seed=42, dest_mode=0)
+
+
+def _phold_form(G, O, cfgd, queue, runs, warmup=1, **kw):
+    """Device-timed whole runs of one queue kind; (events/s, ms per run, windows, result,
+    per-LP stats of the first timed run)."""
+    cfg = G.make_phold_config(**cfgd, queue=queue, **kw)
+    with G.Phold(cfg) as h:
+        for _ in range(warmup):
+            h.populate()
+            h.run()
+        ev, ms, first = 0, 0.0, None
+        for _ in range(runs):
+            h.populate()
+            h.run()
+            r = h.result()
+            if first is None:
+                first = (r, h.lp_stats())
+            ev += r["committed"]
+            ms += r["elapsed_ms"]
+    return ev / (ms / 1e3), ms / runs, first
+
+
+def bench_phold_c1(G, O, args, peak):
+    """1,024 LPs x 16 events, lookahead 1.0 + Exp(1), uniform destinations, end time 100,
+    seed 42 (820,705 events in 100 windows), through the parallel heap queue -- the kind
+    the workload names -- with the four other kinds beside it; each checked against the
+    committed oracle results, bit for bit."""
+    g = golden("phold_plain_1024lp_x16_T100")
+    kinds = {}
+    for queue in ("hq", "laq", "lhq", "lsq", "gaq"):
+        v, ms, (r, st) = _phold_form(G, O, C1, queue, runs=3)
+        by = BYTES_PER_EVENT * r["committed"] + BYTES_PER_LP_WINDOW * C1["num_lps"] * r["steps"]
+        kinds[queue] = {"value": v, "ms_per_run": ms, "exact_vs_oracle": matches_golden(O, g, r, st),
+                        "roofline_frac": by / (ms / 1e3) / 1e9 / peak}
+    cpu = []
+    for _ in range(5):  # one thread, median of 5 (the sequential oracle, the whole run)
+        o = O.phold(O.make_cfg(**C1), 0)
+        cpu.append(o["committed"] / o["seconds"])
+    hq = kinds["hq"]
+    achieved = hq["roofline_frac"] * peak
+    return {"workload": "phold_plain_1024lp_x16_T100_heap_queue", "metric": "PHOLD committed events/s",
+            "value": hq["value"], "unit": "events/s", "events_per_run": g["committed"] if g else None,
+            "windows_per_run": g["windows"] if g else None, "exact_vs_oracle": hq["exact_vs_oracle"],
+            "kinds": kinds, "timing": "device time of whole runs (CUDA events), 3 runs after 1 warm-up",
+            "roofline": {"bound": "latency (0.3 MB working set, L2-resident)", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": hq["roofline_frac"]},
+            "cpu_baseline": {"value": statistics.median(cpu), "unit": "events/s", "cores": 1, "kind": "port",
+                             "sample": "the whole run, sequential std::priority_queue oracle, median of 5",
+                             "cpu_model": cpu_model()}}
+
+
+def bench_phold_c2_gaq(G, O, args, peak):
+    """The 65,536-LP ring workload to end time 1000 through the global array queue (one
+    sorted array for all LPs; each window's children radix-sorted and merged in), checked
+    against the committed oracle results."""
+    name = "phold_large_65536lp_x64_ring16_T1000"
+    g = golden(name)
+    cfgd = {k: WORKLOAD[k] for k in ("num_lps", "events_per_lp", "lookahead", "end_time", "seed", "dest_mode",
+                                     "ring_width")}
+    v, ms, (r, st) = _phold_form(G, O, cfgd, "gaq", runs=2, capacity=256)
+    by = BYTES_PER_EVENT * r["committed"] + BYTES_PER_LP_WINDOW * cfgd["num_lps"] * r["steps"]
+    achieved = by / (ms / 1e3) / 1e9
+    return {"workload": name + "_global_array_queue", "metric": "PHOLD committed events/s", "value": v,
+            "unit": "events/s", "ms_per_run": ms, "windows_per_run": r["steps"],
+            "exact_vs_oracle": matches_golden(O, g, r, st),
+            "timing": "device time of whole runs (CUDA events), 2 runs after 1 warm-up",
+            "roofline": {"bound": "launch (24 dependent kernels per window, replayed as a CUDA graph)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak}}
 
 
 def bench_phold_batched(G, O, args, peak):
@@ -466,15 +575,22 @@ def main():
     def sum_over_ranks(x):
         return reduce_over_ranks(dist, x, "sum", "cuda")
 
-    # warm-up
+    # warm-up; the first run is checked against the committed oracle results when the
+    # workload is the one they were made for (seed 7: rank 0)
     ref_digest = None
-    for _ in range(args.warmup):
+    exact_vs_oracle = None
+    for i in range(args.warmup):
         h.populate()
         h.run()
         r = h.result()
         if r["status_code"] != 0:
             raise SystemExit(f"run failed: {r}")
         ref_digest = (r["digest"], r["committed"])
+        if i == 0:
+            g = golden(WORKLOAD_NAME)
+            if g is not None and all(g["config"][k] == cfgd[k] for k in g["config"]):
+                from oracle import oracle as O
+                exact_vs_oracle = matches_golden(O, g, r, h.lp_stats())
 
     barrier()
     sampler = ClockSampler(local if ws > 1 else 0)
@@ -554,14 +670,19 @@ def main():
         rr = cpu_reference_run(WORKLOAD, CPU_SAMPLE_END, threads)
         cpu = {"value": rr["committed"] / rr["seconds"], "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"end_time {CPU_SAMPLE_END} of 1000 ({rr['committed']} events); window-synchronous per-LP "
-                         f"std::priority_queue port of the reference loop on {threads} threads"}
+                         f"std::priority_queue port of the reference loop on {threads} threads; the live "
+                         f"population is constant (every event makes one child), so the per-event cost of "
+                         f"the sample stands for the whole run",
+               "cpu_model": cpu_model()}
 
     h.close()
     forms = None
     if rank == 0 and not args.no_forms:
         from oracle import oracle as O
         peak, _ = load_peaks()
-        forms = {"astar_plain": bench_astar_plain(G, O, args, peak),
+        forms = {"phold_c1": bench_phold_c1(G, O, args, peak),
+                 "phold_c2_gaq": bench_phold_c2_gaq(G, O, args, peak),
+                 "astar_plain": bench_astar_plain(G, O, args, peak),
                  "astar_batched": bench_astar_batched(G, O, args, peak),
                  "phold_batched": bench_phold_batched(G, O, args, peak),
                  "served": bench_served(G, args, args.served_seconds)}
@@ -583,6 +704,7 @@ def main():
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": f"{peak_kind} hbm_gbs", "kernel": ("lab_" if laq_mode == 2 else "phold_laq_") + args.loop,
                          "algorithmic_bytes_per_run": per_run_bytes},
+            "exact_vs_oracle": exact_vs_oracle,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(args.steps * info["launches_per_run"]),

@@ -62,6 +62,10 @@ def lib():
                                           ctypes.POINTER(OraclePholdSummary)]
         _LIB.oracle_phold_window.argtypes = [ctypes.POINTER(OraclePholdCfg), ctypes.c_int, u32p, u64p,
                                              u64p, ctypes.POINTER(OraclePholdSummary)]
+        _LIB.oracle_phold_one_per_lp.argtypes = [ctypes.POINTER(OraclePholdCfg), u32p, u64p, u64p,
+                                                 ctypes.POINTER(OraclePholdSummary)]
+        _LIB.oracle_phold_digest.argtypes = [ctypes.c_uint32, u32p, u64p, u64p]
+        _LIB.oracle_phold_digest.restype = ctypes.c_uint64
         _LIB.oracle_phold_child.argtypes = [ctypes.POINTER(OraclePholdCfg), f32p, u32p, u32p,
                                             ctypes.c_uint64, f32p, u32p]
         _LIB.oracle_phold_initial.argtypes = [ctypes.POINTER(OraclePholdCfg), f32p, u32p, u32p]
@@ -102,14 +106,18 @@ def make_cfg(num_lps, events_per_lp, lookahead, end_time, seed, dest_mode=0, rin
     return c
 
 
-def phold(cfg, threads=0):
-    """Run the oracle. threads=0: sequential global priority queue; >=1: windowed per-LP driver."""
+def phold(cfg, threads=0, one_per_lp=False):
+    """Run the oracle. threads=0: sequential global priority queue; >=1: windowed per-LP
+    driver; one_per_lp: the reference's schedule (one event per LP per window; its window
+    count is the reference loop's)."""
     L = cfg.num_lps
     count = np.zeros(L, np.uint32)
     csum = np.zeros(L, np.uint64)
     ohash = np.zeros(L, np.uint64)
     s = OraclePholdSummary()
-    if threads == 0:
+    if one_per_lp:
+        rc = lib().oracle_phold_one_per_lp(ctypes.byref(cfg), count, csum, ohash, ctypes.byref(s))
+    elif threads == 0:
         rc = lib().oracle_phold_seq(ctypes.byref(cfg), count, csum, ohash, ctypes.byref(s))
     else:
         rc = lib().oracle_phold_window(ctypes.byref(cfg), threads, count, csum, ohash, ctypes.byref(s))
@@ -119,7 +127,25 @@ def phold(cfg, threads=0):
         "count": count, "csum": csum, "ohash": ohash,
         "committed": int(s.committed), "steps": int(s.steps), "pending": int(s.pending),
         "pending_csum": int(s.pending_csum), "seconds": float(s.seconds),
+        "digest": digest(count, csum, ohash),
     }
+
+
+def digest(count, csum, ohash):
+    """The GPU engine's order-sensitive digest over per-LP outputs."""
+    count = np.ascontiguousarray(count, np.uint32)
+    csum = np.ascontiguousarray(csum, np.uint64)
+    ohash = np.ascontiguousarray(ohash, np.uint64)
+    return int(lib().oracle_phold_digest(len(count), count, csum, ohash))
+
+
+def lp_sha256(count, csum, ohash):
+    """sha256 over the per-LP arrays (count u32, csum u64, ohash u64; little endian)."""
+    import hashlib
+    h = hashlib.sha256()
+    for a, dt in ((count, "<u4"), (csum, "<u8"), (ohash, "<u8")):
+        h.update(np.ascontiguousarray(a).astype(dt).tobytes())
+    return h.hexdigest()
 
 
 def child(cfg, ts, lp, ids):

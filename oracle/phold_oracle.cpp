@@ -16,11 +16,16 @@
 // cross-check each other.  Parity for the ring helpers is pinned by the reference's
 // own known-answer tests (src/test_laq.cu:39-236), see oracle_ring_* below.
 //
-// Two drivers produce identical outputs:
+// Three drivers produce identical per-LP outputs:
 //   oracle_phold_seq     one global std::priority_queue, events popped in key order;
 //   oracle_phold_window  one std::priority_queue per LP, LPs split over host threads,
 //                        window-synchronous steps (the reference's loop run on CPU cores;
-//                        used as the timed CPU baseline).
+//                        used as the timed CPU baseline);
+//   oracle_phold_one_per_lp  the reference's own schedule: every window handles at most
+//                        ONE event per LP (src/phold.cu:84-94 peeks one item per LP per
+//                        call; src/local_array_queue.cu:760-779), so it takes more windows;
+//                        its window count is what the reference's loop reports.
+// The first two count windows in which every LP drains all of its safe events.
 // Build: g++ -O2 -std=c++20 -ffp-contract=off -fPIC -shared (see oracle/build.py).
 
 #include <algorithm>
@@ -327,6 +332,66 @@ int oracle_phold_window(const oracle_phold_cfg* cfg, int nthreads, uint32_t* cou
   out->pending_csum = pcs;
   out->seconds = std::chrono::duration<double>(t1 - t0).count();
   return 0;
+}
+
+// The reference's schedule (src/des.cu:154-214 with src/phold.cu:81-117): each window
+// m = minimum pending timestamp; the loop stops when m >= T; every LP whose earliest event
+// e has e.ts < m + lookahead and e.ts < T handles that ONE event; the children enter the
+// queues after the window (queue_post).  Sequential; meant for small and medium sizes.
+int oracle_phold_one_per_lp(const oracle_phold_cfg* cfg, uint32_t* count, uint64_t* csum, uint64_t* ohash,
+                            oracle_phold_summary* out) {
+  if (!cfg || !count || !csum || !ohash || !out || cfg->num_lps == 0) return 1;
+  Model m{*cfg};
+  const uint32_t L = cfg->num_lps;
+  std::memset(count, 0, sizeof(uint32_t) * L);
+  std::memset(csum, 0, sizeof(uint64_t) * L);
+  std::memset(ohash, 0, sizeof(uint64_t) * L);
+  LpOut o{count, csum, ohash};
+  std::vector<MinHeap> q(L);
+  for (uint32_t lp = 0; lp < L; ++lp)
+    for (uint32_t k = 0; k < cfg->events_per_lp; ++k) q[lp].push(m.initial(lp, k));
+  const float inf = ffrom(0x7f800000u), T = cfg->end_time;
+  std::vector<Ev> children;
+  auto t0 = std::chrono::steady_clock::now();
+  uint64_t committed = 0, steps = 0;
+  for (;;) {
+    float mn = inf;
+    for (uint32_t lp = 0; lp < L; ++lp)
+      if (!q[lp].empty()) mn = std::min(mn, q[lp].top().ts);
+    if (!(mn < T)) break;
+    ++steps;
+    const float bound = mn + cfg->lookahead;
+    children.clear();
+    for (uint32_t lp = 0; lp < L; ++lp) {
+      if (q[lp].empty()) continue;
+      const Ev e = q[lp].top();
+      if (!(e.ts < bound) || !(e.ts < T)) continue;
+      q[lp].pop();
+      o.commit(e);
+      ++committed;
+      children.push_back(m.child(e));
+    }
+    for (const Ev& c : children) q[c.lp].push(c);
+  }
+  auto t1 = std::chrono::steady_clock::now();
+  uint64_t pend = 0, pcs = 0;
+  for (uint32_t lp = 0; lp < L; ++lp)
+    while (!q[lp].empty()) { pcs += ev_hash(q[lp].top()); ++pend; q[lp].pop(); }
+  out->committed = committed;
+  out->steps = steps;
+  out->pending = pend;
+  out->pending_csum = pcs;
+  out->seconds = std::chrono::duration<double>(t1 - t0).count();
+  return 0;
+}
+
+// Order-sensitive digest over the per-LP outputs, as the GPU engine reports it:
+// sum over LPs of mix(mix(mix(lp << 32 | count) ^ csum) + ohash).
+uint64_t oracle_phold_digest(uint32_t num_lps, const uint32_t* count, const uint64_t* csum, const uint64_t* ohash) {
+  uint64_t d = 0;
+  for (uint32_t lp = 0; lp < num_lps; ++lp)
+    d += mix(mix(mix(((uint64_t)lp << 32) | count[lp]) ^ csum[lp]) + ohash[lp]);
+  return d;
 }
 
 // The PHOLD child and the initial events as seen by the oracle (for spot checks of the

@@ -12,28 +12,7 @@
 #include "gpq.h"
 #include "gpq/queue.cuh"
 
-namespace {
-
-__global__ void handle_next_event(gpq_phold_params p, uint32_t L, uint32_t* num_events, unsigned long long* csum,
-                                  unsigned long long* ohash) {
-  for (uint32_t idx = threadIdx.x + blockDim.x * blockIdx.x; idx < L; idx += blockDim.x * gridDim.x) {
-    queue_item* ev = NULL;
-    const int event_index = queue_peek(&ev, (int)idx);
-    if (event_index != -1) {
-      const uint32_t lp = ev->lp;
-      const uint64_t h = gpq_ev_hash(ev->id, gpq_f2u(ev->ts));
-      csum[lp] += h;
-      ohash[lp] += gpq_seq_hash(h, num_events[lp]);
-      num_events[lp]++;
-      const gpq_item child = gpq_phold_child(p, *ev);
-      queue_set_done(event_index);
-      const bool result = queue_insert(child);
-      (void)result;  // a full buffer is reported by the next gpq_queue_post
-    }
-  }
-}
-
-}  // namespace
+#include "phold_handler.cuh"
 
 // Runs the model; per-LP outputs to host arrays of cfg->num_lps.  Returns 0 or a
 // gpq_status.
@@ -42,7 +21,7 @@ extern "C" int dropin_phold_run(const gpq_phold_config* cfg, uint32_t* count, un
                                 unsigned long long* committed_out) {
   const uint32_t L = cfg->num_lps;
   gpq_queue_config qc = {};
-  qc.kind = cfg->queue_kind;  // a local array queue or a local heap queue
+  qc.kind = cfg->queue_kind;  // any queue kind
   qc.num_lps = L;
   qc.capacity = cfg->capacity ? cfg->capacity : 256;
   qc.insert_capacity = cfg->insert_capacity ? cfg->insert_capacity : 64;
@@ -62,14 +41,7 @@ extern "C" int dropin_phold_run(const gpq_phold_config* cfg, uint32_t* count, un
   cudaMemset(d_count, 0, L * sizeof(uint32_t));
   cudaMemset(d_csum, 0, L * sizeof(unsigned long long));
   cudaMemset(d_ohash, 0, L * sizeof(unsigned long long));
-  gpq_phold_params p = {};
-  p.seed = cfg->seed;
-  p.num_lps = L;
-  p.dest_mode = cfg->dest_mode;
-  p.ring_width = cfg->ring_width;
-  p.ring_threshold = cfg->ring_threshold;
-  p.lookahead = cfg->lookahead;
-  p.end_time = cfg->end_time;
+  const gpq_phold_params p = dropin_params(cfg);
   unsigned long long steps = 0;
   while (!st) {
     float m = 0.f;
