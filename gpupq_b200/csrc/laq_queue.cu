@@ -90,6 +90,7 @@ class LaqQueue final : public LocalQueueBase {
   }
 
   gpq_status device_view(gpq_device_queue* v) override {
+    *v = gpq_device_queue{};
     v->ring = ring_;
     v->rd = rd_;
     v->wr = wr_;

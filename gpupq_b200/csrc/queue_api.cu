@@ -21,6 +21,7 @@ gpq_status gpq_queue_create(const gpq_queue_config* cfg, gpq_queue** out) {
   gpq_queue* q = new (std::nothrow) gpq_queue();
   if (!q) return GPQ_ERR_NOMEM;
   q->impl = std::move(impl);
+  q->cfg = *cfg;
   *out = q;
   return GPQ_OK;
 }
@@ -44,13 +45,15 @@ gpq_status gpq_queue_pre(gpq_queue* q, void* stream) {
 
 gpq_status gpq_queue_post(gpq_queue* q, void* stream) {
   GPQ_CHECK_ARG(q, "NULL queue");
-  return q->impl->post(gpq::as_stream(stream, q->impl->stream()));
+  const cudaStream_t st = gpq::as_stream(stream, q->impl->stream());
+  if (q->staged) {
+    const gpq_status s = q->staged->flush(q->impl.get(), st);
+    if (s != GPQ_OK) return s;
+  }
+  return q->impl->post(st);
 }
 
-gpq_status gpq_queue_post_init(gpq_queue* q, void* stream) {
-  GPQ_CHECK_ARG(q, "NULL queue");
-  return q->impl->post(gpq::as_stream(stream, q->impl->stream()));
-}
+gpq_status gpq_queue_post_init(gpq_queue* q, void* stream) { return gpq_queue_post(q, stream); }
 
 gpq_status gpq_queue_get_min(gpq_queue* q, float* min_ts, void* stream) {
   GPQ_CHECK_ARG(q && min_ts, "NULL argument");
@@ -84,20 +87,38 @@ gpq_status gpq_queue_dump(gpq_queue* q, uint32_t lp, gpq_item* out, uint64_t out
 
 gpq_status gpq_queue_counts(gpq_queue* q, uint64_t* enqueued, uint64_t* dequeued, void* stream) {
   GPQ_CHECK_ARG(q && enqueued && dequeued, "NULL argument");
-  return q->impl->counts(enqueued, dequeued, gpq::as_stream(stream, q->impl->stream()));
+  const gpq_status s = q->impl->counts(enqueued, dequeued, gpq::as_stream(stream, q->impl->stream()));
+  if (s == GPQ_OK && q->staged) {  // heads staged and given back untouched are neither
+    *enqueued -= q->staged->restaged();
+    *dequeued -= q->staged->restaged();
+  }
+  return s;
 }
 
 gpq_status gpq_queue_device_view(gpq_queue* q, gpq_device_queue* out) {
   GPQ_CHECK_ARG(q && out, "NULL argument");
+  if (q->staged) {
+    q->staged->fill(out, q->cfg.kind);
+    return GPQ_OK;
+  }
   const gpq_status s = q->impl->device_view(out);
-  if (s == GPQ_ERR_UNSUPPORTED) gpq::set_last_error("device-side access is available for the local array queue only");
-  return s;
+  if (s != GPQ_ERR_UNSUPPORTED) return s;
+  std::unique_ptr<gpq::StagedView> v(new (std::nothrow) gpq::StagedView());
+  if (!v) return GPQ_ERR_NOMEM;
+  const gpq_status si = v->init(q->impl->num_lps(), q->cfg.insert_capacity, q->impl->stream());
+  if (si != GPQ_OK) return si;
+  q->staged = std::move(v);
+  q->staged->fill(out, q->cfg.kind);
+  return GPQ_OK;
 }
 
 gpq_status gpq_queue_set_bound(gpq_queue* q, float bound, void* stream) {
   GPQ_CHECK_ARG(q, "NULL argument");
-  const gpq_status s = q->impl->set_bound(bound, gpq::as_stream(stream, q->impl->stream()));
-  if (s == GPQ_ERR_UNSUPPORTED) gpq::set_last_error("device-side access is available for the local array queue only");
+  const cudaStream_t st = gpq::as_stream(stream, q->impl->stream());
+  if (q->staged) return q->staged->set_bound(q->impl.get(), bound, st);
+  const gpq_status s = q->impl->set_bound(bound, st);
+  if (s == GPQ_ERR_UNSUPPORTED)
+    gpq::set_last_error("gpq_queue_set_bound: take the device view (gpq_queue_device_view) of this queue first");
   return s;
 }
 

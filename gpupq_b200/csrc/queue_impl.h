@@ -8,6 +8,7 @@
 #include <memory>
 
 #include "gpq.h"
+#include "staged_view.h"
 
 namespace gpq {
 
@@ -26,7 +27,9 @@ class QueueImpl {
   virtual gpq_status clear(uint32_t lp, cudaStream_t st) = 0;
   virtual gpq_status dump(uint32_t lp, gpq_item* out, uint64_t out_capacity, uint64_t* n_out, cudaStream_t st) = 0;
   virtual gpq_status counts(uint64_t* enqueued, uint64_t* dequeued, cudaStream_t st) = 0;
-  // Device-side access for model kernels (include/gpq/queue.cuh); local array queue only.
+  // Device-side access for model kernels (include/gpq/queue.cuh) over the kind's own
+  // per-LP arrays (local array and local heap queues); the other kinds are reached through
+  // staged per-LP heads (staged_view.h).
   virtual gpq_status device_view(gpq_device_queue*) { return GPQ_ERR_UNSUPPORTED; }
   virtual gpq_status set_bound(float, cudaStream_t) { return GPQ_ERR_UNSUPPORTED; }
 };
@@ -41,4 +44,6 @@ gpq_status make_queue(const gpq_queue_config& cfg, std::unique_ptr<QueueImpl>& o
 
 struct gpq_queue {
   std::unique_ptr<gpq::QueueImpl> impl;
+  gpq_queue_config cfg{};
+  std::unique_ptr<gpq::StagedView> staged;  // device-side access for GAQ, HQ and LSQ
 };

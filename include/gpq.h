@@ -117,10 +117,18 @@ GPQ_API gpq_status gpq_queue_dump(gpq_queue* q, uint32_t lp, gpq_item* out, uint
  * removed since creation. */
 GPQ_API gpq_status gpq_queue_counts(gpq_queue* q, uint64_t* enqueued, uint64_t* dequeued, void* stream);
 
-/* Device-side access to a local array queue for model kernels: the reference's device
- * queue functions (queue_insert, queue_peek, queue_set_done, queue_is_empty,
- * queue_length, queue_clear, queue_insert_or_update; src/queue.cuh:46-70) are provided
- * as inline __device__ functions over this view by include/gpq/queue.cuh. */
+/* Device-side access to a queue for model kernels: the reference's device queue
+ * functions (queue_insert, queue_peek, queue_set_done, queue_is_empty, queue_length,
+ * queue_clear, queue_insert_or_update, queue_print; src/queue.cuh:7-70) are provided as
+ * inline __device__ functions over this view by include/gpq/queue.cuh.
+ *   local array / local heap queue: the view is the queue's own per-LP arrays;
+ *   global array / heap / local splay queue: `staged` is 1 -- gpq_queue_set_bound moves
+ *     each LP's earliest item below the bound into head[lp] (the reference's one item per
+ *     LP per step, src/global_array_queue.cu:147-179); queue_peek returns it,
+ *     queue_set_done marks it taken, and gpq_queue_post gives back the untaken heads
+ *     together with the inserted items.  queue_length, queue_is_empty and queue_clear are
+ *     not offered on the device for these kinds (the call sets GPQ_ERR_UNSUPPORTED, which
+ *     the next gpq_queue_post returns; the host functions gpq_queue_length/clear work). */
 typedef struct gpq_device_queue {
   gpq_item* ring;               /* [num_lps << cap_log2] per-LP sorted runs (LAQ) or 4-ary heaps (LHQ) */
   uint32_t* rd;                 /* LAQ: per-LP read counter (fel_read); slot = counter & (cap - 1) */
@@ -132,18 +140,38 @@ typedef struct gpq_device_queue {
   unsigned long long* dequeued; /* get_dequeue_count */
   uint32_t* err;                /* sticky error word read by the next gpq_queue_post */
   uint32_t num_lps, cap_log2, ibc;
-  uint32_t kind;                /* GPQ_QUEUE_LAQ or GPQ_QUEUE_LHQ */
+  uint32_t kind;                /* gpq_queue_kind */
   uint32_t* size;               /* LHQ: per-LP heap size (root at slot 0, children of i at 4i+1..4i+4) */
+  gpq_item* head;               /* staged kinds: [num_lps] earliest item below the bound (ts +inf: none) */
+  uint32_t* taken;              /* staged kinds: [num_lps] set by queue_set_done */
+  uint32_t staged;              /* 1 for the global array, heap and local splay queues */
 } gpq_device_queue;
 
-/* Fills *out with the device pointers of a local array queue or a local heap queue
- * (GPQ_ERR_UNSUPPORTED for the other kinds).  The view stays valid until
- * gpq_queue_destroy. */
+/* Fills *out with the device pointers of the queue's device view (allocated at the first
+ * call for the staged kinds).  The view stays valid until gpq_queue_destroy. */
 GPQ_API gpq_status gpq_queue_device_view(gpq_queue* q, gpq_device_queue* out);
 
 /* Sets the window bound queue_peek tests against (the reference's global_min + LOOKAHEAD,
- * src/local_array_queue.cu:760-779); +inf at creation.  Stream-ordered. */
+ * src/local_array_queue.cu:760-779); +inf at creation.  Stream-ordered for the local
+ * array and local heap queues; for the staged kinds it also stages the heads and blocks
+ * on the stream. */
 GPQ_API gpq_status gpq_queue_set_bound(gpq_queue* q, float bound, void* stream);
+
+/* The reference's host queue API over one library-owned queue (src/queue.h:86-115:
+ * queue_init, queue_pre, queue_post, queue_post_init, queue_get_min_ts, queue_finish,
+ * get_enqueue_count, get_dequeue_count).  include/gpq/legacy.h gives these the
+ * reference's names; gpq_legacy_configure sets what the reference's config.h fixes at
+ * compile time (the queue's kind and sizes, LOOKAHEAD, and an end time that caps the
+ * window bound; 0 = none).  Errors are kept: gpq_legacy_status returns the first. */
+GPQ_API gpq_status gpq_legacy_configure(const gpq_queue_config* cfg, float lookahead, float end_time);
+GPQ_API gpq_status gpq_legacy_init(gpq_queue** out);      /* queue_init: (re)creates the queue */
+GPQ_API gpq_queue* gpq_legacy_queue(void);                /* the queue (NULL before queue_init) */
+GPQ_API gpq_status gpq_legacy_pre(void);                  /* queue_pre: bound = min + lookahead */
+GPQ_API gpq_status gpq_legacy_post(void);                 /* queue_post / queue_post_init */
+GPQ_API float gpq_legacy_get_min_ts(void);                /* queue_get_min_ts (cached until post) */
+GPQ_API gpq_status gpq_legacy_counts(uint64_t* enqueued, uint64_t* dequeued);
+GPQ_API gpq_status gpq_legacy_finish(void);               /* queue_finish */
+GPQ_API gpq_status gpq_legacy_status(void);               /* first error since queue_init */
 
 /* ---------------------------------------------------------------------------------- */
 /* 2. PHOLD engine                                                                    */

@@ -1,23 +1,30 @@
 /*
- * gpq/queue.cuh -- the reference's device queue functions for model kernels, over a
- * gpupq_b200 local array queue or local heap queue.
+ * gpq/queue.cuh -- the reference's device queue functions for model kernels, over any
+ * gpupq_b200 queue kind.
  *
  * The reference binds queue_insert / queue_peek / queue_set_done / queue_is_empty /
- * queue_length / queue_clear / queue_insert_or_update to one queue implementation by
- * macro (src/queue.cuh:7-70) and model kernels call them per LP (PHOLD:
+ * queue_length / queue_clear / queue_insert_or_update / queue_print to one queue
+ * implementation by macro (src/queue.cuh:7-70) and model kernels call them per LP (PHOLD:
  * src/phold.cu:81-117).  Including this header in a CUDA translation unit gives those
- * names as inline __device__ functions over the device view of a gpq_queue (local array
- * queue: the head of the LP's sorted run; local heap queue: the root of the LP's 4-ary
- * heap, src/local_heap_queue.cu), so a handler written like the reference's compiles
- * against the library:
+ * names as inline __device__ functions (queue_print as a __global__) over the device view
+ * of a gpq_queue, so a handler written like the reference's compiles against the library:
  *
  *     gpq_item* ev = NULL;
- *     int index = queue_peek(&ev, lp);          // head of lp's run if ts < the window bound
+ *     int index = queue_peek(&ev, lp);          // lp's earliest item if ts < the window bound
  *     if (index != -1) {
  *       gpq_item child = ...;                  // the model's event function
  *       queue_set_done(index);
  *       bool ok = queue_insert(child);         // visible after the next gpq_queue_post
  *     }
+ *
+ * Views by kind:
+ *   local array queue  the head of the LP's sorted run (src/local_array_queue.cu:760-779);
+ *   local heap queue   the root of the LP's 4-ary heap (src/local_heap_queue.cu:430-447);
+ *   global array, heap and local splay queues: the LP's head staged by
+ *                      gpq_queue_set_bound (the reference's one item per LP per step,
+ *                      src/global_array_queue.cu:147-179); queue_length, queue_is_empty
+ *                      and queue_clear are host calls for these kinds (on the device
+ *                      they set GPQ_ERR_UNSUPPORTED, which the next gpq_queue_post returns).
  *
  * The host binds a queue once (gpq_queue_bind, below: it copies the view into this
  * translation unit's __device__ variable), then per step sets the window
@@ -33,6 +40,7 @@
 #define GPQ_QUEUE_CUH
 
 #include <cuda_runtime.h>
+#include <stdio.h>
 
 #include "gpq.h"
 
@@ -91,6 +99,12 @@ static __device__ __forceinline__ void gpq_heap4_pop(queue_item* h, uint32_t n) 
  * the window (ts < bound), else -1; *item points at it until queue_set_done/post. */
 static __device__ __forceinline__ int queue_peek(queue_item** item, int lp) {
   const gpq_device_queue& q = gpq_bound_queue;
+  if (q.staged) {
+    queue_item* it = q.head + lp;
+    if (q.taken[lp] || !(it->ts < *q.bound)) return -1;
+    *item = it;
+    return lp;
+  }
   if (q.kind == GPQ_QUEUE_LHQ) {
     if (q.size[lp] == 0u) return -1;
     queue_item* it = q.ring + ((size_t)lp << q.cap_log2);
@@ -110,6 +124,10 @@ static __device__ __forceinline__ int queue_peek(queue_item** item, int lp) {
 /* queue_set_done (src/queue.cuh:53-54): the peeked item leaves lp's run. */
 static __device__ __forceinline__ void queue_set_done(int index) {
   const gpq_device_queue& q = gpq_bound_queue;
+  if (q.staged) {
+    q.taken[index] = 1u;
+    return;
+  }
   const uint32_t lp = (uint32_t)index >> q.cap_log2;
   if (q.kind == GPQ_QUEUE_LHQ) {
     const uint32_t n = q.size[lp];
@@ -123,8 +141,15 @@ static __device__ __forceinline__ void queue_set_done(int index) {
 
 /* queue_is_empty (src/queue.cuh:59-60): nothing queued and nothing inserted since the
  * last post (src/local_array_queue.cu:807-810). */
+static __device__ __forceinline__ bool gpq_device_call_unsupported(const gpq_device_queue& q) {
+  if (!q.staged) return false;
+  atomicCAS(q.err, 0u, (uint32_t)GPQ_ERR_UNSUPPORTED);
+  return true;
+}
+
 static __device__ __forceinline__ bool queue_is_empty(int lp) {
   const gpq_device_queue& q = gpq_bound_queue;
+  if (gpq_device_call_unsupported(q)) return false;
   const bool none = q.kind == GPQ_QUEUE_LHQ ? q.size[lp] == 0u : q.rd[lp] == q.wr[lp];
   return none && q.icnt[lp] == 0u;
 }
@@ -132,12 +157,14 @@ static __device__ __forceinline__ bool queue_is_empty(int lp) {
 /* queue_length (src/queue.cuh:62-63): items in lp's run or heap. */
 static __device__ __forceinline__ int queue_length(int lp) {
   const gpq_device_queue& q = gpq_bound_queue;
+  if (gpq_device_call_unsupported(q)) return -1;
   return q.kind == GPQ_QUEUE_LHQ ? (int)q.size[lp] : (int)(q.wr[lp] - q.rd[lp]);
 }
 
 /* queue_clear (src/queue.cuh:65-66): drop lp's run. */
 static __device__ __forceinline__ void queue_clear(int lp) {
   const gpq_device_queue& q = gpq_bound_queue;
+  if (gpq_device_call_unsupported(q)) return;
   uint32_t n;
   if (q.kind == GPQ_QUEUE_LHQ) {
     n = q.size[lp];
@@ -153,6 +180,27 @@ static __device__ __forceinline__ void queue_clear(int lp) {
 static __device__ __forceinline__ void queue_insert_or_update(queue_item item, int lp) {
   item.lp = (uint32_t)lp;
   queue_insert(item);
+}
+
+/* queue_print (src/queue.cuh:56-57, a __global__ as in the reference): prints lp's items
+ * in key order (local array queue: its run; local heap queue: its heap in array order;
+ * staged kinds: the staged head -- gpq_queue_dump lists every item of any kind). */
+static __global__ void queue_print(int lp) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const gpq_device_queue& q = gpq_bound_queue;
+  printf("[queue %d] lp %d:", (int)q.kind, lp);
+  if (q.staged) {
+    const queue_item h = q.head[lp];
+    if (gpq_f2u(h.ts) != 0x7f800000u && !q.taken[lp]) printf(" (%.6f, id %u)", h.ts, h.id);
+  } else if (q.kind == GPQ_QUEUE_LHQ) {
+    const queue_item* it = q.ring + ((size_t)lp << q.cap_log2);
+    for (uint32_t i = 0; i < q.size[lp]; ++i) printf(" (%.6f, id %u)", it[i].ts, it[i].id);
+  } else {
+    const uint32_t m = (1u << q.cap_log2) - 1u;
+    const queue_item* it = q.ring + ((size_t)lp << q.cap_log2);
+    for (uint32_t c = q.rd[lp]; c != q.wr[lp]; ++c) printf(" (%.6f, id %u)", it[c & m].ts, it[c & m].id);
+  }
+  printf("\n");
 }
 
 #endif /* GPQ_QUEUE_CUH */

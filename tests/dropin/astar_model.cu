@@ -127,6 +127,7 @@ extern "C" int dropin_astar_run(const gpq_astar_grid* grids, uint32_t agents, ui
   cudaMemset(a.n_done, 0, sizeof(unsigned int));
   const uint32_t blocks = (agents + 127) / 128;
   astar_agent_start<<<blocks, 128>>>(a, agents);
+  if (cudaDeviceSynchronize() != cudaSuccess) st = GPQ_ERR_CUDA;  // the queue posts on its own stream
   if (!st) st = gpq_queue_post(q, NULL);
   unsigned long long rounds = 0;
   unsigned int n_done = 0;
@@ -135,6 +136,7 @@ extern "C" int dropin_astar_run(const gpq_astar_grid* grids, uint32_t agents, ui
     st = gpq_queue_set_bound(q, inf, NULL);  // A*: no window, every open item may be popped
     if (st) break;
     astar_agent_round<<<blocks, 128>>>(a, agents);
+    if (cudaDeviceSynchronize() != cudaSuccess) { st = GPQ_ERR_CUDA; break; }
     st = gpq_queue_post(q, NULL);
     ++rounds;
     if (cudaMemcpy(&n_done, a.n_done, sizeof(n_done), cudaMemcpyDeviceToHost) != cudaSuccess) st = GPQ_ERR_CUDA;
