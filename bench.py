@@ -365,6 +365,54 @@ def bench_phold_c2_gaq(G, O, args, peak):
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak}}
 
 
+ASTAR_REF_BYTES_PER_POP = 16 + 8 * 3 + 3 * 18  # pop + 8 neighbours (wall/closed bits, f_ol) + ~3 pushes with f_ol
+
+
+def bench_astar_ref(G, O, args, peak):
+    """The reference's own A* agent model (half-precision f, eight pops per round, stop at
+    the goal) at its preset's shape: one 256 x 256 map with obstacle squares (0.2 of the
+    cells, mean side 1), 2,048 concurrent agent slots, a pool of 16,384 agents; agents/s.
+    Every agent is checked against the CPU oracle of the same semantics."""
+    m = G.astar_ref_map(256, 256, 0.2, 1.0, seed=14580)
+    agents = G.astar_ref_agents(m, 16384, seed=11)
+    with G.AStarRef(256, 256, slots=2048) as a:
+        for _ in range(2):
+            r = a.solve(m, agents)
+        ms, walls = [], []
+        for _ in range(max(3, args.steps)):
+            t0 = time.perf_counter()
+            r2 = a.solve(m, agents)
+            walls.append(time.perf_counter() - t0)
+            ms.append(a.last_ms())
+            same = all(np.array_equal(r2[k], r[k]) for k in ("found", "pops", "rounds", "cost"))
+            if not same:
+                raise SystemExit("reference-semantics A* is not reproducible")
+    dev_s = statistics.median(ms) / 1e3
+    threads = os.cpu_count() or 1
+    sec_all, want = O.astar_ref(m, agents, threads)
+    exact = (all(np.array_equal(r[k], want[k]) for k in ("found", "pops", "rounds"))
+             and np.array_equal(r["cost"].view(np.uint32), want["cost"].view(np.uint32)))
+    pops = int(r["pops"].sum())
+    sample = 2048
+    sec, _ = O.astar_ref(m, agents[:sample], threads)
+    achieved = pops * ASTAR_REF_BYTES_PER_POP / dev_s / 1e9
+    return {"workload": "astar_reference_semantics_256x256_2048slots_16384agents",
+            "metric": "A* agents/s (reference semantics)", "value": len(agents) / dev_s, "unit": "agents/s",
+            "pops_per_s": pops / dev_s, "ms_per_pool": 1e3 * dev_s, "found": int(r["found"].sum()),
+            "mean_pops_per_agent": pops / len(agents), "exact_vs_oracle": bool(exact),
+            "exact_checked": f"all {len(agents)} agents (found, f at the goal, pops, rounds) against the CPU oracle",
+            "e2e": {"value": len(agents) / statistics.median(walls), "unit": "agents/s",
+                    "h2d_bytes_per_step": int(m.nbytes + agents.nbytes),
+                    "d2h_bytes_per_step": int(len(agents) * G.ASTAR_REF_RESULT_DTYPE.itemsize)},
+            "roofline": {"bound": "latency (dependent heap levels per warp; state L2-resident)", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak},
+            "cpu_baseline": {"value": sample / sec, "unit": "agents/s", "cores": threads, "kind": "port",
+                             "sample": f"first {sample} agents, one sequential agent per host thread",
+                             "cpu_model": cpu_model()},
+            "reference_binary": "not run: its kernel calls __syncthreads() in a thread-dependent branch "
+                                "(src/a_star.cu:526-554), undefined on sm_70 and later"}
+
+
 def bench_phold_batched(G, O, args, peak):
     """The PHOLD runs of the first second of the served stream (LPs log-uniform in
     [256, 65536], 32 events per LP, lookahead 0.5, end time 200), all in one launch of a
@@ -378,9 +426,9 @@ def bench_phold_batched(G, O, args, peak):
     def batch(bucketed, warmup, steps):
         with G.PholdSession(max_lps=lps, max_instances=len(runs), bucketed=bucketed) as s:
             def step():
+                t0 = time.perf_counter()
                 for r in runs:
                     s.admit(r)
-                t0 = time.perf_counter()
                 s.step(0)
                 got = s.collect()
                 return got, time.perf_counter() - t0
@@ -390,35 +438,48 @@ def bench_phold_batched(G, O, args, peak):
     ev, dt, got = batch(False, args.warmup, args.steps)
     ev0, dt0, got0 = batch(True, 1, args.steps)
     same = sorted((r.committed, r.digest) for _, r in got) == sorted((r.committed, r.digest) for _, r in got0)
+    # the plain path: each run alone through its own handle.  Handles are created before
+    # the timing, as the batch's session is; each timed run is populate + all windows +
+    # result, as each timed batch step is admit + all windows + collect.
     plain = {}
     for mode in (2, 0):
         pe, pt, pw = 0, 0.0, 0.0
-        for r in runs[:16]:
-            c = G.make_phold_config(r.num_lps, 32, 0.5, 200.0, r.seed, laq_mode=mode,
-                                    **({"block_threads": 512} if mode == 2 else {}))
-            t0 = time.perf_counter()
-            with G.Phold(c) as h:  # the plain path: a handle per run, populate, run, results
+        handles = [G.Phold(G.make_phold_config(r.num_lps, 32, 0.5, 200.0, r.seed, laq_mode=mode,
+                                               **({"block_threads": 512} if mode == 2 else {})))
+                   for r in runs[:16]]
+        try:
+            for h in handles:  # warm-up
+                h.populate()
+                h.run()
+                h.result()
+            for h in handles:
+                t0 = time.perf_counter()
                 h.populate()
                 h.run()
                 rr = h.result()
-            pw += time.perf_counter() - t0
-            pe += rr["committed"]
-            pt += rr["elapsed_ms"] / 1e3
+                pw += time.perf_counter() - t0
+                pe += rr["committed"]
+                pt += rr["elapsed_ms"] / 1e3
+        finally:
+            for h in handles:
+                h.close()
         plain[mode] = (pe / pw, pe / pt)
     pv = max(plain[2][0], plain[0][0])
+    pdv = max(plain[2][1], plain[0][1])
     achieved = ev * BYTES_PER_EVENT * args.steps / dt / 1e9
     return {"workload": f"phold_batched_{len(runs)}runs_lp256-65536_x32_T200", "metric": "PHOLD events/s (batched)",
             "value": ev * args.steps / dt, "unit": "events/s", "runs": len(runs), "lps": lps,
             "ms_per_batch": 1e3 * dt / args.steps, "queue_form": "sorted rings",
             "time_bucket_session_value": ev0 * args.steps / dt0, "same_results_both_forms": same,
             "plain_value": pv, "plain_bucketed_value": plain[2][0], "plain_sorted_value": plain[0][0],
-            "plain_device_value": max(plain[2][1], plain[0][1]),
-            "plain_sample": "first 16 runs, each alone through its own handle (host wall clock, like the batch), "
-                            "bucketed and sorted queue forms; plain_value is the faster; plain_device_value "
-                            "counts device time only",
+            "plain_device_value": pdv,
+            "plain_sample": "first 16 runs, each alone through its own handle created before the timing "
+                            "(populate + run + result on the host clock, like admit + step + collect of the "
+                            "batch), bucketed and sorted queue forms; plain_value is the faster; "
+                            "plain_device_value counts device time only",
             "batched_over_plain": (ev * args.steps / dt) / pv,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak},
-            "timing": "host wall clock around the session step (populate, all windows, collect)"}
+            "timing": "host wall clock around admit + session step (populate, all windows) + collect"}
 
 
 def bench_served(G, args, duration):
@@ -484,6 +545,13 @@ def run_case(name):
                 t = time.perf_counter()
                 q.post()
                 print(f"post of {N} items: {(time.perf_counter() - t) * 1e3:.2f} ms (host clock)")
+    elif name == "astar_ref_2048":
+        m = G.astar_ref_map(256, 256, 0.2, 1.0, seed=14580)
+        agents = G.astar_ref_agents(m, 4096, seed=11)
+        with G.AStarRef(256, 256, slots=2048) as a:
+            for _ in range(2):
+                r = a.solve(m, agents)
+            print(a.last_ms(), int(r["pops"].sum()))
     elif name == "phold_batched_36":
         reqs, n = G.serve_stream(99, 2000.0, 0.1)
         runs = [reqs[i].phold for i in range(n) if reqs[i].kind == G.REQ_PHOLD][:40]
@@ -518,7 +586,8 @@ def main():
     ap.add_argument("--no-forms", action="store_true", help="skip the A*, batched and served sections")
     ap.add_argument("--served-seconds", type=float, default=1.0, help="length of the served request stream")
     ap.add_argument("--case", default=None,
-                    choices=["astar_batched_1000", "astar_plain_2048", "phold_batched_36", "gaq_sort_32m"],
+                    choices=["astar_batched_1000", "astar_plain_2048", "phold_batched_36", "gaq_sort_32m",
+                             "astar_ref_2048"],
                     help="run one small named workload twice and exit (profiling captures)")
     args = ap.parse_args()
     if args.case:
@@ -684,6 +753,7 @@ def main():
                  "phold_c2_gaq": bench_phold_c2_gaq(G, O, args, peak),
                  "astar_plain": bench_astar_plain(G, O, args, peak),
                  "astar_batched": bench_astar_batched(G, O, args, peak),
+                 "astar_reference_semantics": bench_astar_ref(G, O, args, peak),
                  "phold_batched": bench_phold_batched(G, O, args, peak),
                  "served": bench_served(G, args, args.served_seconds)}
     if rank == 0:

@@ -114,6 +114,23 @@ _SIGS = {
                                ctypes.POINTER(ctypes.c_uint32)], ctypes.c_int),
     "gpq_phold_run_static": ([ctypes.POINTER(PholdConfig), _VP, _VP, _VP, _VP, ctypes.POINTER(PholdResult), _VP],
                              ctypes.c_int),
+    "gpq_astar_ref_create": ([_VP, ctypes.POINTER(_VP)], ctypes.c_int),
+    "gpq_astar_ref_destroy": ([_VP], ctypes.c_int),
+    "gpq_astar_ref_solve": ([_VP, _VP, _VP, ctypes.c_uint32, _VP, _VP], ctypes.c_int),
+    "gpq_astar_ref_last_ms": ([_VP, ctypes.POINTER(ctypes.c_float)], ctypes.c_int),
+    "gpq_astar_ref_map": ([ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float, ctypes.c_float, ctypes.c_uint64, _VP],
+                          ctypes.c_int),
+    "gpq_astar_ref_agents": ([_VP, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, _VP],
+                             ctypes.c_int),
+    "gpq_legacy_configure": ([_VP, ctypes.c_float, ctypes.c_float], ctypes.c_int),
+    "gpq_legacy_init": ([ctypes.POINTER(_VP)], ctypes.c_int),
+    "gpq_legacy_queue": ([], _VP),
+    "gpq_legacy_pre": ([], ctypes.c_int),
+    "gpq_legacy_post": ([], ctypes.c_int),
+    "gpq_legacy_get_min_ts": ([], ctypes.c_float),
+    "gpq_legacy_counts": ([ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
+    "gpq_legacy_finish": ([], ctypes.c_int),
+    "gpq_legacy_status": ([], ctypes.c_int),
     "gpq_host_alloc": ([ctypes.c_uint64, ctypes.POINTER(_VP)], ctypes.c_int),
     "gpq_host_free": ([_VP], ctypes.c_int),
     "gpq_queue_create": ([ctypes.c_void_p, ctypes.POINTER(_VP)], ctypes.c_int),
@@ -462,6 +479,71 @@ ASTAR_GRID_DTYPE = np.dtype([("seed", "<u8"), ("width", "<u4"), ("height", "<u4"
                              ("conn", "<u4"), ("start", "<u4"), ("goal", "<u4")])
 ASTAR_RESULT_DTYPE = np.dtype([("cost", "<u4"), ("path_len", "<u4"), ("expanded", "<u8"), ("gsum", "<u8"),
                                ("path_hash", "<u8"), ("pops", "<u8"), ("windows", "<u4"), ("status", "<i4")])
+
+
+ASTAR_REF_AGENT_DTYPE = np.dtype([("start", "<u4"), ("goal", "<u4")])
+ASTAR_REF_RESULT_DTYPE = np.dtype([("found", "<u4"), ("cost", "<f4"), ("pops", "<u4"), ("rounds", "<u4"),
+                                   ("status", "<u4"), ("reserved", "<u4")])
+
+
+class AstarRefConfig(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in ("width", "height", "slots", "open_capacity")] + \
+        [("reserved", ctypes.c_uint32 * 4)]
+
+
+def astar_ref_map(width, height, obstacle_frac=0.2, size_mean=1.0, seed=0):
+    """The reference's random obstacle map (gpq_astar_ref_map): uint8 [height, width], 1 = wall."""
+    m = np.zeros(width * height, np.uint8)
+    check(lib().gpq_astar_ref_map(width, height, obstacle_frac, size_mean, seed, _ptr(m)), "gpq_astar_ref_map")
+    return m.reshape(height, width)
+
+
+def astar_ref_agents(map2d, n, seed=0):
+    """n agents with random free start and goal cells (gpq_astar_ref_agents)."""
+    m = np.ascontiguousarray(map2d, np.uint8)
+    out = np.zeros(n, ASTAR_REF_AGENT_DTYPE)
+    check(lib().gpq_astar_ref_agents(_ptr(m), m.shape[1], m.shape[0], n, seed, _ptr(out)), "gpq_astar_ref_agents")
+    return out
+
+
+class AStarRef:
+    """Reference-semantics A* (gpq_astar_ref_*): the reference's agents (half-precision f,
+    eight pops per round, stop at the goal) over a pool of agents on one map."""
+
+    def __init__(self, width, height, slots=0, open_capacity=0):
+        c = AstarRefConfig()
+        c.width, c.height, c.slots, c.open_capacity = width, height, slots, open_capacity
+        self._h = ctypes.c_void_p()
+        check(lib().gpq_astar_ref_create(ctypes.byref(c), ctypes.byref(self._h)), "gpq_astar_ref_create")
+
+    def solve(self, map2d, agents):
+        m = np.ascontiguousarray(map2d, np.uint8)
+        a = np.ascontiguousarray(agents, ASTAR_REF_AGENT_DTYPE)
+        out = np.zeros(len(a), ASTAR_REF_RESULT_DTYPE)
+        check(lib().gpq_astar_ref_solve(self._h, _ptr(m), _ptr(a), len(a), _ptr(out), None), "gpq_astar_ref_solve")
+        return out
+
+    def last_ms(self):
+        v = ctypes.c_float()
+        check(lib().gpq_astar_ref_last_ms(self._h, ctypes.byref(v)), "gpq_astar_ref_last_ms")
+        return v.value
+
+    def close(self):
+        if self._h:
+            lib().gpq_astar_ref_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class AstarConfig(ctypes.Structure):

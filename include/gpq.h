@@ -556,6 +556,54 @@ GPQ_API gpq_status gpq_host_free(void* p);
 GPQ_API gpq_status gpq_set_spin_limit(uint64_t iterations);
 
 /* ---------------------------------------------------------------------------------- */
+/* 2c. Reference-semantics A* (the reference's agent model, src/a_star.cu:124-593)     */
+/* ---------------------------------------------------------------------------------- */
+
+/* Semantics in include/gpq/astar_ref.h: half-precision f, eight pops per round, 3 x 3
+ * exploration with clamped coordinates, de-duplication and the f_ol filter, stop when
+ * the goal is popped, a pool of agents handed to concurrent slots (get_new_agent); ties
+ * of (f, h) go by cell id, so results are deterministic.  Agents are independent, so
+ * each slot (one warp) runs its agents to completion inside one persistent launch --
+ * the reference launches one kernel per round for all agents. */
+typedef struct gpq_astar_ref gpq_astar_ref;
+
+typedef struct gpq_astar_ref_config {
+  uint32_t width, height;   /* map size (A_STAR_GRID_X, A_STAR_GRID_Y) */
+  uint32_t slots;           /* concurrent agents (NUM_CONCURRENT_AGENTS); 0 = 2048 */
+  uint32_t open_capacity;   /* open-list items per slot; 0 = 4 * width * height */
+  uint32_t reserved[4];
+} gpq_astar_ref_config;
+
+typedef struct gpq_astar_ref_agent {
+  uint32_t start, goal;     /* cells (y * width + x) */
+} gpq_astar_ref_agent;
+
+typedef struct gpq_astar_ref_result {
+  uint32_t found;           /* the goal was popped */
+  float cost;               /* its f (half precision, as a float) when popped */
+  uint32_t pops;            /* vertices popped, duplicates included */
+  uint32_t rounds;          /* rounds of at most eight pops */
+  uint32_t status;          /* gpq_status; GPQ_ERR_QUEUE_FULL: open_capacity too small */
+  uint32_t reserved;
+} gpq_astar_ref_result;
+
+GPQ_API gpq_status gpq_astar_ref_create(const gpq_astar_ref_config* cfg, gpq_astar_ref** out);
+GPQ_API gpq_status gpq_astar_ref_destroy(gpq_astar_ref* h);
+/* Runs the n agents (HOST arrays) on the map (HOST, width * height bytes, non-zero =
+ * wall); results in agent order.  Blocks on the stream. */
+GPQ_API gpq_status gpq_astar_ref_solve(gpq_astar_ref* h, const uint8_t* map, const gpq_astar_ref_agent* agents,
+                                       uint32_t n, gpq_astar_ref_result* results, void* stream);
+/* Device time of the last solve's search kernel (CUDA events). */
+GPQ_API gpq_status gpq_astar_ref_last_ms(gpq_astar_ref* h, float* ms);
+/* The reference's random map (src/a_star.cu:747-765): obstacle_frac * width * height
+ * squares at uniform positions, side max(1, (int)(size_mean * Exp(1))), drawn from seed. */
+GPQ_API gpq_status gpq_astar_ref_map(uint32_t width, uint32_t height, float obstacle_frac, float size_mean,
+                                     uint64_t seed, uint8_t* map);
+/* n agents with uniformly random free start and goal cells (src/a_star.cu:768-789). */
+GPQ_API gpq_status gpq_astar_ref_agents(const uint8_t* map, uint32_t width, uint32_t height, uint32_t n,
+                                        uint64_t seed, gpq_astar_ref_agent* out);
+
+/* ---------------------------------------------------------------------------------- */
 /* 3. Utilities                                                                       */
 /* ---------------------------------------------------------------------------------- */
 

@@ -1,6 +1,6 @@
 """Build recipe for the CPU oracle (test infrastructure only).
 
-Compiles oracle/phold_oracle.cpp (and the A* oracle) into oracle/_build/libgpq_oracle.so
+Compiles oracle/phold_oracle.cpp (and the two A* oracles) into oracle/_build/libgpq_oracle.so
 with g++.  FP contraction is disabled so that float32 results are bit-identical to the
 GPU build.  Called by __graft_entry__.build() and by the tests when the library is missing.
 """
@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT_DIR, "libgpq_oracle.so")
-SOURCES = ["phold_oracle.cpp", "astar_oracle.cpp"]
+SOURCES = ["phold_oracle.cpp", "astar_oracle.cpp", "astar_ref_oracle.cpp"]
 
 
 def build(force: bool = False) -> str:

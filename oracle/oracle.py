@@ -85,6 +85,15 @@ def lib():
         _LIB.oracle_astar_batch.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int,
                                             ctypes.c_void_p]
         _LIB.oracle_astar_batch.restype = ctypes.c_double
+        _LIB.oracle_astar_ref_run.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
+                                              ctypes.c_uint32, ctypes.c_int, ctypes.c_void_p]
+        _LIB.oracle_astar_ref_run.restype = ctypes.c_double
+        _LIB.oracle_to_half.argtypes = [ctypes.c_float]
+        _LIB.oracle_to_half.restype = ctypes.c_float
+        _LIB.oracle_half_bits.argtypes = [ctypes.c_float]
+        _LIB.oracle_half_bits.restype = ctypes.c_uint32
+        _LIB.oracle_astar_ref_h.argtypes = [ctypes.c_int] * 4
+        _LIB.oracle_astar_ref_h.restype = ctypes.c_float
     return _LIB
 
 
@@ -219,3 +228,19 @@ def astar_batch(grids, threads):
         raise RuntimeError("A* oracle self-check failed")
     return sec, [{"cost": r.cost, "path_len": r.path_len, "expanded": r.expanded, "gsum": r.gsum,
                   "path_hash": r.path_hash, "pops": r.pops} for r in res]
+
+
+ASTAR_REF_RESULT_DTYPE = np.dtype([("found", "<u4"), ("cost", "<f4"), ("pops", "<u4"), ("rounds", "<u4")])
+
+
+def astar_ref(map2d, agents, threads=1):
+    """Reference-semantics A* for every agent ((start, goal) pairs) on a map
+    (uint8 [height, width], non-zero = wall); returns (seconds, results)."""
+    m = np.ascontiguousarray(map2d, np.uint8)
+    sg = np.ascontiguousarray(np.stack([np.asarray(agents["start"], np.uint32),
+                                        np.asarray(agents["goal"], np.uint32)], axis=1))
+    out = np.zeros(len(sg), ASTAR_REF_RESULT_DTYPE)
+    sec = lib().oracle_astar_ref_run(m.shape[1], m.shape[0], ctypes.c_void_p(m.ctypes.data),
+                                     ctypes.c_void_p(sg.ctypes.data), len(sg), threads,
+                                     ctypes.c_void_p(out.ctypes.data))
+    return sec, out
