@@ -365,6 +365,33 @@ def bench_phold_c2_gaq(G, O, args, peak):
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak}}
 
 
+def bench_phold_long_queues(G, O, args, peak):
+    """Long per-LP queues (what the reference's local array queue backed by a heap is for,
+    src/local_array_queue.cu:517-561,603-681): 4,096 LPs with 4,096 pending events each,
+    lookahead 0.01 (about 40 safe events per LP per window), ring +-16, end time 2 --
+    through the bucketed local array queue (near events in time buckets, far ones in the
+    per-LP spill lists), the sorted form and the per-LP heap; each checked against the
+    committed oracle results."""
+    name = "phold_long_4096lp_x4096_ring16_T2"
+    g = golden(name)
+    cfgd = dict(g["config"]) if g else dict(num_lps=4096, events_per_lp=4096, lookahead=0.01, end_time=2.0, seed=23,
+                                            dest_mode=1, ring_width=16)
+    forms = {}
+    for label, queue, kw in (("laq_time_buckets", "laq", dict(laq_mode=2, capacity=8192)),
+                             ("laq_sorted", "laq", dict(laq_mode=0, capacity=8192, insert_capacity=128)),
+                             ("local_heap", "lhq", dict(capacity=8192, insert_capacity=128))):
+        v, ms, (r, st) = _phold_form(G, O, cfgd, queue, runs=2, **kw)
+        forms[label] = {"value": v, "ms_per_run": ms, "exact_vs_oracle": matches_golden(O, g, r, st)}
+    best = forms["laq_time_buckets"]
+    by = BYTES_PER_EVENT * (g["committed"] if g else 0) + BYTES_PER_LP_WINDOW * cfgd["num_lps"] * (
+        g["windows"] if g else 0)
+    achieved = by / (best["ms_per_run"] / 1e3) / 1e9
+    return {"workload": name, "metric": "PHOLD committed events/s", "value": best["value"], "unit": "events/s",
+            "exact_vs_oracle": best["exact_vs_oracle"], "forms": forms,
+            "timing": "device time of whole runs (CUDA events), 2 runs after 1 warm-up",
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak}}
+
+
 ASTAR_REF_BYTES_PER_POP = 16 + 8 * 3 + 3 * 18  # pop + 8 neighbours (wall/closed bits, f_ol) + ~3 pushes with f_ol
 
 
@@ -751,6 +778,7 @@ def main():
         peak, _ = load_peaks()
         forms = {"phold_c1": bench_phold_c1(G, O, args, peak),
                  "phold_c2_gaq": bench_phold_c2_gaq(G, O, args, peak),
+                 "phold_long_queues": bench_phold_long_queues(G, O, args, peak),
                  "astar_plain": bench_astar_plain(G, O, args, peak),
                  "astar_batched": bench_astar_batched(G, O, args, peak),
                  "astar_reference_semantics": bench_astar_ref(G, O, args, peak),

@@ -362,7 +362,9 @@ gpq_status gpq_phold_populate(gpq_phold* h, const gpq_item* initial, uint64_t n,
     h->elapsed_ms = 0.f;
     return GPQ_OK;
   }
-  const uint32_t wpb = 4;
+  // one warp per LP ranks its events in shared memory (24 B each): four warps per CTA up
+  // to 2,048 events per LP, one beyond (8,192 events: 192 KiB)
+  const uint32_t wpb = c.events_per_lp <= 2048 ? 4 : 1;
   const size_t smem = (size_t)wpb * c.events_per_lp * (sizeof(gpq_item) + sizeof(uint64_t));
   GPQ_CUDA_TRY(gpq::raise_smem_limit(phold_populate_kernel, (int)smem));
   const uint32_t grid = (uint32_t)((L + wpb - 1) / wpb);

@@ -93,7 +93,7 @@ inline gpq_status normalize_queue_config(gpq_phold_config* c) {
     GPQ_CHECK_ARG(c->capacity <= 32768, "splay queue capacity must be <= 32768");
   GPQ_CHECK_ARG(c->insert_capacity >= 1 && c->insert_capacity <= 1024, "insert_capacity must be in [1, 1024]");
   GPQ_CHECK_ARG(c->events_per_lp <= c->capacity, "events_per_lp must not exceed capacity");
-  GPQ_CHECK_ARG(c->events_per_lp <= 2048, "events_per_lp must be <= 2048");
+  GPQ_CHECK_ARG(c->events_per_lp <= 8192, "events_per_lp must be <= 8192");
   if (c->block_threads == 0) c->block_threads = 256;
   GPQ_CHECK_ARG(c->block_threads % 32 == 0 && c->block_threads >= 32 && c->block_threads <= 1024,
                 "block_threads must be a multiple of 32 in [32, 1024]");

@@ -36,6 +36,10 @@ CASES = {
                                                   seed=7, dest_mode=1, ring_width=16), "window"),
     "phold_large_65536lp_x64_ring16_T3": (dict(num_lps=65536, events_per_lp=64, lookahead=0.1, end_time=3.0,
                                                seed=7, dest_mode=1, ring_width=16), "window"),
+    # long per-LP queues: 4,096 LPs x 4,096 pending events, lookahead 0.01 (about 40 safe
+    # events per LP per window), ring +-16, end 2
+    "phold_long_4096lp_x4096_ring16_T2": (dict(num_lps=4096, events_per_lp=4096, lookahead=0.01, end_time=2.0,
+                                               seed=23, dest_mode=1, ring_width=16), "window"),
     "phold_large_65536lp_x64_ring16_T3_one_per_lp": (dict(num_lps=65536, events_per_lp=64, lookahead=0.1,
                                                           end_time=3.0, seed=7, dest_mode=1, ring_width=16),
                                                      "one_per_lp"),
