@@ -21,6 +21,7 @@
 // per-LP ranking restores the (ts bits, LP, id) order where it is observable.
 #pragma once
 
+#include "bulk_copy.cuh"
 #include "phold_common.cuh"
 
 static constexpr uint32_t kRsThreads = 256;  // = number of 8-bit digits
@@ -127,7 +128,9 @@ static __global__ void __launch_bounds__(1024) rs_chunk_scan_kernel(const uint32
 }
 
 // Stable scatter of one tile through shared memory.  Warp w owns the tile's items
-// [w * 512, (w + 1) * 512), loaded 32 at a time (coalesced, all 16 loads in flight).  It
+// [w * 512, (w + 1) * 512); they arrive in shared memory with one TMA bulk copy per warp
+// (issued by its lane 0, completed on the warp's own mbarrier, while the CTA scans the
+// tile's digit counts), so each warp starts ranking as soon as its own 8 KB land.  It
 // ranks them without block barriers: an item's rank among the same-digit items of its warp
 // is the warp's running count for the digit (warp-private counters, one leader lane per
 // group of equal digits updates it) plus the lower lanes of its round with that digit.
@@ -142,20 +145,24 @@ static constexpr uint32_t kRsWarpItems = kRsTile / kRsWarps;
 static __global__ void __launch_bounds__(kRsThreads) rs_scatter_kernel(const gpq_item* __restrict__ in, gpq_item* out,
                                                                        uint32_t n, uint32_t kmin, uint32_t shift,
                                                                        const uint32_t* __restrict__ cnt,
-                                                                       const uint32_t* __restrict__ off, uint32_t ntiles) {
+                                                                       const uint32_t* __restrict__ off, uint32_t ntiles,
+                                                                       uint32_t* err) {
   extern __shared__ __align__(16) unsigned char rs_smem[];
-  gpq_item* s_it = reinterpret_cast<gpq_item*>(rs_smem);  // [kRsTile]
+  gpq_item* s_it = reinterpret_cast<gpq_item*>(rs_smem);  // [kRsTile]: the input tile, then the output layout
   __shared__ uint32_t gpos[256], wtot[kRsWarps];
   __shared__ uint32_t wc[kRsWarps][256];  // per-warp digit counts, then the warp's start per digit
+  __shared__ __align__(8) uint64_t bar[kRsWarps];
   const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
   const uint32_t tile = blockIdx.x;
-  const uint32_t base = tile * kRsTile + warp * kRsWarpItems;
-  gpq_item ev[kRsPer];
-#pragma unroll
-  for (uint32_t j = 0; j < kRsPer; ++j) {
-    const uint32_t i = base + j * 32 + lane;
-    if (i < n) ev[j] = in[i];
+  const uint32_t t0 = tile * kRsTile;
+  const uint32_t tn = min(kRsTile, n - t0);
+  const uint32_t w0 = min(warp * kRsWarpItems, tn), wn = min(tn - w0, kRsWarpItems);  // this warp's items
+  if (lane == 0) {
+    mbar_init(&bar[warp]);
+    mbar_arrive_expect_tx(&bar[warp], wn * (uint32_t)sizeof(gpq_item));
+    if (wn) bulk_g2s(s_it + w0, in + t0 + w0, wn * (uint32_t)sizeof(gpq_item), &bar[warp]);
   }
+  const uint32_t base = t0 + warp * kRsWarpItems;
   for (uint32_t d = lane; d < 256; d += 32) wc[warp][d] = 0;
   // the tile's digit runs: exclusive scan of its counts (thread t = digit t)
   const uint32_t c = cnt[(size_t)t * ntiles + tile];
@@ -167,6 +174,13 @@ static __global__ void __launch_bounds__(kRsThreads) rs_scatter_kernel(const gpq
   }
   if (lane == 31) wtot[warp] = incl;
   __syncwarp();
+  const bool arrived = mbar_wait_bounded(&bar[warp], 0, err);
+  gpq_item ev[kRsPer];
+#pragma unroll
+  for (uint32_t j = 0; j < kRsPer; ++j) {
+    const uint32_t k = warp * kRsWarpItems + j * 32 + lane;
+    if (k < tn) ev[j] = s_it[k];
+  }
   // warp-private ranks
   uint32_t rk[kRsPer];
 #pragma unroll
@@ -180,7 +194,7 @@ static __global__ void __launch_bounds__(kRsThreads) rs_scatter_kernel(const gpq
     if (valid && lane == (uint32_t)(__ffs(peers) - 1)) wc[warp][dgt] = before + __popc(peers);
     __syncwarp();
   }
-  __syncthreads();
+  if (!__syncthreads_and(arrived)) return;  // a staging copy did not complete: skip the tile (error recorded)
   // thread t = digit t: the tile's start for t, then each warp's start
   uint32_t wbase = 0;
   for (uint32_t w = 0; w < warp; ++w) wbase += wtot[w];
@@ -197,8 +211,6 @@ static __global__ void __launch_bounds__(kRsThreads) rs_scatter_kernel(const gpq
   for (uint32_t j = 0; j < kRsPer; ++j)
     if (base + j * 32 + lane < n) s_it[wc[warp][rs_digit(ev[j], kmin, shift)] + rk[j]] = ev[j];
   __syncthreads();
-  const uint32_t t0 = tile * kRsTile;
-  const uint32_t tn = min(kRsTile, n - t0);
   for (uint32_t k = t; k < tn; k += kRsThreads) {
     const gpq_item e = s_it[k];
     out[gpos[rs_digit(e, kmin, shift)] + k] = e;
@@ -216,22 +228,45 @@ __device__ __forceinline__ uint32_t mp_search(const gpq_item* A, uint32_t na, co
   return lo;
 }
 
-// Merge path: CTA b writes outputs [b*kMpTile, (b+1)*kMpTile) of merge(A, B).
+// Merge-path splits of merge(A, B): split[b] = A items among the first b * kMpTile outputs,
+// one thread per tile boundary (all searches at once, in their own pass).
+static __global__ void mp_splits_kernel(const gpq_item* __restrict__ A, uint32_t na, const gpq_item* __restrict__ B,
+                                        uint32_t nb, uint32_t* split) {
+  const uint32_t total = na + nb;
+  const uint32_t tiles = (total + kMpTile - 1) / kMpTile;
+  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b <= tiles; b += gridDim.x * blockDim.x)
+    split[b] = mp_search(A, na, B, nb, min(b * kMpTile, total));
+}
+
+// Stages A[a0, a0 + la) and B[b0, b0 + lb) at s[0, la) and s[la, la + lb) with TMA bulk
+// copies issued by thread 0; all threads.  Returns false (for every thread) if the copies
+// did not complete within the bound.
+__device__ __forceinline__ bool mp_stage_inputs(gpq_item* s, const gpq_item* A, uint32_t a0, uint32_t la,
+                                                const gpq_item* B, uint32_t b0, uint32_t lb, uint64_t* bar,
+                                                uint32_t* err) {
+  if (threadIdx.x == 0) mbar_init(bar);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    mbar_arrive_expect_tx(bar, (la + lb) * (uint32_t)sizeof(gpq_item));
+    if (la) bulk_g2s(s, A + a0, la * (uint32_t)sizeof(gpq_item), bar);
+    if (lb) bulk_g2s(s + la, B + b0, lb * (uint32_t)sizeof(gpq_item), bar);
+  }
+  return __syncthreads_and(mbar_wait_bounded(bar, 0, err)) != 0;
+}
+
+// Merge path: CTA b writes outputs [b*kMpTile, (b+1)*kMpTile) of merge(A, B), its inputs
+// located by the precomputed splits and staged by TMA.
 static __global__ void mp_merge_kernel(const gpq_item* __restrict__ A, uint32_t na, const gpq_item* __restrict__ B,
-                                       uint32_t nb, gpq_item* out) {
-  __shared__ gpq_item s[kMpTile];
-  __shared__ uint32_t sa[2];
+                                       uint32_t nb, gpq_item* out, const uint32_t* __restrict__ split, uint32_t* err) {
+  __shared__ __align__(16) gpq_item s[kMpTile];
+  __shared__ __align__(8) uint64_t bar;
   const uint32_t total = na + nb;
   const uint32_t d0 = blockIdx.x * kMpTile;
   const uint32_t d1 = min(d0 + kMpTile, total);
-  if (threadIdx.x < 2) sa[threadIdx.x] = mp_search(A, na, B, nb, threadIdx.x == 0 ? d0 : d1);
-  __syncthreads();
-  const uint32_t a0 = sa[0], a1 = sa[1];
+  const uint32_t a0 = split[blockIdx.x], a1 = split[blockIdx.x + 1];
   const uint32_t b0 = d0 - a0, b1 = d1 - a1;
   const uint32_t la = a1 - a0, lb = b1 - b0;
-  for (uint32_t x = threadIdx.x; x < la; x += kMpThreads) s[x] = A[a0 + x];
-  for (uint32_t x = threadIdx.x; x < lb; x += kMpThreads) s[la + x] = B[b0 + x];
-  __syncthreads();
+  if (!mp_stage_inputs(s, A, a0, la, B, b0, lb, &bar, err)) return;
   // each thread merges its kMpPer outputs into registers, the tile goes back to shared
   // memory in output order, and the CTA writes it with coalesced stores
   const uint32_t my0 = threadIdx.x * kMpPer, len = la + lb;
@@ -629,7 +664,7 @@ static __global__ void gaq_win_splits_kernel(const gpq_item* arr0, const gpq_ite
 
 // Merge the array's unsafe suffix with the sorted children into the other buffer.
 static __global__ void gaq_win_merge_kernel(gpq_item* arr0, gpq_item* arr1, const gpq_item* ch, const gpq_item* ch_tmp,
-                                            const GaqWin* w, const uint32_t* __restrict__ split) {
+                                            const GaqWin* w, const uint32_t* __restrict__ split, uint32_t* err) {
   if (!w->gate) return;
   const uint32_t total = w->total;
   const uint32_t d0 = blockIdx.x * kMpTile;
@@ -645,9 +680,8 @@ static __global__ void gaq_win_merge_kernel(gpq_item* arr0, gpq_item* arr1, cons
   const uint32_t a0 = split[blockIdx.x], a1 = split[blockIdx.x + 1];
   const uint32_t b0 = d0 - a0, b1 = d1 - a1;
   const uint32_t la = a1 - a0, lb = b1 - b0;
-  for (uint32_t x = threadIdx.x; x < la; x += kMpThreads) s[x] = A[a0 + x];
-  for (uint32_t x = threadIdx.x; x < lb; x += kMpThreads) s[la + x] = B[b0 + x];
-  __syncthreads();
+  __shared__ __align__(8) uint64_t bar;
+  if (!mp_stage_inputs(s, A, a0, la, B, b0, lb, &bar, err)) return;
   const uint32_t my0 = threadIdx.x * kMpPer;
   if (my0 < la + lb) {
     uint32_t ia = mp_search(s, la, s + la, lb, my0);

@@ -37,7 +37,7 @@ size_t radix_hist_words(uint32_t n) {
 }
 
 gpq_status radix_sort_by_ts(gpq_item* a, gpq_item* b, uint32_t n, uint32_t kmin, uint32_t kmax, uint32_t* hist,
-                            gpq_item** sorted, cudaStream_t st) {
+                            gpq_item** sorted, uint32_t* err, cudaStream_t st) {
   *sorted = a;
   if (n <= 1 || kmax <= kmin) return GPQ_OK;
   GPQ_CUDA_TRY(gpq::raise_smem_limit(rs_scatter_kernel, (int)(kRsTile * sizeof(gpq_item))));
@@ -57,7 +57,7 @@ gpq_status radix_sort_by_ts(gpq_item* a, gpq_item* b, uint32_t n, uint32_t kmin,
     gpq_status s = scan_exclusive(cnt, off, cells, scratch, st);
     if (s != GPQ_OK) return s;
     rs_scatter_kernel<<<ntiles, kRsThreads, kRsTile * sizeof(gpq_item), st>>>(src, dst, n, kmin, shift, cnt, off,
-                                                                              ntiles);
+                                                                              ntiles, err);
     GPQ_CUDA_TRY(cudaGetLastError());
     std::swap(src, dst);
   }
@@ -65,12 +65,15 @@ gpq_status radix_sort_by_ts(gpq_item* a, gpq_item* b, uint32_t n, uint32_t kmin,
   return GPQ_OK;
 }
 
-gpq_status merge_by_ts(const gpq_item* A, uint32_t na, const gpq_item* B, uint32_t nb, gpq_item* out,
-                       cudaStream_t st) {
+size_t merge_split_words(uint32_t total) { return (size_t)(total + kMpTile - 1) / kMpTile + 2; }
+
+gpq_status merge_by_ts(const gpq_item* A, uint32_t na, const gpq_item* B, uint32_t nb, gpq_item* out, uint32_t* split,
+                       uint32_t* err, cudaStream_t st) {
   const uint32_t total = na + nb;
   if (total == 0) return GPQ_OK;
   const uint32_t grid = (total + kMpTile - 1) / kMpTile;
-  mp_merge_kernel<<<grid, kMpThreads, 0, st>>>(A, na, B, nb, out);
+  mp_splits_kernel<<<(grid + 1 + 255) / 256, 256, 0, st>>>(A, na, B, nb, split);
+  mp_merge_kernel<<<grid, kMpThreads, 0, st>>>(A, na, B, nb, out, split, err);
   GPQ_CUDA_TRY(cudaGetLastError());
   return GPQ_OK;
 }
@@ -198,7 +201,8 @@ gpq_status gaq_engine_populate(GaqEngine* g, const PholdDev& d, const gpq_item* 
   GPQ_CUDA_TRY(cudaMemcpyAsync(g->h_info, g->info, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
   GPQ_CUDA_TRY(cudaStreamSynchronize(st));
   gpq_item* sorted = nullptr;
-  gpq_status s = radix_sort_by_ts(g->ch, g->ch_tmp, g->cap, g->h_info[0], g->h_info[1], g->hist, &sorted, st);
+  gpq_status s = radix_sort_by_ts(g->ch, g->ch_tmp, g->cap, g->h_info[0], g->h_info[1], g->hist, &sorted,
+                                  &d.ctrl->err, st);
   if (s != GPQ_OK) return s;
   GPQ_CUDA_TRY(cudaMemcpyAsync(g->arr[0], sorted, (size_t)g->cap * sizeof(gpq_item), cudaMemcpyDeviceToDevice, st));
   g->cur = 0;
@@ -237,7 +241,8 @@ static gpq_status gaq_capture(GaqEngine* g, const PholdDev& d, cudaStream_t st) 
   gaq_win_splits_kernel<<<(mgrid + 1 + 255) / 256, 256, 0, st>>>(g->arr[0], g->arr[1], g->ch, g->ch_tmp, g->win,
                                                                   g->split);
   gaq_win_merge_kernel<<<mgrid, kMpThreads, 2 * kMpTile * sizeof(gpq_item), st>>>(g->arr[0], g->arr[1], g->ch,
-                                                                                  g->ch_tmp, g->win, g->split);
+                                                                                  g->ch_tmp, g->win, g->split,
+                                                                                  &d.ctrl->err);
   gaq_win_end_kernel<<<1, 32, 0, st>>>(g->win);
   const cudaError_t ce = cudaStreamEndCapture(st, &g->graph);
   if (ce != cudaSuccess) {

@@ -112,7 +112,7 @@ class GaqQueue final : public QueueImpl {
   ~GaqQueue() override {
     for (void* p : {(void*)arr_[0], (void*)arr_[1], (void*)pend_, (void*)pend_tmp_, (void*)hist_, (void*)scan_tmp_, (void*)idx_,
                     (void*)cnt_, (void*)out_cnt_, (void*)off_, (void*)tmp_, (void*)taken_, (void*)keep_,
-                    (void*)words_, (void*)out_})
+                    (void*)words_, (void*)out_, (void*)split_})
       if (p) cudaFree(p);
     if (h_words_) cudaFreeHost(h_words_);
     if (own_) cudaStreamDestroy(own_);
@@ -133,6 +133,7 @@ class GaqQueue final : public QueueImpl {
     GPQ_CUDA_TRY(cudaMalloc(&pend_, (size_t)pend_cap_ * sizeof(gpq_item)));
     GPQ_CUDA_TRY(cudaMalloc(&pend_tmp_, (size_t)pend_cap_ * sizeof(gpq_item)));
     GPQ_CUDA_TRY(cudaMalloc(&hist_, radix_hist_words(pend_cap_) * sizeof(uint32_t)));
+    GPQ_CUDA_TRY(cudaMalloc(&split_, merge_split_words(cap_) * sizeof(uint32_t)));
     GPQ_CUDA_TRY(cudaMalloc(&scan_tmp_, scan_scratch_words((uint64_t)std::max(cap_, L_) + 1) * sizeof(uint32_t)));
     GPQ_CUDA_TRY(cudaMalloc(&idx_, (size_t)L_ * lpcap_ * sizeof(uint32_t)));
     GPQ_CUDA_TRY(cudaMalloc(&tmp_, (size_t)L_ * lpcap_ * sizeof(gpq_item)));
@@ -177,14 +178,21 @@ class GaqQueue final : public QueueImpl {
     GPQ_CUDA_TRY(cudaMemcpyAsync(h_words_, words_, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     GPQ_CUDA_TRY(cudaStreamSynchronize(st));
     gpq_item* sorted = nullptr;
-    gpq_status s = radix_sort_by_ts(pend_, pend_tmp_, npend_, h_words_[0], h_words_[1], hist_, &sorted, st);
+    gpq_status s = radix_sort_by_ts(pend_, pend_tmp_, npend_, h_words_[0], h_words_[1], hist_, &sorted,
+                                    words_ + kBulkErrWord, st);
     if (s != GPQ_OK) return s;
-    s = merge_by_ts(arr_[cur_], n_, sorted, npend_, arr_[cur_ ^ 1], st);
+    s = merge_by_ts(arr_[cur_], n_, sorted, npend_, arr_[cur_ ^ 1], split_, words_ + kBulkErrWord, st);
     if (s != GPQ_OK) return s;
     cur_ ^= 1;
     n_ += npend_;
     npend_ = 0;
+    uint32_t berr = 0;
+    GPQ_CUDA_TRY(cudaMemcpyAsync(&berr, words_ + kBulkErrWord, 4, cudaMemcpyDeviceToHost, st));
     GPQ_CUDA_TRY(cudaStreamSynchronize(st));
+    if (berr) {
+      set_last_error("global array queue: a staged sort or merge tile did not arrive in time");
+      return (gpq_status)berr;
+    }
     return GPQ_OK;
   }
 
@@ -310,7 +318,9 @@ class GaqQueue final : public QueueImpl {
   gpq_item* tmp_ = nullptr;
   uint32_t* taken_ = nullptr;
   uint32_t* keep_ = nullptr;
-  uint32_t* words_ = nullptr;
+  uint32_t* words_ = nullptr;  // [16] scratch words; [kBulkErrWord] the sort/merge staging error
+  static constexpr uint32_t kBulkErrWord = 15;
+  uint32_t* split_ = nullptr;  // merge-path splits of the post's merge
   uint32_t* h_words_ = nullptr;
   gpq_item* out_ = nullptr;
   uint32_t out_n_ = 0;

@@ -318,7 +318,8 @@ gpq_status gpq_phold_populate(gpq_phold* h, const gpq_item* initial, uint64_t n,
     GPQ_CUDA_TRY(cudaMemcpyAsync(hmm, h->hq_mm, sizeof(hmm), cudaMemcpyDeviceToHost, st));
     GPQ_CUDA_TRY(cudaStreamSynchronize(st));
     gpq_item* sorted = nullptr;
-    gpq_status ss = gpq::radix_sort_by_ts(h->hq_sort[0], h->hq_sort[1], N, hmm[0], hmm[1], h->hq_hist, &sorted, st);
+    gpq_status ss = gpq::radix_sort_by_ts(h->hq_sort[0], h->hq_sort[1], N, hmm[0], hmm[1], h->hq_hist, &sorted,
+                                          &h->ctrl->err, st);
     if (ss != GPQ_OK) return ss;
     // The sorted population laid out in level order is a valid heap of full nodes.
     GPQ_CUDA_TRY(cudaMemcpyAsync(h->hq.nodes, sorted, (size_t)N * sizeof(gpq_item), cudaMemcpyDeviceToDevice, st));
