@@ -1,0 +1,815 @@
+// Parallel heap queue with large nodes, worked by the whole GPU (PHOLD engine, node sizes
+// above the one-CTA limit kHqMaxR).
+//
+// Reference: src/heap_queue.cu merges a root of HQ_NODE_SIZE items (256 K by default,
+// src/config.h:88) with moderngpu over the whole GPU, node by node, driven from host
+// threads (:1541-1553, :1609-1774).  Here the heap keeps the layout and the operations of
+// hq.cuh -- sorted r-item nodes with max(parent) <= min(child), insert-update pieces along
+// root-to-target paths, the root's safe prefix in batches, copy-last and delete-update --
+// inside one persistent cooperative launch over every SM:
+//   * merges are tiled: a CTA takes kHqgTile outputs, finds where they start and end in
+//     both inputs with a block-wide search (each round probes 384 positions at once, so a
+//     split costs three or four global round trips, not twenty), stages both input slices
+//     in shared memory and merges kHqgIpt outputs per thread there;
+//   * sorts are a block merge sort per chunk (a sorting network in registers, then
+//     merge rounds in shared memory) followed by tiled merge rounds over the chunks;
+//   * the heap's control state (root buffer and offset, root count, last node and its
+//     count: every node between the root and the last one is full) lives in registers of
+//     every thread, and every block takes each decision itself from data that no block
+//     writes in the same phase, so phases are separated by data barriers only;
+//   * the root has two buffers and an offset: a batch's removal advances the offset, and
+//     every merge into the root writes the other buffer;
+//   * the refill takes the largest items of the last node(s) -- suffixes of sorted nodes,
+//     so one merge of at most two runs replaces a sort.
+// A batch's per-LP ranks (the order-sensitive hash needs each event's position in its
+// LP's sequence) come from a sort of (lp, position) keys: an event's rank is its LP's
+// count so far plus its distance from the first key of its LP.
+#pragma once
+
+#include "hq.cuh"
+
+static constexpr uint32_t kHqgThreads = 768;
+static constexpr uint32_t kHqgIpt = 8;                          // items per thread (sorts, merges)
+static constexpr uint32_t kHqgTile = kHqgThreads * kHqgIpt;     // 6,144 items per CTA tile
+static constexpr uint32_t kHqgKpt = 16;                         // keys per thread
+static constexpr uint32_t kHqgKeyTile = kHqgThreads * kHqgKpt;  // 12,288 keys per CTA tile
+static constexpr uint32_t kHqgMaxR = 1u << 22;                  // node size limit of the grid form
+
+// Shared-memory tiles are padded by one element per kPer (a thread's run), so that a
+// thread's kPer consecutive elements and its neighbours' fall in different banks.
+__host__ __device__ inline size_t hqg_smem_bytes() {
+  return 2 * (size_t)(kHqgTile + kHqgTile / kHqgIpt) * sizeof(gpq_item);
+}
+
+struct HqgItemOps {
+  using T = gpq_item;
+  static constexpr uint32_t kPer = kHqgIpt;
+  static __device__ __forceinline__ bool less(const T& a, const T& b) { return hq_less(a, b); }
+  static __device__ __forceinline__ T maxv() { return hq_max_item(); }
+};
+
+struct HqgKeyOps {
+  using T = unsigned long long;
+  static constexpr uint32_t kPer = kHqgKpt;
+  static __device__ __forceinline__ bool less(T a, T b) { return a < b; }
+  static __device__ __forceinline__ T maxv() { return ~0ull; }
+};
+
+template <class Ops>
+__device__ __forceinline__ uint32_t hqg_pad(uint32_t j) { return j + j / Ops::kPer; }
+template <class Ops>
+__host__ __device__ constexpr uint32_t hqg_tile_cap() { return kHqgThreads * (Ops::kPer + 1); }
+
+struct HqgDev {
+  HqDev h;
+  gpq_item* root2;          // [r] the root's second buffer
+  gpq_item* t0;             // [2r] merge output of a non-root node / delete-update
+  gpq_item* t1;             // [3r] delete-update
+  gpq_item* pa;             // [r] insert pieces (alternating)
+  gpq_item* pb;             // [r]
+  gpq_item* e2;             // [population] sort scratch of the children
+  gpq_item* bref;           // [r] refill: the two suffixes merged
+  unsigned long long* k0;   // [r] (lp, position) keys of a batch
+  unsigned long long* k1;   // [r]
+  uint32_t* rank;           // [r] an event's position in its LP's sequence
+  uint32_t* addc;           // [r] run length at the last event of an LP's run, else 0
+  uint32_t* ovf;            // bucket overflows of the one-phase paths (zeroed per launch)
+};
+
+struct HqgSync {
+  const PholdDev* d;
+  unsigned long long target;
+  bool ok;
+};
+
+__device__ __forceinline__ bool hqg_bar(HqgSync& s) {
+  s.target += gridDim.x;
+  if (s.ok && !grid_barrier(&s.d->ctrl->bar, s.target, s.d->spin_limit, &s.d->ctrl->err)) s.ok = false;
+  return s.ok;
+}
+
+__device__ __forceinline__ uint32_t hqg_tid() { return blockIdx.x * blockDim.x + threadIdx.x; }
+__device__ __forceinline__ uint32_t hqg_nthreads() { return gridDim.x * blockDim.x; }
+
+// ---------------------------------------------------------------------------------------
+// Block-wide searches.
+
+// First i in [lo, hi) with pred(i) true (pred monotone: false ... false true ... true), or
+// hi; every thread of the block gets the answer.  Each round probes blockDim.x positions.
+template <class Pred>
+__device__ uint32_t hqg_cta_search(uint32_t lo, uint32_t hi, Pred pred) {
+  __shared__ uint32_t s_lo, s_hi, s_first;
+  if (threadIdx.x == 0) { s_lo = lo; s_hi = hi; }
+  __syncthreads();
+  const uint32_t m = blockDim.x, k = threadIdx.x;
+  for (;;) {
+    const uint32_t l = s_lo, h = s_hi;
+    if (l >= h) break;
+    if (k == 0) s_first = m;
+    __syncthreads();
+    const uint32_t i = l + (uint32_t)(((uint64_t)(h - l) * (k + 1)) / (m + 1));
+    if (pred(i)) atomicMin(&s_first, k);
+    __syncthreads();
+    if (k == 0) {
+      const uint32_t f = s_first;
+      s_lo = f > 0 ? l + (uint32_t)(((uint64_t)(h - l) * f) / (m + 1)) + 1 : l;
+      s_hi = f < m ? l + (uint32_t)(((uint64_t)(h - l) * (f + 1)) / (m + 1)) : h;
+    }
+    __syncthreads();
+  }
+  const uint32_t r = s_lo;
+  __syncthreads();
+  return r;
+}
+
+// Merge-path splits of diagonals d0 and d1 of merge(A, B) (A first on ties): the number
+// of A items among the first d outputs.  Two halves of the block search one each.
+template <class Ops>
+__device__ void hqg_cta_split2(const typename Ops::T* A, uint32_t na, const typename Ops::T* B, uint32_t nb,
+                               uint32_t d0, uint32_t d1, uint32_t* x0, uint32_t* x1) {
+  __shared__ uint32_t s_lo[2], s_hi[2], s_first[2];
+  const uint32_t half = blockDim.x >> 1;
+  const uint32_t which = threadIdx.x >= half ? 1u : 0u, k = threadIdx.x - which * half;
+  const uint32_t d = which ? d1 : d0;
+  if (k == 0) {
+    s_lo[which] = d > nb ? d - nb : 0u;
+    s_hi[which] = min(d, na);
+  }
+  __syncthreads();
+  for (;;) {
+    const uint32_t l = s_lo[which], h = s_hi[which];
+    if (s_lo[0] >= s_hi[0] && s_lo[1] >= s_hi[1]) break;
+    if (k == 0) s_first[which] = half;
+    __syncthreads();
+    if (l < h) {
+      const uint32_t i = l + (uint32_t)(((uint64_t)(h - l) * (k + 1)) / (half + 1));
+      if (Ops::less(B[d - 1 - i], A[i])) atomicMin(&s_first[which], k);
+    }
+    __syncthreads();
+    if (k == 0 && l < h) {
+      const uint32_t f = s_first[which];
+      s_lo[which] = f > 0 ? l + (uint32_t)(((uint64_t)(h - l) * f) / (half + 1)) + 1 : l;
+      s_hi[which] = f < half ? l + (uint32_t)(((uint64_t)(h - l) * (f + 1)) / (half + 1)) : h;
+    }
+    __syncthreads();
+  }
+  *x0 = s_lo[0];
+  *x1 = s_lo[1];
+  __syncthreads();
+}
+
+// Merge-path split of diagonal `diag` of merge(A, B) with A = XA[aoff, aoff + na) and
+// B = XB[boff, boff + nb), both in padded shared-memory tiles.
+template <class Ops>
+__device__ __forceinline__ uint32_t hqg_split(const typename Ops::T* XA, uint32_t aoff, uint32_t na,
+                                              const typename Ops::T* XB, uint32_t boff, uint32_t nb, uint32_t diag) {
+  uint32_t lo = diag > nb ? diag - nb : 0u, hi = min(diag, na);
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (!Ops::less(XB[hqg_pad<Ops>(boff + diag - 1 - mid)], XA[hqg_pad<Ops>(aoff + mid)])) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+// Outputs [dg, dg + kPer) of merge(A, B) (A, B as above; fewer at the end) to out(k, v),
+// k = 0, 1, ...  The two heads are kept in registers: one shared-memory load per output.
+template <class Ops, class Out>
+__device__ __forceinline__ void hqg_merge_run(const typename Ops::T* XA, uint32_t aoff, uint32_t na,
+                                              const typename Ops::T* XB, uint32_t boff, uint32_t nb, uint32_t dg,
+                                              Out out) {
+  using T = typename Ops::T;
+  uint32_t ia = hqg_split<Ops>(XA, aoff, na, XB, boff, nb, dg), ib = dg - ia;
+  T a = ia < na ? XA[hqg_pad<Ops>(aoff + ia)] : Ops::maxv();
+  T b = ib < nb ? XB[hqg_pad<Ops>(boff + ib)] : Ops::maxv();
+  const uint32_t n = min(Ops::kPer, na + nb - dg);
+  for (uint32_t k = 0; k < n; ++k) {
+    const bool take_a = ib >= nb || (ia < na && !Ops::less(b, a));
+    if (take_a) {
+      out(k, a);
+      if (++ia < na) a = XA[hqg_pad<Ops>(aoff + ia)];
+    } else {
+      out(k, b);
+      if (++ib < nb) b = XB[hqg_pad<Ops>(boff + ib)];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Tiled merge: one CTA produces outputs [d0, d1) of merge(A, B) through out(o, v); sa and
+// sb are two padded tiles.
+
+template <class Ops, class Out>
+__device__ void hqg_merge_tile(const typename Ops::T* A, uint32_t na, const typename Ops::T* B, uint32_t nb,
+                               uint32_t d0, uint32_t d1, typename Ops::T* sa, typename Ops::T* sb, Out out) {
+  uint32_t a0, a1;
+  hqg_cta_split2<Ops>(A, na, B, nb, d0, d1, &a0, &a1);
+  const uint32_t la = a1 - a0, lb = (d1 - a1) - (d0 - a0), b0 = d0 - a0, n = la + lb;
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) sa[hqg_pad<Ops>(i)] = i < la ? A[a0 + i] : B[b0 + i - la];
+  __syncthreads();
+  const uint32_t ld = threadIdx.x * Ops::kPer;
+  if (ld < n)
+    hqg_merge_run<Ops>(sa, 0, la, sa, la, lb, ld, [&](uint32_t k, const typename Ops::T& v) { sb[hqg_pad<Ops>(ld + k)] = v; });
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) out(d0 + i, sb[hqg_pad<Ops>(i)]);
+}
+
+// out(o, v) for every output of merge(A, B); all CTAs; ends with a barrier.
+template <class Ops, class Out>
+__device__ void hqg_merge(const typename Ops::T* A, uint32_t na, const typename Ops::T* B, uint32_t nb,
+                          unsigned char* smem, HqgSync& s, Out out) {
+  constexpr uint32_t tile = kHqgThreads * Ops::kPer;
+  typename Ops::T* sa = reinterpret_cast<typename Ops::T*>(smem);
+  typename Ops::T* sb = sa + hqg_tile_cap<Ops>();
+  const uint32_t total = na + nb;
+  for (uint32_t t = blockIdx.x; t * tile < total; t += gridDim.x)
+    hqg_merge_tile<Ops>(A, na, B, nb, t * tile, min(t * tile + tile, total), sa, sb, out);
+  hqg_bar(s);
+}
+
+struct HqgStore {
+  gpq_item* p;
+  __device__ __forceinline__ void operator()(uint32_t o, const gpq_item& v) const { p[o] = v; }
+};
+
+// The first `n` outputs to p, the rest to q.
+struct HqgStore2 {
+  gpq_item* p;
+  gpq_item* q;
+  uint32_t n;
+  __device__ __forceinline__ void operator()(uint32_t o, const gpq_item& v) const {
+    if (o < n) p[o] = v; else q[o - n] = v;
+  }
+};
+
+// ---------------------------------------------------------------------------------------
+// Sorts.
+
+// Odd-even transposition network over kPer values in registers.
+template <class Ops>
+__device__ __forceinline__ void hqg_reg_sort(typename Ops::T (&v)[Ops::kPer]) {
+#pragma unroll
+  for (uint32_t r = 0; r < Ops::kPer; ++r) {
+#pragma unroll
+    for (uint32_t i = r & 1u; i + 1 < Ops::kPer; i += 2) {
+      if (Ops::less(v[i + 1], v[i])) {
+        const typename Ops::T x = v[i];
+        v[i] = v[i + 1];
+        v[i + 1] = x;
+      }
+    }
+  }
+}
+
+static constexpr uint32_t kHqgRankSortMax = 512;
+
+// Block merge sort of the padded tile sa holding n values (n <= kThreads * kPer; sb is a
+// second padded tile).  Returns the tile that holds the sorted values in [0, n).  Up to
+// kHqgRankSortMax values (all distinct, as items and (lp, position) keys are) are placed
+// by rank instead: each thread counts the values below its own, reading the tile in step
+// with the other threads (broadcast reads), one pass without dependent rounds.
+template <class Ops>
+__device__ typename Ops::T* hqg_cta_sort(typename Ops::T* sa, typename Ops::T* sb, uint32_t n) {
+  using T = typename Ops::T;
+  constexpr uint32_t P = Ops::kPer;
+  if (n <= kHqgRankSortMax) {
+    if (threadIdx.x < n) {
+      const T x = sa[hqg_pad<Ops>(threadIdx.x)];
+      uint32_t rk = 0;
+      for (uint32_t j = 0; j < n; ++j) rk += Ops::less(sa[hqg_pad<Ops>(j)], x) ? 1u : 0u;
+      sb[hqg_pad<Ops>(rk)] = x;
+    }
+    __syncthreads();
+    return sb;
+  }
+  const uint32_t nn = (n + P - 1) / P * P;
+  const uint32_t b = threadIdx.x * P;
+  if (b < nn) {
+    T v[P];
+#pragma unroll
+    for (uint32_t k = 0; k < P; ++k) v[k] = (b + k < n) ? sa[hqg_pad<Ops>(b + k)] : Ops::maxv();
+    hqg_reg_sort<Ops>(v);
+#pragma unroll
+    for (uint32_t k = 0; k < P; ++k) sa[hqg_pad<Ops>(b + k)] = v[k];
+  }
+  __syncthreads();
+  for (uint32_t w = P; w < nn; w <<= 1) {
+    if (b < nn) {
+      const uint32_t p0 = b / (2 * w) * (2 * w);
+      const uint32_t na = min(w, nn - p0), nb = min(w, nn - p0 - na);
+      hqg_merge_run<Ops>(sa, p0, na, sa, p0 + na, nb, b - p0, [&](uint32_t k, const T& v) { sb[hqg_pad<Ops>(b + k)] = v; });
+    }
+    __syncthreads();
+    T* x = sa;
+    sa = sb;
+    sb = x;
+  }
+  return sa;
+}
+
+// Sorts n values, value j given by load(j), into buf (tmp: scratch of n); all CTAs.
+// Returns the buffer holding the result; ends with a barrier.
+template <class Ops, class Load>
+__device__ typename Ops::T* hqg_sort(typename Ops::T* buf, typename Ops::T* tmp, uint32_t n, unsigned char* smem,
+                                     HqgSync& s, Load load) {
+  using T = typename Ops::T;
+  constexpr uint32_t tile = kHqgThreads * Ops::kPer;
+  T* sa = reinterpret_cast<T*>(smem);
+  T* sb = sa + hqg_tile_cap<Ops>();
+  for (uint32_t c = blockIdx.x; c * tile < n; c += gridDim.x) {
+    const uint32_t c0 = c * tile, cn = min(tile, n - c0);
+    for (uint32_t i = threadIdx.x; i < cn; i += blockDim.x) sa[hqg_pad<Ops>(i)] = load(c0 + i);
+    __syncthreads();
+    const T* sorted = hqg_cta_sort<Ops>(sa, sb, cn);
+    for (uint32_t i = threadIdx.x; i < cn; i += blockDim.x) buf[c0 + i] = sorted[hqg_pad<Ops>(i)];
+    __syncthreads();
+  }
+  hqg_bar(s);
+  for (uint32_t w = tile; w < n; w <<= 1) {  // runs of w into runs of 2w, tile by tile
+    for (uint32_t t = blockIdx.x; t * tile < n; t += gridDim.x) {
+      const uint32_t o0 = t * tile, p0 = o0 / (2 * w) * (2 * w);
+      const uint32_t na = min(w, n - p0), nb = min(w, n - p0 - na);
+      const uint32_t d0 = o0 - p0, d1 = min(d0 + tile, na + nb);
+      hqg_merge_tile<Ops>(buf + p0, na, buf + p0 + na, nb, d0, d1, sa, sb,
+                          [&](uint32_t o, const T& v) { tmp[p0 + o] = v; });
+      __syncthreads();
+    }
+    hqg_bar(s);
+    T* x = buf;
+    buf = tmp;
+    tmp = x;
+  }
+  return buf;
+}
+
+// ---------------------------------------------------------------------------------------
+// The heap's control state, the same in every thread of the grid.
+
+struct HqgState {
+  gpq_item* root;   // buffer holding the root
+  gpq_item* spare;  // the root's other buffer
+  uint32_t off;     // first live item of the root
+  uint32_t cnt0;    // live items of the root
+  uint32_t last;    // last non-empty node
+  uint32_t cntl;    // items of node `last` (last > 0)
+  __device__ __forceinline__ uint32_t cnt(uint32_t p, uint32_t r) const {
+    return p == 0 ? cnt0 : (p == last ? cntl : r);
+  }
+  __device__ __forceinline__ void swap_root() {
+    gpq_item* x = root;
+    root = spare;
+    spare = x;
+    off = 0;
+  }
+};
+
+__device__ __forceinline__ gpq_item* hqg_node(const HqgDev& g, const HqgState& q, uint32_t p) {
+  return p == 0 ? q.root + q.off : g.h.nodes + (size_t)p * g.h.r;
+}
+
+__device__ __forceinline__ void hqg_copy(gpq_item* dst, const gpq_item* src, uint32_t n, HqgSync& s) {
+  for (uint32_t i = hqg_tid(); i < n; i += hqg_nthreads()) dst[i] = src[i];
+  hqg_bar(s);
+}
+
+// Inserts the sorted items src[0, k) (insert-update pieces: each piece fills the last
+// node or a new one and walks the root-to-target path, every full ancestor keeping the
+// smallest r).  Returns false if the heap ran out of nodes (error recorded) or a barrier
+// failed.
+__device__ bool hqg_insert(const PholdDev& d, const HqgDev& g, HqgState& q, const gpq_item* src, uint32_t k,
+                           unsigned char* smem, HqgSync& s) {
+  const uint32_t r = g.h.r;
+  uint32_t done = 0;
+  while (done < k) {
+    uint32_t tgt = q.last;
+    if (q.cnt(q.last, r) == r) {
+      tgt = q.last + 1;
+      if (tgt >= g.h.maxnodes) {
+        if (hqg_tid() == 0) gpq_set_error(&d.ctrl->err, GPQ_ERR_QUEUE_FULL);
+        return false;
+      }
+      q.last = tgt;
+      q.cntl = 0;
+    }
+    const uint32_t nt = q.cnt(tgt, r), px = min(k - done, r - nt);
+    uint32_t depth = 0;
+    while (((tgt + 1) >> (depth + 1)) != 0) ++depth;
+    const gpq_item* piece = src + done;
+    bool use_a = true;
+    for (uint32_t l = 0; l < depth; ++l) {  // full ancestors on the path
+      const uint32_t p = ((tgt + 1) >> (depth - l)) - 1;
+      gpq_item* pout = use_a ? g.pa : g.pb;
+      use_a = !use_a;
+      if (p == 0) {
+        hqg_merge<HqgItemOps>(q.root + q.off, r, piece, px, smem, s, HqgStore2{q.spare, pout, r});
+        q.swap_root();
+      } else {
+        gpq_item* node = g.h.nodes + (size_t)p * r;
+        hqg_merge<HqgItemOps>(node, r, piece, px, smem, s, HqgStore2{g.t0, pout, r});
+        hqg_copy(node, g.t0, r, s);
+      }
+      piece = pout;
+    }
+    if (tgt == 0) {
+      hqg_merge<HqgItemOps>(q.root + q.off, nt, piece, px, smem, s, HqgStore{q.spare});
+      q.swap_root();
+      q.cnt0 = nt + px;
+    } else {
+      gpq_item* node = g.h.nodes + (size_t)tgt * r;
+      hqg_merge<HqgItemOps>(node, nt, piece, px, smem, s, HqgStore{g.t0});
+      hqg_copy(node, g.t0, nt + px, s);
+      q.cntl = nt + px;
+    }
+    done += px;
+    if (!s.ok) return false;
+  }
+  return true;
+}
+
+// After a batch: refill the root from the largest items of the last nodes (copy-last) and
+// restore the order along one path (delete-update).  Returns false if a barrier failed.
+__device__ bool hqg_refill(const HqgDev& g, HqgState& q, unsigned char* smem, HqgSync& s) {
+  const uint32_t r = g.h.r;
+  if (q.last == 0) return true;  // the root holds every item
+  const uint32_t keep = q.cnt0, want = r - keep;
+  // The taken items are suffixes of one or two sorted nodes: node `last` (cntl items) and,
+  // if it runs out, the full node before it (never the root).
+  const uint32_t l1 = q.last, n1 = q.cntl, t1 = min(want, n1);
+  const gpq_item* s1 = g.h.nodes + (size_t)l1 * r + (n1 - t1);
+  q.cntl = n1 - t1;
+  if (q.cntl == 0) {
+    q.last = l1 - 1;
+    q.cntl = r;
+  }
+  uint32_t t2 = 0;
+  const gpq_item* s2 = nullptr;
+  if (t1 < want && q.last > 0) {
+    t2 = want - t1;  // <= r: node last - 1 is full
+    s2 = g.h.nodes + (size_t)q.last * r + (r - t2);
+    q.cntl = r - t2;
+    if (q.cntl == 0) {
+      q.last -= 1;
+      q.cntl = r;
+    }
+  }
+  const gpq_item* run = s1;
+  if (t2 > 0) {
+    hqg_merge<HqgItemOps>(s1, t1, s2, t2, smem, s, HqgStore{g.bref});
+    run = g.bref;
+  }
+  hqg_merge<HqgItemOps>(q.root + q.off, keep, run, t1 + t2, smem, s, HqgStore{q.spare});
+  q.swap_root();
+  q.cnt0 = keep + t1 + t2;
+  if (q.last == 0) q.cntl = 0;
+  // delete-update
+  uint32_t p = 0;
+  while (s.ok) {
+    const uint32_t c1 = 2 * p + 1, c2 = 2 * p + 2;
+    const uint32_t np = q.cnt(p, r);
+    const uint32_t m1 = (c1 <= q.last) ? q.cnt(c1, r) : 0u;
+    const uint32_t m2 = (c2 <= q.last) ? q.cnt(c2, r) : 0u;
+    if (np == 0 || (m1 == 0 && m2 == 0)) break;
+    const gpq_item* P = hqg_node(g, q, p);
+    const gpq_item* C1 = g.h.nodes + (size_t)c1 * r;
+    const gpq_item* C2 = g.h.nodes + (size_t)c2 * r;
+    const gpq_item pmax = P[np - 1];
+    const bool ok1 = m1 == 0 || hq_less(pmax, C1[0]);
+    const bool ok2 = m2 == 0 || hq_less(pmax, C2[0]);
+    if (ok1 && ok2) break;
+    // The child with the larger old maximum (or a partial c2, the last node) takes the
+    // middle items, the other one the largest, and the walk continues there
+    // (delete_update_post, src/heap_queue.cu:728-784).
+    uint32_t mid, lrg;
+    if (m2 == 0) {
+      mid = lrg = c1;
+    } else if (m1 == 0) {
+      mid = lrg = c2;
+    } else {
+      const bool mid2 = m2 < r || hq_less(C1[m1 - 1], C2[m2 - 1]);
+      mid = mid2 ? c2 : c1;
+      lrg = mid2 ? c1 : c2;
+    }
+    hqg_merge<HqgItemOps>(P, np, C1, m1, smem, s, HqgStore{g.t0});
+    hqg_merge<HqgItemOps>(g.t0, np + m1, C2, m2, smem, s, HqgStore{g.t1});
+    const uint32_t nmid = (mid == c1) ? m1 : m2;
+    gpq_item* Pw = hqg_node(g, q, p);
+    gpq_item* Mw = g.h.nodes + (size_t)mid * r;
+    gpq_item* Lw = g.h.nodes + (size_t)lrg * r;
+    for (uint32_t i = hqg_tid(); i < np + m1 + m2; i += hqg_nthreads()) {
+      const gpq_item v = g.t1[i];
+      if (i < np) Pw[i] = v;
+      else if (i < np + nmid) Mw[i - np] = v;
+      else Lw[i - np - nmid] = v;
+    }
+    hqg_bar(s);
+    p = lrg;
+  }
+  return s.ok;
+}
+
+// ---------------------------------------------------------------------------------------
+// Per-LP ranks of a batch.
+
+// Positions [t0, t0 + tn) of the sorted keys K[0, n) (staged in sk): rank[i] = count[lp]
+// + p - (first position of lp's run) and addc[i] = run length at the run's last key.
+// gseg = first position of the run holding position t0.
+// sk is a padded shared-memory tile.
+__device__ void hqg_rank_tile(const PholdDev& d, const HqgDev& g, const unsigned long long* sk, uint32_t t0,
+                              uint32_t tn, uint32_t n, uint32_t gseg, const unsigned long long* K) {
+  auto at = [sk](uint32_t j) { return sk[hqg_pad<HqgKeyOps>(j)]; };
+  const uint32_t lp0 = (uint32_t)(at(0) >> 32);
+  for (uint32_t j = threadIdx.x; j < tn; j += blockDim.x) {
+    const unsigned long long key = at(j);
+    const uint32_t lp = (uint32_t)(key >> 32), i = (uint32_t)key;
+    uint32_t seg;
+    if (lp == lp0) {
+      seg = gseg;
+    } else {
+      const unsigned long long lo_key = (unsigned long long)lp << 32;
+      uint32_t lo = 0, hi = j;
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (at(mid) < lo_key) lo = mid + 1; else hi = mid;
+      }
+      seg = t0 + lo;
+    }
+    const uint32_t p = t0 + j;
+    g.rank[i] = d.count[lp] + (p - seg);
+    const uint64_t nxt = (j + 1 < tn) ? at(j + 1) : (p + 1 < n ? K[p + 1] : ~0ull);
+    g.addc[i] = ((uint32_t)(nxt >> 32) != lp || p + 1 == n) ? p - seg + 1 : 0u;
+  }
+}
+
+// Ranks of the c events root[0, c); ends with a barrier.
+__device__ void hqg_ranks(const PholdDev& d, const HqgDev& g, const gpq_item* root, uint32_t c, unsigned char* smem,
+                          HqgSync& s) {
+  auto load = [root](uint32_t j) { return ((unsigned long long)root[j].lp << 32) | j; };
+  unsigned long long* sa = reinterpret_cast<unsigned long long*>(smem);
+  if (c <= kHqgKeyTile) {  // one CTA sorts and ranks the whole batch
+    if (blockIdx.x == gridDim.x - 1) {
+      for (uint32_t j = threadIdx.x; j < c; j += blockDim.x) sa[hqg_pad<HqgKeyOps>(j)] = load(j);
+      __syncthreads();
+      const unsigned long long* sk = hqg_cta_sort<HqgKeyOps>(sa, sa + hqg_tile_cap<HqgKeyOps>(), c);
+      hqg_rank_tile(d, g, sk, 0, c, c, 0, nullptr);
+      __syncthreads();
+    }
+    hqg_bar(s);
+    return;
+  }
+  const unsigned long long* K = hqg_sort<HqgKeyOps>(g.k0, g.k1, c, smem, s, load);
+  for (uint32_t t = blockIdx.x; t * kHqgKeyTile < c; t += gridDim.x) {
+    const uint32_t t0 = t * kHqgKeyTile, tn = min(kHqgKeyTile, c - t0);
+    for (uint32_t j = threadIdx.x; j < tn; j += blockDim.x) sa[hqg_pad<HqgKeyOps>(j)] = K[t0 + j];
+    __syncthreads();
+    const unsigned long long lo_key = sa[0] & 0xffffffff00000000ull;
+    const uint32_t gseg = hqg_cta_search(0, t0, [K, lo_key](uint32_t i) { return K[i] >= lo_key; });
+    hqg_rank_tile(d, g, sa, t0, tn, c, gseg, K);
+    __syncthreads();
+  }
+  hqg_bar(s);
+}
+
+// ---------------------------------------------------------------------------------------
+// One-phase paths for small windows.  Buckets whose contents one CTA holds in shared
+// memory replace the sorts: each CTA scans the whole input and keeps its bucket's share.
+
+static constexpr uint32_t kHqgScanMax = 32768;  // children a one-phase insert scans
+static constexpr uint32_t kHqgScanPer = 128;    // items per bucket aimed at
+
+// visit(i, v, i < n) for i in [0, n) rounded up, v = load(i) (a zero value past n), every
+// thread of the CTA with all lanes of each warp together (visit may use warp
+// collectives); U loads in flight per thread.
+template <uint32_t U, class Load, class Visit>
+__device__ __forceinline__ void hqg_cta_scan(uint32_t n, Load load, Visit visit) {
+  using V = decltype(load(0u));
+  for (uint32_t base = 0; base < n; base += blockDim.x * U) {
+    V x[U];
+#pragma unroll
+    for (uint32_t u = 0; u < U; ++u) {
+      const uint32_t i = base + u * blockDim.x + threadIdx.x;
+      x[u] = (i < n) ? load(i) : V{};
+    }
+#pragma unroll
+    for (uint32_t u = 0; u < U; ++u) {
+      const uint32_t i = base + u * blockDim.x + threadIdx.x;
+      visit(i, x[u], i < n);
+    }
+  }
+}
+
+// A slot of a shared-memory counter for every lane with `take` set, one atomic per warp.
+__device__ __forceinline__ uint32_t hqg_warp_slot(uint32_t* ctr, bool take) {
+  const uint32_t m = __ballot_sync(GPQ_FULL_MASK, take);
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t leader = m != 0u ? (uint32_t)(__ffs(m) - 1) : 0u;
+  uint32_t b = 0;
+  if (m != 0u && lane == leader) b = atomicAdd(ctr, (uint32_t)__popc(m));
+  b = __shfl_sync(GPQ_FULL_MASK, b, (int)leader);
+  return b + __popc(m & ((1u << lane) - 1u));
+}
+
+// Buckets of the one-phase insert into a root of nr items with nch children (0 = the
+// general path).
+__device__ __forceinline__ uint32_t hqg_insert_buckets(const HqgState& q, uint32_t r, uint32_t nch) {
+  const uint32_t nr = q.cnt0, total = nr + nch;
+  if (q.last != 0 || total > r || nch > kHqgScanMax) return 0;
+  uint32_t B = min(gridDim.x, max(1u, total / kHqgScanPer));
+  if (nr < B) B = max(1u, nr);
+  return (nr / B + 1 <= kHqgTile) ? B : 0u;
+}
+
+// The children C[0, nch) into a heap whose root holds every item and has room for them:
+// the new root is R u C (R = the root's items) in one phase.  The splitters are R's
+// quantiles (R is sorted): bucket b holds R's b-th slice and the children from that
+// slice's first item up to the next slice's first item.  CTA b collects its children by
+// scanning all of them, sorts them in shared memory, merges them with its slice and
+// writes the result at (slice start + children below the slice) of the root's other
+// buffer.  Returns false when a bucket overflowed shared memory (the heap is unchanged;
+// the caller takes the general path) or a barrier failed.
+__device__ bool hqg_insert_scan(const HqgDev& g, HqgState& q, const gpq_item* C, uint32_t nch, uint32_t B,
+                                unsigned char* smem, HqgSync& s, uint32_t& ovf_seen) {
+  const gpq_item* R = q.root + q.off;
+  const uint32_t nr = q.cnt0;
+  gpq_item* sa = reinterpret_cast<gpq_item*>(smem);
+  gpq_item* sb = sa + hqg_tile_cap<HqgItemOps>();
+  __shared__ uint32_t s_nc, s_below;
+  for (uint32_t b = blockIdx.x; b < B; b += gridDim.x) {
+    const uint32_t r0 = (uint32_t)((uint64_t)b * nr / B), r1 = (uint32_t)((uint64_t)(b + 1) * nr / B);
+    const bool has_lo = b > 0, has_hi = b + 1 < B;
+    const gpq_item lo = has_lo ? R[r0] : hq_max_item(), hi = has_hi ? R[r1] : hq_max_item();
+    if (threadIdx.x == 0) {
+      s_nc = 0;
+      s_below = 0;
+    }
+    __syncthreads();
+    uint32_t below = 0;
+    hqg_cta_scan<4>(nch, [C](uint32_t i) { return C[i]; }, [&](uint32_t, const gpq_item& x, bool valid) {
+      const bool lo_ok = valid && !(has_lo && hq_less(x, lo));
+      below += (valid && !lo_ok) ? 1u : 0u;
+      const bool take = lo_ok && (!has_hi || hq_less(x, hi));
+      const uint32_t slot = hqg_warp_slot(&s_nc, take);
+      if (take && slot < kHqgTile) sa[hqg_pad<HqgItemOps>(slot)] = x;
+    });
+    below = warp_sum_u32(below);
+    if ((threadIdx.x & 31u) == 0 && below) atomicAdd(&s_below, below);
+    __syncthreads();
+    const uint32_t nc = s_nc, nbw = s_below, nrb = r1 - r0;
+    if (nc > kHqgTile) {
+      if (threadIdx.x == 0) atomicAdd(g.ovf, 1u);
+      __syncthreads();
+      continue;
+    }
+    gpq_item* X = hqg_cta_sort<HqgItemOps>(sa, sb, nc);
+    gpq_item* Y = (X == sa) ? sb : sa;
+    for (uint32_t j = threadIdx.x; j < nrb; j += blockDim.x) Y[hqg_pad<HqgItemOps>(j)] = R[r0 + j];
+    __syncthreads();
+    gpq_item* dst = q.spare + r0 + nbw;
+    const uint32_t ld = threadIdx.x * kHqgIpt;
+    if (ld < nc + nrb)
+      hqg_merge_run<HqgItemOps>(Y, 0, nrb, X, 0, nc, ld, [&](uint32_t k, const gpq_item& v) { dst[ld + k] = v; });
+    __syncthreads();
+  }
+  if (!hqg_bar(s)) return false;
+  const uint32_t o = ld_relaxed_u32(g.ovf);
+  if (o != ovf_seen) {
+    ovf_seen = o;
+    return false;
+  }
+  q.swap_root();
+  q.cnt0 = nr + nch;
+  return true;
+}
+
+// A batch of c <= kHqgKeyTile events root[0, c) in one phase: LP-range buckets, so that
+// every LP's events of the batch are in one CTA, which sorts their (lp, position) keys in
+// shared memory, takes each event's rank from its run, folds the event into its LP's
+// outputs, writes its child to ch[base + position] and advances the LP's count (the LP's
+// one writer).  Ends with a barrier.
+__device__ void hqg_process_scan(const PholdDev& d, const HqgDev& g, const gpq_item* root, uint32_t c, uint32_t base,
+                                 unsigned char* smem, HqgSync& s) {
+  const uint32_t L = d.L;
+  const uint32_t B = min(gridDim.x, max(1u, c / 64u));
+  unsigned long long* sa = reinterpret_cast<unsigned long long*>(smem);
+  unsigned long long* sb = sa + hqg_tile_cap<HqgKeyOps>();
+  __shared__ uint32_t s_n;
+  for (uint32_t b = blockIdx.x; b < B; b += gridDim.x) {
+    const uint32_t lo = (uint32_t)((uint64_t)b * L / B), hi = (uint32_t)((uint64_t)(b + 1) * L / B);
+    if (threadIdx.x == 0) s_n = 0;
+    __syncthreads();
+    hqg_cta_scan<8>(c, [root](uint32_t i) { return root[i].lp; }, [&](uint32_t i, uint32_t lp, bool valid) {
+      const bool take = valid && lp >= lo && lp < hi;
+      const uint32_t slot = hqg_warp_slot(&s_n, take);
+      if (take && slot < kHqgKeyTile) sa[hqg_pad<HqgKeyOps>(slot)] = ((unsigned long long)lp << 32) | i;
+    });
+    __syncthreads();
+    uint32_t n = s_n;
+    if (n > kHqgKeyTile) {  // cannot happen (n <= c <= kHqgKeyTile); reported, not written
+      if (threadIdx.x == 0) gpq_set_error(&d.ctrl->err, GPQ_ERR_INSERT_FULL);
+      n = 0;
+    }
+    const unsigned long long* K = hqg_cta_sort<HqgKeyOps>(sa, sb, n);
+    auto seg_of = [K](uint32_t j, uint32_t lp) {
+      const unsigned long long lo_key = (unsigned long long)lp << 32;
+      uint32_t l = 0, h = j;
+      while (l < h) {
+        const uint32_t mid = (l + h) >> 1;
+        if (K[hqg_pad<HqgKeyOps>(mid)] < lo_key) l = mid + 1; else h = mid;
+      }
+      return l;
+    };
+    for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
+      const unsigned long long key = K[hqg_pad<HqgKeyOps>(j)];
+      const uint32_t lp = (uint32_t)(key >> 32), i = (uint32_t)key;
+      const gpq_item e = root[i];
+      const uint64_t hh = gpq_ev_hash(e.id, gpq_f2u(e.ts));
+      atomicAdd(&d.csum[lp], (unsigned long long)hh);
+      atomicAdd(&d.ohash[lp], (unsigned long long)gpq_seq_hash(hh, (uint64_t)d.count[lp] + (j - seg_of(j, lp))));
+      g.h.ch[base + i] = gpq_phold_child(d.p, e);
+    }
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
+      const uint32_t lp = (uint32_t)(K[hqg_pad<HqgKeyOps>(j)] >> 32);
+      if (j + 1 == n || (uint32_t)(K[hqg_pad<HqgKeyOps>(j + 1)] >> 32) != lp) d.count[lp] += j - seg_of(j, lp) + 1;
+    }
+    __syncthreads();
+  }
+  hqg_bar(s);
+}
+
+// ---------------------------------------------------------------------------------------
+// All windows of one heap (des_run over the parallel heap), the whole grid.  Per window:
+// the previous window's children sorted and inserted, the bound fixed from the root's
+// head, then batches -- the root's prefix below the bound, folded into the per-LP outputs
+// with ranks from the key sort, its children appended to h.ch, the root refilled -- until
+// the root's head reaches the bound.  The root always holds the r smallest items, so the
+// batches come in global key order; a child is never safe in its parent's window.
+static __global__ void __launch_bounds__(kHqgThreads, 1) hqg_phold_kernel(PholdDev d, HqgDev g, uint32_t max_steps) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const HqDev& h = g.h;
+  const uint32_t r = h.r;
+  HqgSync s{&d, 0ull, true};
+  HqgState q;
+  q.root = h.nodes;
+  q.spare = g.root2;
+  q.off = 0;
+  q.last = h.meta[0];
+  q.cnt0 = h.cnt[0];
+  q.cntl = q.last > 0 ? h.cnt[q.last] : 0u;
+  uint32_t steps = 0, nch = 0, ovf_seen = 0;
+  while (s.ok) {
+    if (nch > 0) {  // the previous window's children
+      const uint32_t B = hqg_insert_buckets(q, r, nch);
+      const bool done = B != 0 && hqg_insert_scan(g, q, h.ch, nch, B, smem, s, ovf_seen);
+      if (!s.ok) break;
+      if (!done) {
+        const gpq_item* ch = h.ch;
+        const gpq_item* sorted = hqg_sort<HqgItemOps>(h.ch, g.e2, nch, smem, s, [ch](uint32_t j) { return ch[j]; });
+        if (!hqg_insert(d, g, q, sorted, nch, smem, s)) break;
+      }
+      nch = 0;
+    }
+    if (q.cnt0 == 0 || (max_steps != 0 && steps >= max_steps)) break;
+    const float m = q.root[q.off].ts;
+    if (!(m < d.p.end_time)) break;
+    const uint32_t lim = min(gpq_f2u(GPQ_FADD(m, d.p.lookahead)), gpq_f2u(d.p.end_time));
+    ++steps;
+    while (s.ok) {  // batches of the window
+      const gpq_item* root = q.root + q.off;
+      const uint32_t c = hqg_cta_search(0, q.cnt0, [root, lim](uint32_t i) { return gpq_f2u(root[i].ts) >= lim; });
+      if (c == 0) break;
+      if (c <= kHqgKeyTile) {
+        hqg_process_scan(d, g, root, c, nch, smem, s);
+      } else {
+        hqg_ranks(d, g, root, c, smem, s);
+        for (uint32_t i = hqg_tid(); i < c; i += hqg_nthreads()) {
+          const gpq_item e = root[i];
+          const uint64_t hh = gpq_ev_hash(e.id, gpq_f2u(e.ts));
+          const uint32_t add = g.addc[i];
+          if (add) d.count[e.lp] += add;  // the LP's one writer in this batch
+          atomicAdd(&d.csum[e.lp], (unsigned long long)hh);
+          atomicAdd(&d.ohash[e.lp], (unsigned long long)gpq_seq_hash(hh, (uint64_t)g.rank[i]));
+          h.ch[nch + i] = gpq_phold_child(d.p, e);
+        }
+        hqg_bar(s);
+      }
+      nch += c;
+      q.off += c;
+      q.cnt0 -= c;
+      if (!hqg_refill(g, q, smem, s)) break;
+    }
+  }
+  // Leave the root in node 0's storage at offset 0 and the counts in h.cnt / h.meta.
+  if (s.ok && q.root != h.nodes) {
+    hqg_copy(h.nodes, q.root + q.off, q.cnt0, s);
+  } else if (s.ok && q.off != 0) {
+    hqg_copy(g.root2, q.root + q.off, q.cnt0, s);
+    hqg_copy(h.nodes, g.root2, q.cnt0, s);
+  }
+  if (blockIdx.x == 0) {
+    for (uint32_t i = threadIdx.x; i <= q.last; i += blockDim.x) h.cnt[i] = q.cnt(i, r);
+    if (threadIdx.x == 0) {
+      h.meta[0] = q.last;
+      h.meta[1] = steps;
+      d.ctrl->steps = steps;
+    }
+  }
+}

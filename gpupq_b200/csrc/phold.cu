@@ -15,6 +15,7 @@
 #include "phold_host.h"
 #include "gaq.cuh"
 #include "gaq_engine.h"
+#include "hq_grid.cuh"
 #include "hq_kernels.cuh"
 #include "lab.cuh"
 #include "phold_kernels.cuh"
@@ -114,8 +115,12 @@ struct gpq_phold {
   PholdKernelSet ks{};
   gpq::GaqEngine* gaq = nullptr;  // global array queue state (queue_kind == GPQ_QUEUE_GAQ)
   uint64_t gaq_windows = 0;
-  // parallel heap (queue_kind == GPQ_QUEUE_HQ): one CTA runs the heap
+  // parallel heap (queue_kind == GPQ_QUEUE_HQ): one CTA runs the heap up to node size
+  // kHqMaxR, the whole GPU (one cooperative launch) above it
   HqDev hq{};
+  HqgDev hqg{};
+  bool hq_grid = false;
+  uint32_t hqg_blocks = 0;
   gpq_item* hq_sort[2] = {nullptr, nullptr};
   uint32_t* hq_hist = nullptr;
   uint32_t* hq_mm = nullptr;
@@ -138,7 +143,9 @@ struct gpq_phold {
     if (gaq) gpq::gaq_engine_destroy(gaq);
     for (void* p : {(void*)hq.nodes, (void*)hq.cnt, (void*)hq.meta, (void*)hq_sort[0], (void*)hq_sort[1],
                     (void*)hq_hist, (void*)hq_mm, (void*)lab.keys, (void*)lab.cnt, (void*)lab.spill,
-                    (void*)lab.scnt, (void*)lab.wj})
+                    (void*)lab.scnt, (void*)lab.wj, (void*)hqg.root2, (void*)hqg.t0, (void*)hqg.t1,
+                    (void*)hqg.pa, (void*)hqg.pb, (void*)hqg.bref, (void*)hqg.k0, (void*)hqg.k1, (void*)hqg.rank,
+                    (void*)hqg.addc, (void*)hqg.ovf})
       if (p) cudaFree(p);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -187,8 +194,10 @@ gpq_status gpq_phold_create(const gpq_phold_config* cfg_in, gpq_phold** out) {
   const size_t L = c.num_lps;
   if (c.queue_kind == GPQ_QUEUE_HQ) {
     const uint32_t r = c.node_size ? c.node_size : 1024;
-    if (!gpq::is_pow2(r) || r < 2 || r > kHqMaxR || c.num_lps > (1u << 21)) {
-      gpq::set_last_error("heap queue: node_size must be a power of two in [2, %u] and num_lps <= 2^21", kHqMaxR);
+    const bool grid = r > kHqMaxR;
+    if (!gpq::is_pow2(r) || r < 2 || r > kHqgMaxR || (!grid && c.num_lps > (1u << 21))) {
+      gpq::set_last_error("heap queue: node_size must be a power of two in [2, %u] (num_lps <= 2^21 up to node "
+                          "size %u, where one CTA works the heap)", kHqgMaxR, kHqMaxR);
       return fail(GPQ_ERR_INVALID);
     }
     const uint64_t N = (uint64_t)c.num_lps * c.events_per_lp;
@@ -203,7 +212,33 @@ gpq_status gpq_phold_create(const gpq_phold_config* cfg_in, gpq_phold** out) {
     h->hq.ch = h->hq_sort[1];  // after populate: the children of a window
     TRY(cudaMalloc(&h->hq_hist, gpq::radix_hist_words((uint32_t)N) * sizeof(uint32_t)));
     TRY(cudaMalloc(&h->hq_mm, 2 * sizeof(uint32_t)));
-    TRY(gpq::raise_smem_limit(hq_phold_kernel, (int)hq_smem_bytes(r)));
+    if (grid) {
+      HqgDev& g = h->hqg;
+      h->hq_grid = true;
+      TRY(cudaMalloc(&g.root2, (size_t)r * sizeof(gpq_item)));
+      TRY(cudaMalloc(&g.t0, (size_t)2 * r * sizeof(gpq_item)));
+      TRY(cudaMalloc(&g.t1, (size_t)3 * r * sizeof(gpq_item)));
+      TRY(cudaMalloc(&g.pa, (size_t)r * sizeof(gpq_item)));
+      TRY(cudaMalloc(&g.pb, (size_t)r * sizeof(gpq_item)));
+      TRY(cudaMalloc(&g.bref, (size_t)r * sizeof(gpq_item)));
+      TRY(cudaMalloc(&g.k0, (size_t)r * sizeof(unsigned long long)));
+      TRY(cudaMalloc(&g.k1, (size_t)r * sizeof(unsigned long long)));
+      TRY(cudaMalloc(&g.rank, (size_t)r * sizeof(uint32_t)));
+      TRY(cudaMalloc(&g.addc, (size_t)r * sizeof(uint32_t)));
+      TRY(cudaMalloc(&g.ovf, sizeof(uint32_t)));
+      g.e2 = h->hq_sort[0];  // after populate: the sort scratch of a window's children
+      TRY(gpq::raise_smem_limit(hqg_phold_kernel, hqg_smem_bytes()));
+      int per_sm = 0;
+      TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hqg_phold_kernel, (int)kHqgThreads,
+                                                        hqg_smem_bytes()));
+      if (per_sm < 1) {
+        gpq::set_last_error("heap queue: the grid kernel does not fit on an SM");
+        return fail(GPQ_ERR_INVALID);
+      }
+      h->hqg_blocks = (uint32_t)h->num_sms;  // one CTA per SM: the barriers stay short
+    } else {
+      TRY(gpq::raise_smem_limit(hq_phold_kernel, (int)hq_smem_bytes(r)));
+    }
   } else if (c.queue_kind == GPQ_QUEUE_LAQ && c.laq_mode == 2) {
     gpq::LabGeometry geo{};
     const gpq_status gs = gpq::lab_geometry(c, &geo);
@@ -409,10 +444,23 @@ static gpq_status run_plain(gpq_phold* h, uint32_t nsteps, int* done, cudaStream
   return GPQ_OK;
 }
 
-// Parallel heap: one CTA runs up to nsteps windows (0 = all) of the heap.
+// Parallel heap: up to nsteps windows (0 = all) of the heap -- one CTA for nodes up to
+// kHqMaxR items, one cooperative launch over every SM for larger nodes.
 static gpq_status run_hq(gpq_phold* h, uint32_t nsteps, int* done, cudaStream_t st) {
-  hq_phold_kernel<<<1, 512, hq_smem_bytes(h->hq.r), st>>>(h->dev(), h->hq, nsteps);
-  GPQ_CUDA_TRY(cudaGetLastError());
+  if (h->hq_grid) {
+    GPQ_CUDA_TRY(cudaMemsetAsync(&h->ctrl->bar, 0, sizeof(unsigned long long), st));
+    GPQ_CUDA_TRY(cudaMemsetAsync(h->hqg.ovf, 0, sizeof(uint32_t), st));
+    PholdDev d = h->dev();
+    HqgDev g = h->hqg;
+    g.h = h->hq;
+    void* args[] = {&d, &g, &nsteps};
+    GPQ_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)hqg_phold_kernel, dim3(h->hqg_blocks), dim3(kHqgThreads),
+                                             args, hqg_smem_bytes(), st));
+    h->last_grid = h->hqg_blocks;
+  } else {
+    hq_phold_kernel<<<1, 512, hq_smem_bytes(h->hq.r), st>>>(h->dev(), h->hq, nsteps);
+    GPQ_CUDA_TRY(cudaGetLastError());
+  }
   uint32_t meta[2];
   GPQ_CUDA_TRY(cudaMemcpyAsync(meta, h->hq.meta, sizeof(meta), cudaMemcpyDeviceToHost, st));
   GPQ_CUDA_TRY(cudaStreamSynchronize(st));
