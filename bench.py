@@ -320,14 +320,18 @@ def _phold_form(G, O, cfgd, queue, runs, warmup=1, **kw):
 def bench_phold_c1(G, O, args, peak):
     """1,024 LPs x 16 events, lookahead 1.0 + Exp(1), uniform destinations, end time 100,
     seed 42 (820,705 events in 100 windows), through the parallel heap queue -- the kind
-    the workload names -- with the four other kinds beside it; each checked against the
-    committed oracle results, bit for bit."""
+    the workload names, in its whole-GPU form and its one-CTA form -- with the four other
+    kinds beside it; each checked against the committed oracle results, bit for bit."""
     g = golden("phold_plain_1024lp_x16_T100")
     kinds = {}
-    for queue in ("hq", "laq", "lhq", "lsq", "gaq"):
-        v, ms, (r, st) = _phold_form(G, O, C1, queue, runs=3)
+    # "hq": the default node size (the reference's 256 K root, here lowered to the
+    # 16,384-item population: one node, worked by the whole GPU); "hq_one_cta": 1,024-item
+    # nodes, one CTA working the heap
+    for label, queue, kw in (("hq", "hq", {}), ("hq_one_cta", "hq", {"node_size": 1024}), ("laq", "laq", {}),
+                             ("lhq", "lhq", {}), ("lsq", "lsq", {}), ("gaq", "gaq", {})):
+        v, ms, (r, st) = _phold_form(G, O, C1, queue, runs=3, **kw)
         by = BYTES_PER_EVENT * r["committed"] + BYTES_PER_LP_WINDOW * C1["num_lps"] * r["steps"]
-        kinds[queue] = {"value": v, "ms_per_run": ms, "exact_vs_oracle": matches_golden(O, g, r, st),
+        kinds[label] = {"value": v, "ms_per_run": ms, "exact_vs_oracle": matches_golden(O, g, r, st),
                         "roofline_frac": by / (ms / 1e3) / 1e9 / peak}
     cpu = []
     for _ in range(5):  # one thread, median of 5 (the sequential oracle, the whole run)

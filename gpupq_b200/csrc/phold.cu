@@ -193,7 +193,14 @@ gpq_status gpq_phold_create(const gpq_phold_config* cfg_in, gpq_phold** out) {
   TRY(cudaEventCreate(&h->ev1));
   const size_t L = c.num_lps;
   if (c.queue_kind == GPQ_QUEUE_HQ) {
-    const uint32_t r = c.node_size ? c.node_size : 1024;
+    // Default node size: the reference's 256 K root; a smaller population gets a root that
+    // just holds it (a larger root changes nothing but its buffers' size).
+    uint32_t r = c.node_size;
+    if (r == 0) {
+      const uint64_t pop = (uint64_t)c.num_lps * c.events_per_lp;
+      r = 2048;
+      while (r < pop && r < (256u << 10)) r <<= 1;
+    }
     const bool grid = r > kHqMaxR;
     if (!gpq::is_pow2(r) || r < 2 || r > kHqgMaxR || (!grid && c.num_lps > (1u << 21))) {
       gpq::set_last_error("heap queue: node_size must be a power of two in [2, %u] (num_lps <= 2^21 up to node "

@@ -196,7 +196,11 @@ typedef struct gpq_phold_config {
   uint32_t ctas_per_sm;     /* persistent grid: CTAs per SM; 0 = occupancy maximum */
   uint32_t max_steps;       /* safety cap on windows; 0 = none */
   uint32_t lanes_per_lp;    /* LAQ: lanes that work on one LP (4, 8, 16 or 32); 0 = tuned default */
-  uint32_t node_size;       /* HQ: items per heap node r (power of two <= 1024); 0 = 1024 */
+  uint32_t node_size;       /* HQ: items per heap node r, a power of two in [2, 2^22]: one CTA
+                             * works a heap of nodes up to 1,024 items, the whole GPU (one
+                             * cooperative launch) larger ones; 0 = the reference's 256 K
+                             * (HQ_NODE_SIZE, src/config.h:88), lowered to the population
+                             * rounded up to a power of two (at least 2,048) */
   uint32_t laq_mode;        /* LAQ: 0 = sorted runs, children merged each window; 1 = unordered
                                arrays, each window's safe events selected and ranked; 2 = time
                                buckets of 8-byte keys per LP, each window's buckets ranked
