@@ -629,6 +629,15 @@ def run_case(name):
                 t = time.perf_counter()
                 q.post()
                 print(f"post of {N} items: {(time.perf_counter() - t) * 1e3:.2f} ms (host clock)")
+    elif name == "phold_c1_heap":
+        # C1 through the whole-GPU heap queue (one 16,384-item root), two runs
+        cfg = G.make_phold_config(**C1, queue="hq")
+        with G.Phold(cfg) as h:
+            for _ in range(2):
+                h.populate()
+                h.run()
+                r = h.result()
+            print(r["committed"], r["steps"], r["elapsed_ms"], h.launch_info())
     elif name == "astar_ref_2048":
         m = G.astar_ref_map(256, 256, 0.2, 1.0, seed=14580)
         agents = G.astar_ref_agents(m, 4096, seed=11)
@@ -671,7 +680,7 @@ def main():
     ap.add_argument("--served-seconds", type=float, default=1.0, help="length of the served request stream")
     ap.add_argument("--case", default=None,
                     choices=["astar_batched_1000", "astar_plain_2048", "phold_batched_36", "gaq_sort_32m",
-                             "astar_ref_2048"],
+                             "astar_ref_2048", "phold_c1_heap"],
                     help="run one small named workload twice and exit (profiling captures)")
     args = ap.parse_args()
     if args.case:

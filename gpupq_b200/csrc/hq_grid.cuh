@@ -272,12 +272,20 @@ __device__ typename Ops::T* hqg_cta_sort(typename Ops::T* sa, typename Ops::T* s
   using T = typename Ops::T;
   constexpr uint32_t P = Ops::kPer;
   if (n <= kHqgRankSortMax) {
-    if (threadIdx.x < n) {
-      const T x = sa[hqg_pad<Ops>(threadIdx.x)];
-      uint32_t rk = 0;
-      for (uint32_t j = 0; j < n; ++j) rk += Ops::less(sa[hqg_pad<Ops>(j)], x) ? 1u : 0u;
-      sb[hqg_pad<Ops>(rk)] = x;
+    // G lanes (a power of two dividing 32) share one value's count when the block has
+    // G threads per value
+    uint32_t G = 1;
+    while (G < 32 && (G * 2) * n <= blockDim.x) G *= 2;
+    const uint32_t e = threadIdx.x / G, sub = threadIdx.x % G;
+    const bool valid = e < n;
+    T x{};
+    uint32_t rk = 0;
+    if (valid) {
+      x = sa[hqg_pad<Ops>(e)];
+      for (uint32_t j = sub; j < n; j += G) rk += Ops::less(sa[hqg_pad<Ops>(j)], x) ? 1u : 0u;
     }
+    for (uint32_t o = G / 2; o > 0; o >>= 1) rk += __shfl_xor_sync(GPQ_FULL_MASK, rk, o, G);
+    if (valid && sub == 0) sb[hqg_pad<Ops>(rk)] = x;
     __syncthreads();
     return sb;
   }

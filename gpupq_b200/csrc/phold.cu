@@ -639,7 +639,7 @@ gpq_status gpq_phold_lp_stats(gpq_phold* h, uint32_t* count, uint64_t* csum, uin
 gpq_status gpq_phold_launch_info(gpq_phold* h, uint32_t* grid, uint32_t* block, uint32_t* launches_per_run) {
   GPQ_CHECK_ARG(h, "handle is NULL");
   if (grid) *grid = h->last_grid;
-  if (block) *block = h->block;
+  if (block) *block = h->hq_grid ? kHqgThreads : h->block;
   if (launches_per_run)
     *launches_per_run = h->is_hq ? 1u
                       : h->gaq ? (uint32_t)(h->gaq_windows * gpq::gaq_engine_launches_per_window())
