@@ -4,8 +4,9 @@ gpq_phold_run_static exists for callers that cannot allocate device memory while
 run -- e.g. an application whose device memory belongs to another allocator or a fixed
 plan, or a latency-bound loop that cannot pay for cudaMalloc/cudaFree.  It keeps all
 queue state in one fixed 16 MiB device array, so its results must equal the normal
-create/populate/run path exactly.  This file is collected last on purpose: a run that
-stops at the first failure has executed every other test before it.
+create/populate/run path exactly.  Its file name sorts it after the other test files so
+that a run stopping at the first failure has executed them first; no test depends on that
+order (each test here creates its own handles and static runs).
 """
 import ctypes
 
