@@ -61,7 +61,7 @@ class PholdConfig(ctypes.Structure):
         ("lanes_per_lp", ctypes.c_uint32),
         ("node_size", ctypes.c_uint32),
         ("laq_mode", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 1),
+        ("gaq_engine", ctypes.c_uint32),
     ]
 
 
@@ -252,7 +252,7 @@ def presets():
 def make_phold_config(num_lps, events_per_lp, lookahead, end_time, seed, dest_mode=DEST_UNIFORM,
                       ring_width=16, ring_frac=0.9, queue="laq", capacity=256, insert_capacity=64,
                       loop="persistent", block_threads=0, ctas_per_sm=0, max_steps=0, lanes_per_lp=0, node_size=0,
-                      laq_mode=0):
+                      laq_mode=0, gaq_engine=0):
     c = PholdConfig()
     c.seed = seed
     c.num_lps = num_lps
@@ -272,6 +272,7 @@ def make_phold_config(num_lps, events_per_lp, lookahead, end_time, seed, dest_mo
     c.lanes_per_lp = lanes_per_lp
     c.node_size = node_size
     c.laq_mode = laq_mode
+    c.gaq_engine = gaq_engine
     return c
 
 

@@ -8,7 +8,7 @@
 // root-to-target paths, the root's safe prefix in batches, copy-last and delete-update --
 // inside one persistent cooperative launch over every SM:
 //   * merges are tiled: a CTA takes kHqgTile outputs, finds where they start and end in
-//     both inputs with a block-wide search (each round probes 384 positions at once, so a
+//     both inputs with a block-wide search (each round probes 256 positions at once, so a
 //     split costs three or four global round trips, not twenty), stages both input slices
 //     in shared memory and merges kHqgIpt outputs per thread there;
 //   * sorts are a block merge sort per chunk (a sorting network in registers, then
@@ -28,17 +28,25 @@
 
 #include "hq.cuh"
 
-static constexpr uint32_t kHqgThreads = 768;
+static constexpr uint32_t kHqgThreads = 512;
 static constexpr uint32_t kHqgIpt = 8;                          // items per thread (sorts, merges)
-static constexpr uint32_t kHqgTile = kHqgThreads * kHqgIpt;     // 6,144 items per CTA tile
+static constexpr uint32_t kHqgTile = kHqgThreads * kHqgIpt;     // 4,096 items per CTA tile
 static constexpr uint32_t kHqgKpt = 16;                         // keys per thread
-static constexpr uint32_t kHqgKeyTile = kHqgThreads * kHqgKpt;  // 12,288 keys per CTA tile
+static constexpr uint32_t kHqgKeyTile = kHqgThreads * kHqgKpt;  // 8,192 keys per CTA tile
 static constexpr uint32_t kHqgMaxR = 1u << 22;                  // node size limit of the grid form
 
-// Shared-memory tiles are padded by one element per kPer (a thread's run), so that a
-// thread's kPer consecutive elements and its neighbours' fall in different banks.
-__host__ __device__ inline size_t hqg_smem_bytes() {
+// Shared memory: two tiles, padded by one element per kPer (a thread's run), so that a
+// thread's kPer consecutive elements and its neighbours' fall in different banks; then an
+// auxiliary area of kHqgAux words (bin counts, and one packed word per element of a tile)
+// for the counting sorts and the bucket lists.
+static constexpr uint32_t kHqgAux = 16384;
+static constexpr uint32_t kHqgBins = kHqgAux / 2;  // bins of a counting sort
+__host__ __device__ inline size_t hqg_tiles_bytes() {
   return 2 * (size_t)(kHqgTile + kHqgTile / kHqgIpt) * sizeof(gpq_item);
+}
+__host__ __device__ inline size_t hqg_smem_bytes() { return hqg_tiles_bytes() + (size_t)kHqgAux * sizeof(uint32_t); }
+__device__ __forceinline__ uint32_t* hqg_aux(unsigned char* smem) {
+  return reinterpret_cast<uint32_t*>(smem + hqg_tiles_bytes());
 }
 
 struct HqgItemOps {
@@ -74,6 +82,12 @@ struct HqgDev {
   uint32_t* rank;           // [r] an event's position in its LP's sequence
   uint32_t* addc;           // [r] run length at the last event of an LP's run, else 0
   uint32_t* ovf;            // bucket overflows of the one-phase paths (zeroed per launch)
+  // Bucket lists that each phase fills for the next (heaps whose root holds every item;
+  // null otherwise).  Counts are double-buffered by window parity and zeroed per launch.
+  gpq_item* ilist;            // [max buckets][kHqgListCapI] children by root-quantile bucket
+  uint32_t* icnt;             // [2][max buckets]
+  unsigned long long* plist;  // [max buckets][kHqgListCapP] next batch's (lp, position) keys by LP range
+  uint32_t* pcnt;             // [2][max buckets]
 };
 
 struct HqgSync {
@@ -687,20 +701,361 @@ __device__ bool hqg_insert_scan(const HqgDev& g, HqgState& q, const gpq_item* C,
   return true;
 }
 
+// ---------------------------------------------------------------------------------------
+// Bucket lists passed between phases (heaps whose root holds every item, the global
+// array queue's layout).  The batch phase files every child into a bucket of the root's
+// remainder R (splitters: R's quantiles, as in the one-phase insert); the insert phase
+// sorts each bucket in shared memory, streams its R slice past it and, while writing the
+// new root, files the next batch's (lp, position) keys into LP-range lists (the next
+// bound follows from the smallest child, which the batch phase records).  A window then
+// costs two phases whose CTAs read only their own buckets.  A list that overflows sends
+// the phase down the paths above (the children are also kept in h.ch).
+
+static constexpr uint32_t kHqgListCapI = kHqgTile;     // children per insert bucket
+static constexpr uint32_t kHqgListCapP = kHqgKeyTile;  // keys per LP-range bucket
+static constexpr uint32_t kHqgMaxBuckets = 160;        // >= the grid (one CTA per SM)
+
+struct HqgLists {
+  bool ins;     // this window's children are filed in the insert lists
+  bool proc;    // unused
+  uint32_t BI;  // insert buckets
+  uint32_t BP;  // unused
+};
+
+// LP-range buckets: LP lp belongs to bucket floor(lp * B / L), whose first LP is
+// ceil(b * L / B).
+__device__ __forceinline__ uint32_t hqg_lp_bucket(uint32_t lp, uint32_t B, uint32_t L) {
+  return (uint32_t)((uint64_t)lp * B / L);
+}
+__device__ __forceinline__ uint32_t hqg_lp_first(uint32_t b, uint32_t B, uint32_t L) {
+  return (uint32_t)(((uint64_t)b * L + B - 1) / B);
+}
+
+// Insert buckets for a batch of c events leaving nr items in the root.
+__device__ __forceinline__ uint32_t hqg_list_ibuckets(uint32_t nr, uint32_t c) {
+  if (nr == 0) return 1u;
+  return min(gridDim.x, max(1u, min(nr, (nr + c) / 256u)));
+}
+
+// Where a batch phase files its children (ins.on == false: nowhere).
+struct HqgIns {
+  bool on;
+  uint32_t BI;
+  const gpq_item* spl;  // [BI - 1] splitters (shared memory)
+  uint32_t* icnt;       // [BI] this window's counts
+  gpq_item* ilist;
+};
+
+// Bucket of x among the splitters: the number of splitters below it.
+__device__ __forceinline__ uint32_t hqg_bucket_of(const gpq_item* spl, uint32_t ns, const gpq_item& x) {
+  uint32_t lo = 0, hi = ns;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (hq_less(spl[mid], x)) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+// Appends v to list `bucket` (cap entries each) for every lane with `take`; lanes of a warp
+// that share a bucket take one atomic.  All lanes of the warp.  Returns false if the
+// bucket was full (the entry is counted, not stored: the reader sees the overflow).
+template <class T>
+__device__ __forceinline__ void hqg_list_append(uint32_t* cnt, T* list, uint32_t cap, bool take, uint32_t bucket,
+                                                const T& v) {
+  const uint32_t key = take ? bucket : (0x80000000u | (threadIdx.x & 31u));
+  const uint32_t peers = __match_any_sync(GPQ_FULL_MASK, key);
+  const uint32_t lane = threadIdx.x & 31u, leader = (uint32_t)(__ffs(peers) - 1);
+  uint32_t b = 0;
+  if (take && lane == leader) b = atomicAdd(&cnt[bucket], (uint32_t)__popc(peers));
+  b = __shfl_sync(GPQ_FULL_MASK, b, (int)leader);
+  const uint32_t slot = b + __popc(peers & ((1u << lane) - 1u));
+  if (take && slot < cap) list[(size_t)bucket * cap + slot] = v;
+}
+
+// Loads the BI - 1 splitters of the root remainder R[0, nr) into shared memory.
+__device__ __forceinline__ void hqg_load_splitters(gpq_item* spl, const gpq_item* R, uint32_t nr, uint32_t BI) {
+  for (uint32_t k = threadIdx.x; k + 1 < BI; k += blockDim.x) spl[k] = R[(uint32_t)((uint64_t)(k + 1) * nr / BI)];
+  __syncthreads();
+}
+
+// Exclusive scan of a[0, n) in shared memory by the CTA (n <= kHqgBins); returns the total
+// and sets *mx to the largest entry.  All threads.
+__device__ uint32_t hqg_block_scan(uint32_t* a, uint32_t n, uint32_t* mx) {
+  __shared__ uint32_t s_w[32], s_m[32];
+  const uint32_t per = (n + blockDim.x - 1) / blockDim.x;
+  const uint32_t b0 = min(n, threadIdx.x * per), b1 = min(n, b0 + per);
+  uint32_t sum = 0, m = 0;
+  for (uint32_t i = b0; i < b1; ++i) {
+    sum += a[i];
+    m = max(m, a[i]);
+  }
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  uint32_t incl = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t v = __shfl_up_sync(GPQ_FULL_MASK, incl, o);
+    if (lane >= (uint32_t)o) incl += v;
+  }
+  m = __reduce_max_sync(GPQ_FULL_MASK, m);
+  if (lane == 31) s_w[warp] = incl;
+  if (lane == 0) s_m[warp] = m;
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t nw = blockDim.x >> 5;
+    const uint32_t v = lane < nw ? s_w[lane] : 0u;
+    uint32_t wi = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t u = __shfl_up_sync(GPQ_FULL_MASK, wi, o);
+      if (lane >= (uint32_t)o) wi += u;
+    }
+    const uint32_t mm = __reduce_max_sync(GPQ_FULL_MASK, lane < nw ? s_m[lane] : 0u);
+    s_w[lane] = wi - v;
+    if (lane == 31) s_m[0] = wi;  // total
+    if (lane == 30) s_m[1] = mm;
+  }
+  __syncthreads();
+  uint32_t run = s_w[warp] + incl - sum;
+  for (uint32_t i = b0; i < b1; ++i) {
+    const uint32_t v = a[i];
+    a[i] = run;
+    run += v;
+  }
+  const uint32_t total = s_m[0];
+  *mx = s_m[1];
+  __syncthreads();
+  return total;
+}
+
+static constexpr uint32_t kHqgRunMax = 64;  // longest bin a thread sorts by insertion
+
+// Sorts the n items of the padded tile in (n <= kHqgTile; LPs below L) into out: a
+// counting sort over bins of v = (ts bits - min) * 2^16 + lp * 2^16 / L (monotone in the
+// item order; the LP part spreads equal timestamps, frequent where float32 spacing is
+// coarse), bin = v * NB / (v range), then each bin sorted by the full item order
+// (insertion sort, one thread per bin).  Returns false, with out unusable, when some bin
+// has more than kHqgRunMax items.  bins: kHqgBins words.  All threads.
+__device__ bool hqg_bin_sort_items(const gpq_item* in, gpq_item* out, uint32_t n, uint32_t L, uint32_t* bins) {
+  __shared__ uint32_t s_tmin, s_tmax;
+  if (threadIdx.x == 0) {
+    s_tmin = 0xffffffffu;
+    s_tmax = 0u;
+  }
+  __syncthreads();
+  uint32_t tmin = 0xffffffffu, tmax = 0u;
+  for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
+    const uint32_t t = gpq_f2u(in[hqg_pad<HqgItemOps>(j)].ts);
+    tmin = min(tmin, t);
+    tmax = max(tmax, t);
+  }
+  tmin = warp_min_u32(tmin);
+  tmax = __reduce_max_sync(GPQ_FULL_MASK, tmax);
+  if ((threadIdx.x & 31u) == 0) {
+    atomicMin(&s_tmin, tmin);
+    atomicMax(&s_tmax, tmax);
+  }
+  const uint32_t NB = max(1u, min(kHqgBins, n));
+  for (uint32_t b = threadIdx.x; b < NB; b += blockDim.x) bins[b] = 0u;
+  __syncthreads();
+  const uint32_t t0 = s_tmin;
+  const uint64_t span = ((uint64_t)(s_tmax - t0) + 1u) << 16;  // <= 2^48
+  auto bin_of = [t0, span, NB, L](const gpq_item& x) {
+    const uint64_t v = ((uint64_t)(gpq_f2u(x.ts) - t0) << 16) + (((uint64_t)x.lp << 16) / L);
+    return (uint32_t)(v * NB / span);  // v * NB < 2^61
+  };
+  for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) atomicAdd(&bins[bin_of(in[hqg_pad<HqgItemOps>(j)])], 1u);
+  __syncthreads();
+  uint32_t mx = 0;
+  hqg_block_scan(bins, NB, &mx);
+  if (mx > kHqgRunMax) return false;
+  for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
+    const gpq_item x = in[hqg_pad<HqgItemOps>(j)];
+    const uint32_t pos = atomicAdd(&bins[bin_of(x)], 1u);
+    if (pos < n) out[hqg_pad<HqgItemOps>(pos)] = x;
+  }
+  __syncthreads();
+  for (uint32_t b = threadIdx.x; b < NB; b += blockDim.x) {
+    const uint32_t e = bins[b], st = b ? bins[b - 1] : 0u;
+    for (uint32_t x = st + 1; x < e; ++x) {
+      const gpq_item v = out[hqg_pad<HqgItemOps>(x)];
+      uint32_t y = x;
+      while (y > st && hq_less(v, out[hqg_pad<HqgItemOps>(y - 1)])) {
+        out[hqg_pad<HqgItemOps>(y)] = out[hqg_pad<HqgItemOps>(y - 1)];
+        --y;
+      }
+      out[hqg_pad<HqgItemOps>(y)] = v;
+    }
+  }
+  __syncthreads();
+  return true;
+}
+
+// Groups the n (lp, position) keys of in (padded tile) by LP into out (padded tile): a
+// counting sort over the LP range [lp0, lp0 + W), then each LP's run sorted by position
+// (insertion sort, one thread per LP).  On return bins[b] is the end of LP lp0 + b's run
+// (its start: bins[b - 1], or 0).  Returns false, with out unusable, when W exceeds
+// kHqgBins or some LP has more than kHqgRunMax keys.  All threads.
+__device__ bool hqg_group_by_lp(const unsigned long long* in, unsigned long long* out, uint32_t n, uint32_t lp0,
+                                uint32_t W, uint32_t* bins) {
+  __shared__ int s_outside;
+  if (W > kHqgBins || W == 0) return false;
+  for (uint32_t b = threadIdx.x; b < W; b += blockDim.x) bins[b] = 0u;
+  if (threadIdx.x == 0) s_outside = 0;
+  __syncthreads();
+  for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
+    const uint32_t bi = (uint32_t)(in[hqg_pad<HqgKeyOps>(j)] >> 32) - lp0;
+    if (bi < W) atomicAdd(&bins[bi], 1u);
+    else s_outside = 1;  // a key outside the range: not binned (the merge sort takes any keys)
+  }
+  __syncthreads();
+  if (s_outside) return false;
+  uint32_t mx = 0;
+  hqg_block_scan(bins, W, &mx);
+  if (mx > kHqgRunMax) return false;
+  for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
+    const unsigned long long k = in[hqg_pad<HqgKeyOps>(j)];
+    const uint32_t pos = atomicAdd(&bins[(uint32_t)(k >> 32) - lp0], 1u);
+    if (pos < n) out[hqg_pad<HqgKeyOps>(pos)] = k;
+  }
+  __syncthreads();
+  for (uint32_t b = threadIdx.x; b < W; b += blockDim.x) {
+    const uint32_t e = bins[b], st = b ? bins[b - 1] : 0u;
+    for (uint32_t x = st + 1; x < e; ++x) {  // insertion sort of the run by position
+      const unsigned long long v = out[hqg_pad<HqgKeyOps>(x)];
+      uint32_t y = x;
+      while (y > st && out[hqg_pad<HqgKeyOps>(y - 1)] > v) {
+        out[hqg_pad<HqgKeyOps>(y)] = out[hqg_pad<HqgKeyOps>(y - 1)];
+        --y;
+      }
+      out[hqg_pad<HqgKeyOps>(y)] = v;
+    }
+  }
+  __syncthreads();
+  return true;
+}
+
+// The n (lp, position) keys K of one LP range (padded tile, grouped by LP with positions
+// ascending -- every LP's events of the batch), seg(j, lp) = the first position of lp's run:
+// each event folded into its LP's outputs in order (the per-LP sums of a warp's run added
+// by one lane), its child written to ch[base + position] and filed by `ins` (counted per
+// bucket in shared memory, one reservation per bucket, then written), the LP's count
+// advanced.  aux: kHqgBins words for the children's bucket slots.  All threads.
+template <class Seg>
+__device__ void hqg_process_keys(const PholdDev& d, const HqgDev& g, const gpq_item* root,
+                                 const unsigned long long* K, uint32_t n, uint32_t base, const HqgIns& ins,
+                                 uint32_t* slots, Seg seg) {
+  __shared__ uint32_t s_bc[kHqgMaxBuckets], s_gb[kHqgMaxBuckets];
+  if (ins.on) {
+    for (uint32_t k = threadIdx.x; k < ins.BI; k += blockDim.x) s_bc[k] = 0u;
+    __syncthreads();
+  }
+  const uint32_t lane = threadIdx.x & 31u;
+  const bool direct = n <= blockDim.x;
+  for (uint32_t j0 = 0; j0 < n; j0 += blockDim.x) {
+    const uint32_t j = j0 + threadIdx.x;
+    const bool valid = j < n;
+    uint32_t lp = 0;
+    unsigned long long cs = 0, oh = 0;
+    gpq_item chd{};
+    if (valid) {
+      const unsigned long long key = K[hqg_pad<HqgKeyOps>(j)];
+      lp = (uint32_t)(key >> 32);
+      const uint32_t i = (uint32_t)key;
+      const gpq_item e = root[i];
+      const uint64_t hh = gpq_ev_hash(e.id, gpq_f2u(e.ts));
+      cs = hh;
+      oh = gpq_seq_hash(hh, (uint64_t)d.count[lp] + (j - seg(j, lp)));
+      const gpq_item ch = gpq_phold_child(d.p, e);
+      g.h.ch[base + i] = ch;
+      if (ins.on && !direct && j < kHqgBins) {
+        const uint32_t bk = hqg_bucket_of(ins.spl, ins.BI - 1, ch);
+        slots[j] = (bk << 16) | atomicAdd(&s_bc[bk], 1u);
+      }
+      if (ins.on && direct) chd = ch;
+    }
+    if (ins.on && direct) {  // one round: each warp files its children directly
+      const uint32_t bk = valid ? hqg_bucket_of(ins.spl, ins.BI - 1, chd) : 0u;
+      hqg_list_append<gpq_item>(ins.icnt, ins.ilist, kHqgListCapI, valid, bk, chd);
+    }
+    // the LP's runs are contiguous in the warp: sum each run into its first lane
+    const uint32_t peers = __match_any_sync(GPQ_FULL_MASK, valid ? lp : (0x80000000u | lane));
+    const uint32_t last = 31u - __clz(peers);
+#pragma unroll
+    for (uint32_t o = 1; o < 32; o <<= 1) {
+      const unsigned long long c2 = __shfl_down_sync(GPQ_FULL_MASK, cs, o);
+      const unsigned long long o2 = __shfl_down_sync(GPQ_FULL_MASK, oh, o);
+      if (lane + o <= last) {
+        cs += c2;
+        oh += o2;
+      }
+    }
+    if (valid && lane == (uint32_t)(__ffs(peers) - 1)) {
+      atomicAdd(&d.csum[lp], cs);
+      atomicAdd(&d.ohash[lp], oh);
+    }
+  }
+  __syncthreads();
+  for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
+    const uint32_t lp = (uint32_t)(K[hqg_pad<HqgKeyOps>(j)] >> 32);
+    if (j + 1 == n || (uint32_t)(K[hqg_pad<HqgKeyOps>(j + 1)] >> 32) != lp) d.count[lp] += j - seg(j, lp) + 1;
+  }
+  if (ins.on && !direct) {  // one reservation per bucket, then the children into their lists
+    for (uint32_t k = threadIdx.x; k < ins.BI; k += blockDim.x)
+      s_gb[k] = s_bc[k] ? atomicAdd(&ins.icnt[k], s_bc[k]) : 0u;
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
+      const uint32_t i = (uint32_t)K[hqg_pad<HqgKeyOps>(j)];
+      const gpq_item ch = g.h.ch[base + i];
+      if (j < kHqgBins) {
+        const uint32_t sv = slots[j], bk = sv >> 16, slot = s_gb[bk] + (sv & 0xffffu);
+        if (slot < kHqgListCapI) ins.ilist[(size_t)bk * kHqgListCapI + slot] = ch;
+      } else {  // beyond the slot area (more than kHqgBins keys): one atomic each
+        const uint32_t bk = hqg_bucket_of(ins.spl, ins.BI - 1, ch);
+        const uint32_t slot = atomicAdd(&ins.icnt[bk], 1u);
+        if (slot < kHqgListCapI) ins.ilist[(size_t)bk * kHqgListCapI + slot] = ch;
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// Sorts the n keys of sa (an LP range of W LPs from lp0) for hqg_process_keys and runs it:
+// grouped by LP when it can, else the block merge sort.
+__device__ void hqg_sort_and_process(const PholdDev& d, const HqgDev& g, const gpq_item* root,
+                                     unsigned long long* sa, unsigned long long* sb, uint32_t n, uint32_t lp0,
+                                     uint32_t W, uint32_t base, const HqgIns& ins, uint32_t* aux) {
+  uint32_t* bins = aux;
+  uint32_t* slots = aux + kHqgBins;
+  if (hqg_group_by_lp(sa, sb, n, lp0, W, bins)) {
+    hqg_process_keys(d, g, root, sb, n, base, ins, slots,
+                     [bins, lp0](uint32_t, uint32_t lp) { return lp > lp0 ? bins[lp - lp0 - 1] : 0u; });
+  } else {
+    const unsigned long long* K = hqg_cta_sort<HqgKeyOps>(sa, sb, n);
+    hqg_process_keys(d, g, root, K, n, base, ins, slots, [K](uint32_t j, uint32_t lp) {
+      const unsigned long long lo_key = (unsigned long long)lp << 32;
+      uint32_t l = 0, h = j;
+      while (l < h) {
+        const uint32_t mid = (l + h) >> 1;
+        if (K[hqg_pad<HqgKeyOps>(mid)] < lo_key) l = mid + 1; else h = mid;
+      }
+      return l;
+    });
+  }
+}
+
 // A batch of c <= kHqgKeyTile events root[0, c) in one phase: LP-range buckets, so that
-// every LP's events of the batch are in one CTA, which sorts their (lp, position) keys in
-// shared memory, takes each event's rank from its run, folds the event into its LP's
-// outputs, writes its child to ch[base + position] and advances the LP's count (the LP's
-// one writer).  Ends with a barrier.
+// every LP's events of the batch are in one CTA, which collects their (lp, position) keys
+// by scanning the batch, sorts them in shared memory and processes them in order
+// (hqg_process_keys).  Ends with a barrier.
 __device__ void hqg_process_scan(const PholdDev& d, const HqgDev& g, const gpq_item* root, uint32_t c, uint32_t base,
-                                 unsigned char* smem, HqgSync& s) {
+                                 const HqgIns& ins, unsigned char* smem, HqgSync& s) {
   const uint32_t L = d.L;
   const uint32_t B = min(gridDim.x, max(1u, c / 64u));
   unsigned long long* sa = reinterpret_cast<unsigned long long*>(smem);
   unsigned long long* sb = sa + hqg_tile_cap<HqgKeyOps>();
   __shared__ uint32_t s_n;
   for (uint32_t b = blockIdx.x; b < B; b += gridDim.x) {
-    const uint32_t lo = (uint32_t)((uint64_t)b * L / B), hi = (uint32_t)((uint64_t)(b + 1) * L / B);
+    const uint32_t lo = hqg_lp_first(b, B, L), hi = hqg_lp_first(b + 1, B, L);
     if (threadIdx.x == 0) s_n = 0;
     __syncthreads();
     hqg_cta_scan<8>(c, [root](uint32_t i) { return root[i].lp; }, [&](uint32_t i, uint32_t lp, bool valid) {
@@ -714,29 +1069,178 @@ __device__ void hqg_process_scan(const PholdDev& d, const HqgDev& g, const gpq_i
       if (threadIdx.x == 0) gpq_set_error(&d.ctrl->err, GPQ_ERR_INSERT_FULL);
       n = 0;
     }
-    const unsigned long long* K = hqg_cta_sort<HqgKeyOps>(sa, sb, n);
-    auto seg_of = [K](uint32_t j, uint32_t lp) {
-      const unsigned long long lo_key = (unsigned long long)lp << 32;
-      uint32_t l = 0, h = j;
-      while (l < h) {
-        const uint32_t mid = (l + h) >> 1;
-        if (K[hqg_pad<HqgKeyOps>(mid)] < lo_key) l = mid + 1; else h = mid;
+    hqg_sort_and_process(d, g, root, sa, sb, n, lo, hi - lo, base, ins, hqg_aux(smem));
+  }
+  hqg_bar(s);
+}
+
+// A batch whose keys the insert phase filed into BP LP-range lists (counts pc, none above
+// kHqgListCapP): each CTA sorts its list and processes it.  Ends with a barrier.
+__device__ void hqg_process_lists(const PholdDev& d, const HqgDev& g, const gpq_item* root, const uint32_t* pc,
+                                  uint32_t BP, uint32_t base, const HqgIns& ins, unsigned char* smem, HqgSync& s) {
+  unsigned long long* sa = reinterpret_cast<unsigned long long*>(smem);
+  unsigned long long* sb = sa + hqg_tile_cap<HqgKeyOps>();
+  const uint32_t L = d.L;
+  for (uint32_t b = blockIdx.x; b < BP; b += gridDim.x) {
+    const uint32_t n = min(pc[b], kHqgListCapP);
+    const uint32_t lo = hqg_lp_first(b, BP, L), hi = hqg_lp_first(b + 1, BP, L);
+    const unsigned long long* src = g.plist + (size_t)b * kHqgListCapP;
+    for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) sa[hqg_pad<HqgKeyOps>(j)] = src[j];
+    __syncthreads();
+    hqg_sort_and_process(d, g, root, sa, sb, n, lo, hi - lo, base, ins, hqg_aux(smem));
+  }
+  hqg_bar(s);
+}
+
+// The children of the last batch, filed in BI insert lists (this window's counts ic), into
+// the root (all of whose items stay: R = root[off, off + cnt0)): CTA b sorts its list in
+// shared memory and streams R's slice b past it -- an R item lands at (slice start +
+// children below the slice + its index + children below it), the children between two R
+// items right after the first -- into the root's other buffer.  Returns false, with
+// nothing written, when a list overflowed.
+__device__ bool hqg_insert_lists(const HqgDev& g, HqgState& q, uint32_t nch, uint32_t BI, const uint32_t* ic,
+                                 uint32_t L, unsigned char* smem, HqgSync& s) {
+  __shared__ uint32_t s_pre[kHqgMaxBuckets + 1];
+  __shared__ int s_ovf;
+  uint32_t* aux = hqg_aux(smem);
+  const gpq_item* R = q.root + q.off;
+  const uint32_t nr = q.cnt0;
+  for (uint32_t k = threadIdx.x; k < BI; k += blockDim.x) s_pre[k] = ic[k];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t run = 0;
+    int ovf = 0;
+    for (uint32_t k = 0; k < BI; ++k) {
+      const uint32_t v = s_pre[k];
+      ovf |= v > kHqgListCapI ? 1 : 0;
+      s_pre[k] = run;
+      run += v;
+    }
+    s_pre[BI] = run;
+    s_ovf = ovf || run != nch;
+  }
+  __syncthreads();
+  if (s_ovf) return false;  // the same decision in every block: nothing written
+  gpq_item* sa = reinterpret_cast<gpq_item*>(smem);
+  gpq_item* sb = sa + hqg_tile_cap<HqgItemOps>();
+  gpq_item* out = q.spare;
+  for (uint32_t b = blockIdx.x; b < BI; b += gridDim.x) {
+    const uint32_t nc = s_pre[b + 1] - s_pre[b];
+    const gpq_item* src = g.ilist + (size_t)b * kHqgListCapI;
+    for (uint32_t j = threadIdx.x; j < nc; j += blockDim.x) sa[hqg_pad<HqgItemOps>(j)] = src[j];
+    __syncthreads();
+    const gpq_item* X = hqg_bin_sort_items(sa, sb, nc, L, aux) ? sb : hqg_cta_sort<HqgItemOps>(sa, sb, nc);
+    gpq_item* Y = (X == sa) ? sb : sa;  // two staging halves for R's tiles
+    const uint32_t r0 = (uint32_t)((uint64_t)b * nr / BI), r1 = (uint32_t)((uint64_t)(b + 1) * nr / BI);
+    const uint32_t nrb = r1 - r0, base = r0 + s_pre[b];
+    // R's slice in tiles of kStreamTile staged in shared memory (the next tile's loads in
+    // flight while the current one merges); each tile merged with the children between its
+    // first item and the next tile's (merge path, kHqgIpt outputs a thread).  chis[t]: the
+    // children below tile t + 1's first item, for all tiles at once.
+    constexpr uint32_t kStreamTile = 2048, kPerT = kStreamTile / kHqgThreads;
+    static_assert(kStreamTile % kHqgThreads == 0, "stream tile");
+    constexpr uint32_t kHalf = kStreamTile + kStreamTile / kHqgIpt;  // padded half of a tile
+    const uint32_t ntiles = (nrb + kStreamTile - 1) / kStreamTile;
+    // aux: the tiles' child counts at its end (kChis words), the merged output of a tile
+    // before it (padded; a tile whose output is larger is stored directly)
+    constexpr uint32_t kChis = 2048;
+    constexpr uint32_t kOutCap = ((kHqgAux - kChis) * 4u / sizeof(gpq_item)) * kHqgIpt / (kHqgIpt + 1);
+    uint32_t* chis = aux + (kHqgAux - kChis);
+    gpq_item* ostage = reinterpret_cast<gpq_item*>(aux);
+    uint32_t cpos = 0;  // children below the current tile's first item
+    for (uint32_t tb = 0; tb < ntiles; tb += kChis) {  // boundaries, kChis at a time
+      const uint32_t tcnt = min(kChis, ntiles - tb);
+      for (uint32_t t = threadIdx.x; t < tcnt; t += blockDim.x) {
+        const uint32_t tt = tb + t, nxt = (tt + 1) * kStreamTile;
+        uint32_t chi = nc;
+        if (nxt < nrb) {
+          const gpq_item nx = R[r0 + nxt];
+          uint32_t lo = 0, hi = nc;
+          while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (hq_less(X[hqg_pad<HqgItemOps>(mid)], nx)) lo = mid + 1; else hi = mid;
+          }
+          chi = lo;
+        }
+        chis[t] = chi;
       }
-      return l;
-    };
-    for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
-      const unsigned long long key = K[hqg_pad<HqgKeyOps>(j)];
-      const uint32_t lp = (uint32_t)(key >> 32), i = (uint32_t)key;
-      const gpq_item e = root[i];
-      const uint64_t hh = gpq_ev_hash(e.id, gpq_f2u(e.ts));
-      atomicAdd(&d.csum[lp], (unsigned long long)hh);
-      atomicAdd(&d.ohash[lp], (unsigned long long)gpq_seq_hash(hh, (uint64_t)d.count[lp] + (j - seg_of(j, lp))));
-      g.h.ch[base + i] = gpq_phold_child(d.p, e);
+      gpq_item pre[kPerT];
+      auto fetch = [&](uint32_t tt) {
+        const uint32_t t0 = tt * kStreamTile;
+#pragma unroll
+        for (uint32_t u = 0; u < kPerT; ++u) {
+          const uint32_t i = t0 + u * blockDim.x + threadIdx.x;
+          if (i < nrb) pre[u] = R[r0 + i];
+        }
+      };
+      auto stage = [&](uint32_t tt, gpq_item* Yh) {
+        const uint32_t t0 = tt * kStreamTile;
+#pragma unroll
+        for (uint32_t u = 0; u < kPerT; ++u) {
+          const uint32_t i = u * blockDim.x + threadIdx.x;
+          if (t0 + i < nrb) Yh[hqg_pad<HqgItemOps>(i)] = pre[u];
+        }
+      };
+      fetch(tb);
+      stage(tb, Y);
+      __syncthreads();
+      for (uint32_t t = 0; t < tcnt; ++t) {
+        const uint32_t tt = tb + t, t0 = tt * kStreamTile;
+        gpq_item* Yh = Y + (t & 1u) * kHalf;
+        if (t + 1 < tcnt) fetch(tt + 1);  // in flight during the merge
+        const uint32_t tn = min(kStreamTile, nrb - t0), chi = chis[t], cn = chi - cpos, total = tn + cn;
+        gpq_item* dst = out + base + t0 + cpos;
+        const bool staged = total <= kOutCap;
+        for (uint32_t o0 = threadIdx.x * kHqgIpt; o0 < total; o0 += blockDim.x * kHqgIpt) {
+          if (staged)
+            hqg_merge_run<HqgItemOps>(Yh, 0, tn, X, cpos, cn, o0,
+                                      [&](uint32_t k, const gpq_item& v) { ostage[hqg_pad<HqgItemOps>(o0 + k)] = v; });
+          else
+            hqg_merge_run<HqgItemOps>(Yh, 0, tn, X, cpos, cn, o0, [&](uint32_t k, const gpq_item& v) { dst[o0 + k] = v; });
+        }
+        if (t + 1 < tcnt) stage(tt + 1, Y + ((t + 1) & 1u) * kHalf);
+        __syncthreads();
+        if (staged) {  // coalesced stores
+          for (uint32_t i = threadIdx.x; i < total; i += blockDim.x) dst[i] = ostage[hqg_pad<HqgItemOps>(i)];
+          __syncthreads();
+        }
+        cpos = chi;
+      }
+    }
+    for (uint32_t j = cpos + threadIdx.x; j < nc; j += blockDim.x) out[base + nrb + j] = X[hqg_pad<HqgItemOps>(j)];
+    __syncthreads();
+  }
+  if (!hqg_bar(s)) return false;
+  q.swap_root();
+  q.cnt0 = nr + nch;
+  return true;
+}
+
+// The batch root[0, c) filed into BP LP-range lists (counts pc, zero on entry) for
+// hqg_process_lists: each CTA takes an equal slice of the batch, counts its keys per range
+// in shared memory, reserves each range's share with one atomic and writes them.  Ends
+// with a barrier.
+__device__ void hqg_file_batch(const PholdDev& d, const HqgDev& g, const gpq_item* root, uint32_t c, uint32_t BP,
+                               uint32_t* pc, unsigned char* smem, HqgSync& s) {
+  __shared__ uint32_t s_pb[kHqgMaxBuckets];
+  uint32_t* aux = hqg_aux(smem);
+  const uint32_t L = d.L;
+  const uint32_t per = (c + gridDim.x - 1) / gridDim.x;
+  const uint32_t lo = min(c, blockIdx.x * per), hi = min(c, lo + per);
+  for (uint32_t p0 = lo; p0 < hi; p0 += kHqgAux) {
+    const uint32_t pn = min(kHqgAux, hi - p0);
+    for (uint32_t k = threadIdx.x; k < BP; k += blockDim.x) s_pb[k] = 0u;
+    __syncthreads();
+    for (uint32_t p = threadIdx.x; p < pn; p += blockDim.x) {
+      const uint32_t bk = hqg_lp_bucket(root[p0 + p].lp, BP, L);
+      aux[p] = (bk << 16) | atomicAdd(&s_pb[bk], 1u);
     }
     __syncthreads();
-    for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
-      const uint32_t lp = (uint32_t)(K[hqg_pad<HqgKeyOps>(j)] >> 32);
-      if (j + 1 == n || (uint32_t)(K[hqg_pad<HqgKeyOps>(j + 1)] >> 32) != lp) d.count[lp] += j - seg_of(j, lp) + 1;
+    for (uint32_t k = threadIdx.x; k < BP; k += blockDim.x) s_pb[k] = s_pb[k] ? atomicAdd(&pc[k], s_pb[k]) : 0u;
+    __syncthreads();
+    for (uint32_t p = threadIdx.x; p < pn; p += blockDim.x) {
+      const uint32_t sv = aux[p], bk = sv >> 16, slot = s_pb[bk] + (sv & 0xffffu);
+      if (slot < kHqgListCapP) g.plist[(size_t)bk * kHqgListCapP + slot] = ((unsigned long long)root[p0 + p].lp << 32) | (p0 + p);
     }
     __syncthreads();
   }
@@ -763,15 +1267,31 @@ static __global__ void __launch_bounds__(kHqgThreads, 1) hqg_phold_kernel(PholdD
   q.cnt0 = h.cnt[0];
   q.cntl = q.last > 0 ? h.cnt[q.last] : 0u;
   uint32_t steps = 0, nch = 0, ovf_seen = 0;
+  HqgLists lists{false, false, 0u, 0u};
+  __shared__ gpq_item s_spl[kHqgMaxBuckets];
+  __shared__ uint32_t s_pc[kHqgMaxBuckets];
+  __shared__ int s_pc_ovf;
+  __shared__ uint32_t s_pc_sum;
   while (s.ok) {
     if (nch > 0) {  // the previous window's children
-      const uint32_t B = hqg_insert_buckets(q, r, nch);
-      const bool done = B != 0 && hqg_insert_scan(g, q, h.ch, nch, B, smem, s, ovf_seen);
-      if (!s.ok) break;
+      bool done = false;
+      if (g.icnt != nullptr && blockIdx.x == 0)  // the next window's insert counts start at zero
+        for (uint32_t k = threadIdx.x; k < kHqgMaxBuckets; k += blockDim.x)
+          g.icnt[((steps + 1u) & 1u) * kHqgMaxBuckets + k] = 0u;
+      if (lists.ins) {
+        done = hqg_insert_lists(g, q, nch, lists.BI, g.icnt + (steps & 1u) * kHqgMaxBuckets, d.L, smem, s);
+        if (!s.ok) break;
+      }
+      lists.ins = false;
       if (!done) {
-        const gpq_item* ch = h.ch;
-        const gpq_item* sorted = hqg_sort<HqgItemOps>(h.ch, g.e2, nch, smem, s, [ch](uint32_t j) { return ch[j]; });
-        if (!hqg_insert(d, g, q, sorted, nch, smem, s)) break;
+        const uint32_t B = hqg_insert_buckets(q, r, nch);
+        const bool done1 = B != 0 && hqg_insert_scan(g, q, h.ch, nch, B, smem, s, ovf_seen);
+        if (!s.ok) break;
+        if (!done1) {
+          const gpq_item* ch = h.ch;
+          const gpq_item* sorted = hqg_sort<HqgItemOps>(h.ch, g.e2, nch, smem, s, [ch](uint32_t j) { return ch[j]; });
+          if (!hqg_insert(d, g, q, sorted, nch, smem, s)) break;
+        }
       }
       nch = 0;
     }
@@ -784,21 +1304,71 @@ static __global__ void __launch_bounds__(kHqgThreads, 1) hqg_phold_kernel(PholdD
       const gpq_item* root = q.root + q.off;
       const uint32_t c = hqg_cta_search(0, q.cnt0, [root, lim](uint32_t i) { return gpq_f2u(root[i].ts) >= lim; });
       if (c == 0) break;
-      if (c <= kHqgKeyTile) {
-        hqg_process_scan(d, g, root, c, nch, smem, s);
+      // LP-range lists for a large batch (a heap whose root holds every item)
+      bool from_lists = false;
+      uint32_t BP = 0;
+      if (g.pcnt != nullptr && blockIdx.x == 0)  // the next window's range counts start at zero
+        for (uint32_t k = threadIdx.x; k < kHqgMaxBuckets; k += blockDim.x)
+          g.pcnt[((steps + 1u) & 1u) * kHqgMaxBuckets + k] = 0u;
+      if (c > kHqgKeyTile && g.plist != nullptr && q.last == 0) {
+        uint32_t* pc = g.pcnt + (steps & 1u) * kHqgMaxBuckets;
+        BP = min(gridDim.x, max(1u, c / 64u));
+        hqg_file_batch(d, g, root, c, BP, pc, smem, s);
+        if (!s.ok) break;
+        for (uint32_t k = threadIdx.x; k < BP; k += blockDim.x) s_pc[k] = ld_relaxed_u32(&pc[k]);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          uint32_t sum = 0;
+          int ovf = 0;
+          for (uint32_t k = 0; k < BP; ++k) {
+            sum += s_pc[k];
+            ovf |= s_pc[k] > kHqgListCapP ? 1 : 0;
+          }
+          s_pc_sum = sum;
+          s_pc_ovf = ovf;
+        }
+        __syncthreads();
+        from_lists = !s_pc_ovf && s_pc_sum == c;
+      }
+      HqgIns ins{};
+      ins.on = g.ilist != nullptr && q.last == 0 && nch == 0;
+      if (ins.on) {
+        const uint32_t nr = q.cnt0 - c;
+        ins.BI = hqg_list_ibuckets(nr, c);
+        hqg_load_splitters(s_spl, root + c, nr, ins.BI);
+        ins.spl = s_spl;
+        ins.icnt = g.icnt + (steps & 1u) * kHqgMaxBuckets;
+        ins.ilist = g.ilist;
+      }
+      if (from_lists) {
+        hqg_process_lists(d, g, root, s_pc, BP, nch, ins, smem, s);
+      } else if (c <= kHqgKeyTile) {
+        hqg_process_scan(d, g, root, c, nch, ins, smem, s);
       } else {
         hqg_ranks(d, g, root, c, smem, s);
-        for (uint32_t i = hqg_tid(); i < c; i += hqg_nthreads()) {
-          const gpq_item e = root[i];
-          const uint64_t hh = gpq_ev_hash(e.id, gpq_f2u(e.ts));
-          const uint32_t add = g.addc[i];
-          if (add) d.count[e.lp] += add;  // the LP's one writer in this batch
-          atomicAdd(&d.csum[e.lp], (unsigned long long)hh);
-          atomicAdd(&d.ohash[e.lp], (unsigned long long)gpq_seq_hash(hh, (uint64_t)g.rank[i]));
-          h.ch[nch + i] = gpq_phold_child(d.p, e);
+        for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < c; i0 += hqg_nthreads()) {
+          const uint32_t i = i0 + threadIdx.x;
+          const bool valid = i < c;
+          gpq_item ch{};
+          if (valid) {
+            const gpq_item e = root[i];
+            const uint64_t hh = gpq_ev_hash(e.id, gpq_f2u(e.ts));
+            const uint32_t add = g.addc[i];
+            if (add) d.count[e.lp] += add;  // the LP's one writer in this batch
+            atomicAdd(&d.csum[e.lp], (unsigned long long)hh);
+            atomicAdd(&d.ohash[e.lp], (unsigned long long)gpq_seq_hash(hh, (uint64_t)g.rank[i]));
+            ch = gpq_phold_child(d.p, e);
+            h.ch[nch + i] = ch;
+          }
+          if (ins.on) {
+            const uint32_t bk = valid ? hqg_bucket_of(ins.spl, ins.BI - 1, ch) : 0u;
+            hqg_list_append<gpq_item>(ins.icnt, ins.ilist, kHqgListCapI, valid, bk, ch);
+          }
         }
         hqg_bar(s);
       }
+      lists.ins = ins.on;
+      lists.BI = ins.BI;
       nch += c;
       q.off += c;
       q.cnt0 -= c;

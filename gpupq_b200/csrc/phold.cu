@@ -145,7 +145,8 @@ struct gpq_phold {
                     (void*)hq_hist, (void*)hq_mm, (void*)lab.keys, (void*)lab.cnt, (void*)lab.spill,
                     (void*)lab.scnt, (void*)lab.wj, (void*)hqg.root2, (void*)hqg.t0, (void*)hqg.t1,
                     (void*)hqg.pa, (void*)hqg.pb, (void*)hqg.bref, (void*)hqg.k0, (void*)hqg.k1, (void*)hqg.rank,
-                    (void*)hqg.addc, (void*)hqg.ovf})
+                    (void*)hqg.addc, (void*)hqg.ovf, (void*)hqg.ilist, (void*)hqg.icnt, (void*)hqg.plist,
+                    (void*)hqg.pcnt})
       if (p) cudaFree(p);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -192,14 +193,21 @@ gpq_status gpq_phold_create(const gpq_phold_config* cfg_in, gpq_phold** out) {
   TRY(cudaEventCreate(&h->ev0));
   TRY(cudaEventCreate(&h->ev1));
   const size_t L = c.num_lps;
-  if (c.queue_kind == GPQ_QUEUE_HQ) {
+  // The global array queue as one sorted array in one launch: the heap kernel with a single
+  // node that holds the population.
+  const uint64_t pop = (uint64_t)c.num_lps * c.events_per_lp;
+  const bool gaq_array = c.queue_kind == GPQ_QUEUE_GAQ && c.gaq_engine == 0 && pop <= kHqgMaxR;
+  if (c.gaq_engine > 1) {
+    gpq::set_last_error("gaq_engine must be 0 or 1");
+    return fail(GPQ_ERR_INVALID);
+  }
+  if (c.queue_kind == GPQ_QUEUE_HQ || gaq_array) {
     // Default node size: the reference's 256 K root; a smaller population gets a root that
     // just holds it (a larger root changes nothing but its buffers' size).
-    uint32_t r = c.node_size;
+    uint32_t r = gaq_array ? 0u : c.node_size;
     if (r == 0) {
-      const uint64_t pop = (uint64_t)c.num_lps * c.events_per_lp;
       r = 2048;
-      while (r < pop && r < (256u << 10)) r <<= 1;
+      while (r < pop && r < (gaq_array ? kHqgMaxR : (256u << 10))) r <<= 1;
     }
     const bool grid = r > kHqMaxR;
     if (!gpq::is_pow2(r) || r < 2 || r > kHqgMaxR || (!grid && c.num_lps > (1u << 21))) {
@@ -233,6 +241,12 @@ gpq_status gpq_phold_create(const gpq_phold_config* cfg_in, gpq_phold** out) {
       TRY(cudaMalloc(&g.rank, (size_t)r * sizeof(uint32_t)));
       TRY(cudaMalloc(&g.addc, (size_t)r * sizeof(uint32_t)));
       TRY(cudaMalloc(&g.ovf, sizeof(uint32_t)));
+      if ((uint64_t)c.num_lps * c.events_per_lp <= r) {  // the root holds every item: bucket lists
+        TRY(cudaMalloc(&g.ilist, (size_t)kHqgMaxBuckets * kHqgListCapI * sizeof(gpq_item)));
+        TRY(cudaMalloc(&g.icnt, 2 * kHqgMaxBuckets * sizeof(uint32_t)));
+        TRY(cudaMalloc(&g.plist, (size_t)kHqgMaxBuckets * kHqgListCapP * sizeof(unsigned long long)));
+        TRY(cudaMalloc(&g.pcnt, 2 * kHqgMaxBuckets * sizeof(uint32_t)));
+      }
       g.e2 = h->hq_sort[0];  // after populate: the sort scratch of a window's children
       TRY(gpq::raise_smem_limit(hqg_phold_kernel, hqg_smem_bytes()));
       int per_sm = 0;
@@ -242,7 +256,7 @@ gpq_status gpq_phold_create(const gpq_phold_config* cfg_in, gpq_phold** out) {
         gpq::set_last_error("heap queue: the grid kernel does not fit on an SM");
         return fail(GPQ_ERR_INVALID);
       }
-      h->hqg_blocks = (uint32_t)h->num_sms;  // one CTA per SM: the barriers stay short
+      h->hqg_blocks = std::min<uint32_t>((uint32_t)h->num_sms, kHqgMaxBuckets);  // one CTA per SM
     } else {
       TRY(gpq::raise_smem_limit(hq_phold_kernel, (int)hq_smem_bytes(r)));
     }
@@ -263,7 +277,7 @@ gpq_status gpq_phold_create(const gpq_phold_config* cfg_in, gpq_phold** out) {
     TRY(cudaMalloc(&q.spill, 2 * L * q.F * sizeof(unsigned long long)));
     TRY(cudaMalloc(&q.scnt, 2 * L * sizeof(uint32_t)));
     TRY(cudaMalloc(&q.wj, 4 * sizeof(uint32_t)));
-  } else if (c.queue_kind != GPQ_QUEUE_GAQ) {
+  } else if (c.queue_kind != GPQ_QUEUE_GAQ) {  // per-LP queues
     TRY(cudaMalloc(&h->items, (L << h->cap_log2) * sizeof(gpq_item)));
     TRY(cudaMalloc(&h->qa, L * sizeof(uint32_t)));
     TRY(cudaMalloc(&h->qb, L * sizeof(uint32_t)));
@@ -457,6 +471,10 @@ static gpq_status run_hq(gpq_phold* h, uint32_t nsteps, int* done, cudaStream_t 
   if (h->hq_grid) {
     GPQ_CUDA_TRY(cudaMemsetAsync(&h->ctrl->bar, 0, sizeof(unsigned long long), st));
     GPQ_CUDA_TRY(cudaMemsetAsync(h->hqg.ovf, 0, sizeof(uint32_t), st));
+    if (h->hqg.icnt) {
+      GPQ_CUDA_TRY(cudaMemsetAsync(h->hqg.icnt, 0, 2 * kHqgMaxBuckets * sizeof(uint32_t), st));
+      GPQ_CUDA_TRY(cudaMemsetAsync(h->hqg.pcnt, 0, 2 * kHqgMaxBuckets * sizeof(uint32_t), st));
+    }
     PholdDev d = h->dev();
     HqgDev g = h->hqg;
     g.h = h->hq;

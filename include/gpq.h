@@ -206,7 +206,11 @@ typedef struct gpq_phold_config {
                                buckets of 8-byte keys per LP, each window's buckets ranked
                                (bucket geometry from lookahead and events_per_lp; capacity and
                                insert_capacity unused) */
-  uint32_t reserved[1];
+  uint32_t gaq_engine;      /* GAQ: 0 = one sorted array worked by the whole GPU in one
+                             * cooperative launch when the population fits 4 M items (the heap
+                             * kernel with a single node), else the kernel sequence below;
+                             * 1 = the kernel sequence per window (radix sort, merge) replayed
+                             * as a CUDA graph */
 } gpq_phold_config;
 
 typedef struct gpq_phold_result {

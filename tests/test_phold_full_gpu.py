@@ -40,17 +40,19 @@ def _check(name, queue="laq", laq_mode=0, loop="persistent", **kw):
 
 @pytest.mark.gpu
 @pytest.mark.slow
-@pytest.mark.parametrize("queue,laq_mode", [("laq", 2), ("laq", 0), ("gaq", 0)])
-def test_large_workload_full_end_time(gpu_lib, queue, laq_mode):
-    """65,536 LPs x 64, ring +-16, lookahead 0.1, end time 1000, seed 7."""
-    r = _check("phold_large_65536lp_x64_ring16_T1000", queue=queue, laq_mode=laq_mode, capacity=256)
+@pytest.mark.parametrize("queue,laq_mode,gaq_engine", [("laq", 2, 0), ("laq", 0, 0), ("gaq", 0, 0), ("gaq", 0, 1)])
+def test_large_workload_full_end_time(gpu_lib, queue, laq_mode, gaq_engine):
+    """65,536 LPs x 64, ring +-16, lookahead 0.1, end time 1000, seed 7 (the global array
+    queue as one sorted array in one launch, and as the graph-replayed kernel sequence)."""
+    r = _check("phold_large_65536lp_x64_ring16_T1000", queue=queue, laq_mode=laq_mode, capacity=256,
+               gaq_engine=gaq_engine)
     assert r["committed"] > 3_800_000_000
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("queue", ["laq", "lhq", "lsq", "gaq", "hq"])
-def test_plain_workload_every_kind(gpu_lib, queue):
-    _check("phold_plain_1024lp_x16_T100", queue=queue)
+@pytest.mark.parametrize("queue,gaq_engine", [("laq", 0), ("lhq", 0), ("lsq", 0), ("gaq", 0), ("gaq", 1), ("hq", 0)])
+def test_plain_workload_every_kind(gpu_lib, queue, gaq_engine):
+    _check("phold_plain_1024lp_x16_T100", queue=queue, gaq_engine=gaq_engine)
 
 
 def test_golden_one_per_lp_entries_agree_with_full_drain():

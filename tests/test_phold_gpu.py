@@ -31,6 +31,8 @@ def _run(cfgd, **kw):
         kw = dict(kw, queue="laq", laq_mode=1)
     if kw.get("queue") == "laqb":  # the local array queue's bucketed form
         kw = dict(kw, queue="laq", laq_mode=2)
+    if kw.get("queue") == "gaqg":  # the global array queue's graph-replayed kernel sequence
+        kw = dict(kw, queue="gaq", gaq_engine=1)
     cfg = G.make_phold_config(**cfgd, **kw)
     with G.Phold(cfg) as h:
         h.populate()
@@ -68,7 +70,7 @@ def test_children_match_oracle(gpu_lib):
 
 QUEUE_SHAPES = [("laq", 4), ("laq", 8), ("laq", 16), ("laq", 32), ("laqs", 4), ("laqs", 8), ("laqs", 32), ("laqb", 4),
                 ("laqb", 8), ("laqb", 16), ("laqb", 32), ("lhq", 1),
-                ("lhq", 8), ("lhq", 32), ("lsq", 1), ("gaq", 8), ("hq", 8)]
+                ("lhq", 8), ("lhq", 32), ("lsq", 1), ("gaq", 8), ("gaqg", 8), ("hq", 8)]
 
 
 @pytest.mark.parametrize("loop", ["plain", "persistent"])
@@ -95,7 +97,7 @@ def test_phold_heap_queue_node_sizes(gpu_lib, node_size):
     ("laq", "persistent", 16, 512), ("laq", "persistent", 32, 256), ("laqs", "persistent", 8, 128),
     ("laqs", "plain", 16, 256), ("laqb", "persistent", 4, 128), ("laqb", "persistent", 8, 128),
     ("laqb", "persistent", 16, 256), ("laqb", "plain", 8, 256), ("lhq", "persistent", 8, 128), ("lhq", "plain", 4, 256), ("lsq", "persistent", 1, 128), ("lsq", "plain", 1, 256),
-    ("gaq", "plain", 8, 256), ("hq", "persistent", 8, 256)])
+    ("gaq", "plain", 8, 256), ("gaqg", "plain", 8, 256), ("hq", "persistent", 8, 256)])
 def test_phold_large_reduced_bit_exact(gpu_lib, queue, loop, lanes, block):
     """The 65,536-LP ring workload cut to end time 3 (checked by the threaded oracle)."""
     cfgd = dict(num_lps=65536, events_per_lp=64, lookahead=0.1, end_time=3.0, seed=7, dest_mode=1, ring_width=16)
@@ -124,6 +126,7 @@ def test_phold_large_reduced_bit_exact(gpu_lib, queue, loop, lanes, block):
                                               ("laqb", "persistent", 8), ("laqb", "plain", 32), ("laqb", "persistent", 32),
                                               ("lhq", "persistent", 8), ("lhq", "plain", 1),
                                               ("lsq", "persistent", 1), ("lsq", "plain", 1), ("gaq", "plain", 8),
+                                              ("gaqg", "plain", 8),
                                               ("hq", "persistent", 8)])
 def test_phold_edge_shapes(gpu_lib, cfgd, kw, queue, loop, lanes):
     o = _oracle(cfgd)

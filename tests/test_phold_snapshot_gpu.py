@@ -11,10 +11,12 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 C1 = dict(num_lps=1024, events_per_lp=16, lookahead=1.0, end_time=100.0, seed=42, dest_mode=0)
-KINDS = [("laq", 0), ("laq", 1), ("laq", 2), ("lhq", 0), ("lsq", 0), ("gaq", 0), ("hq", 0)]
+KINDS = [("laq", 0), ("laq", 1), ("laq", 2), ("lhq", 0), ("lsq", 0), ("gaq", 0), ("gaqg", 0), ("hq", 0)]
 
 
 def _cfg(queue, mode, loop="plain", **over):
+    if queue == "gaqg":  # the global array queue's graph-replayed kernel sequence
+        return G.make_phold_config(**dict(C1, **over), queue="gaq", gaq_engine=1, loop=loop)
     return G.make_phold_config(**dict(C1, **over), queue=queue, laq_mode=mode, loop=loop)
 
 

@@ -225,6 +225,22 @@ def _alone(case, queue):
 
 
 KEYS = ("committed", "steps", "pending", "pending_csum", "digest", "final_min")
+ORACLE_KEYS = ("committed", "steps", "pending", "pending_csum", "digest")
+_ORACLE_RUNS = {}
+
+
+def _oracle_run(case):
+    """The unsharded CPU oracle of a GPU case (the checker for the sharded device runs)."""
+    key = tuple(sorted(case.items()))
+    if key not in _ORACLE_RUNS:
+        _ORACLE_RUNS[key] = O.phold(O.make_cfg(**case), threads=4)
+    return _ORACLE_RUNS[key]
+
+
+def _assert_oracle(res, case):
+    want = _oracle_run(case)
+    for k in ORACLE_KEYS:
+        assert res[k] == want[k], (k, res[k], want[k])
 
 
 @pytest.mark.gpu
@@ -244,6 +260,7 @@ def test_device_shards_in_one_process(gpu_lib, case, world, queue):
     for k in KEYS:
         assert res[k] == want[k], (k, res[k], want[k])
     assert res["status"] == 0
+    _assert_oracle(res, c)
 
 
 def _device_worker(rank, world, port, case, q):
@@ -279,6 +296,7 @@ def test_device_shards_over_gloo(gpu_lib):
     want = _alone(c, "laq")
     for k in KEYS:
         assert res[k] == want[k], (k, res[k], want[k])
+    _assert_oracle(res, c)
 
 
 @pytest.mark.gpu
