@@ -665,6 +665,17 @@ def run_case(name):
                 h.run()
                 r = h.result()
             print(r["committed"], r["steps"], r["elapsed_ms"], h.launch_info())
+    elif name == "gaq_array_c2_t20":
+        # the 65,536-LP ring workload to end time 20 through the global array queue as one
+        # sorted array in one launch (76 M events, 200 windows), two runs
+        cfgd = {k: WORKLOAD[k] for k in ("num_lps", "events_per_lp", "lookahead", "seed", "dest_mode", "ring_width")}
+        cfg = G.make_phold_config(**cfgd, end_time=20.0, queue="gaq", capacity=256)
+        with G.Phold(cfg) as h:
+            for _ in range(2):
+                h.populate()
+                h.run()
+                r = h.result()
+            print(r["committed"], r["steps"], r["elapsed_ms"], h.launch_info())
     elif name == "astar_ref_2048":
         m = G.astar_ref_map(256, 256, 0.2, 1.0, seed=14580)
         agents = G.astar_ref_agents(m, 4096, seed=11)
@@ -707,7 +718,7 @@ def main():
     ap.add_argument("--served-seconds", type=float, default=1.0, help="length of the served request stream")
     ap.add_argument("--case", default=None,
                     choices=["astar_batched_1000", "astar_plain_2048", "phold_batched_36", "gaq_sort_32m",
-                             "astar_ref_2048", "phold_c1_heap"],
+                             "astar_ref_2048", "phold_c1_heap", "gaq_array_c2_t20"],
                     help="run one small named workload twice and exit (profiling captures)")
     args = ap.parse_args()
     if args.case:
