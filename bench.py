@@ -896,6 +896,9 @@ def main():
                  "astar_reference_semantics": bench_astar_ref(G, O, args, peak),
                  "phold_batched": bench_phold_batched(G, O, args, peak),
                  "served": bench_served(G, args, args.served_seconds)}
+        if cpu is not None:  # the global array queue form runs the headline's workload
+            forms["phold_c2_gaq"]["cpu_baseline"] = dict(cpu, note="the same workload and CPU runs as the line's "
+                                                                   "cpu_baseline")
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,

@@ -94,7 +94,27 @@ struct LabCtx {
   uint32_t lp_base;    // the run's first LP in the LP space
   uint32_t* err;       // the run's sticky error word
   uint32_t* err_slot;  // error slot read by the next window's exit decision
+  // A shard of a sharded run owns LPs [lp_begin, lp_end); a child for another shard's LP
+  // goes to outbox[dest][out_cap] (dest = lp / shard_lps, count out_n[dest]) for the host
+  // to hand over between windows.  outbox == nullptr: every LP is local.
+  gpq_item* outbox = nullptr;
+  uint32_t* out_n = nullptr;
+  uint32_t out_cap = 0, shard_lps = 1, lp_begin = 0, lp_end = 0xffffffffu;
 };
+
+// A child of another shard's LP into the outbox; returns false for a local child.
+__device__ __forceinline__ bool lab_handover(const LabCtx& x, const gpq_item& ch) {
+  if (x.outbox == nullptr || (ch.lp >= x.lp_begin && ch.lp < x.lp_end)) return false;
+  const uint32_t dest = ch.lp / x.shard_lps;
+  const uint32_t slot = atomicAdd(&x.out_n[dest], 1u);
+  if (slot < x.out_cap) {
+    x.outbox[(size_t)dest * x.out_cap + slot] = ch;
+  } else {
+    gpq_set_error(x.err, GPQ_ERR_INSERT_FULL);
+    atomicOr(x.err_slot, 1u);
+  }
+  return true;
+}
 
 __device__ __forceinline__ void lab_fail(const LabCtx& x, uint32_t code) {
   gpq_set_error(x.err, code);
@@ -168,7 +188,7 @@ __device__ __forceinline__ uint32_t lab_process_event(const LabCtx& x, const Lab
   atomicAdd(&st.ohash[slot], (unsigned long long)gpq_seq_hash(h, (uint64_t)st.seq0[slot] + idx));
   const gpq_item ch = lab_child(x, e);
   const uint32_t cb = gpq_f2u(ch.ts);
-  lab_push(x, q, ch.lp, lab_key(cb, ch.id), lab_bucket(cb, w.inv_w), w);
+  if (!lab_handover(x, ch)) lab_push(x, q, ch.lp, lab_key(cb, ch.id), lab_bucket(cb, w.inv_w), w);
   return cb;
 }
 
@@ -604,10 +624,12 @@ __device__ __forceinline__ uint32_t lab_event_batch(const LabCtx& x, const LabDe
         atomicAdd(&st.ohash[slot], (unsigned long long)gpq_seq_hash(h, (uint64_t)st.seq0[slot] + idx));
         const gpq_item ch = lab_child(x, e);
         const uint32_t cb = gpq_f2u(ch.ts);
-        key[u] = lab_key(cb, ch.id);
-        lp[u] = ch.lp;
-        jb[u] = lab_bucket(cb, w.inv_w);
         mn = min(mn, cb);
+        if (!lab_handover(x, ch)) {
+          key[u] = lab_key(cb, ch.id);
+          lp[u] = ch.lp;
+          jb[u] = lab_bucket(cb, w.inv_w);
+        }
       }
     }
   }
@@ -914,7 +936,15 @@ __device__ __forceinline__ void lab_window_body(const PholdDev& d, const LabDev&
                                                 unsigned char* smem_raw, uint32_t* red, uint32_t lp_lo,
                                                 uint32_t lp_hi, bool resident) {
   const LabWin w = lab_window(d, q, s, m);
-  const LabCtx x{d.p, d.L, 0u, &d.ctrl->err, &d.ctrl->errs[(s + 1u) % 3u]};
+  LabCtx x{d.p, d.L, 0u, &d.ctrl->err, &d.ctrl->errs[(s + 1u) % 3u]};
+  if (d.outbox != nullptr) {
+    x.outbox = d.outbox;
+    x.out_n = d.out_n;
+    x.out_cap = d.out_cap;
+    x.shard_lps = d.shard_lps;
+    x.lp_begin = d.lp_begin;
+    x.lp_end = d.lp_end;
+  }
   const uint32_t warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const LabWarpSmem sm = lab_warp_smem(smem_raw + (size_t)warp * lab_warp_smem_bytes());
   const uint32_t pw = (lp_hi - lp_lo + nw - 1u) / nw;
@@ -947,8 +977,8 @@ static __global__ void __launch_bounds__(1024, 1) lab_window_kernel(PholdDev d, 
     d.ctrl->phase = s + 1u;
     q.wj[s & 3u] = lab_bucket(gpq_f2u(GPQ_FADD(m, d.p.lookahead)), q.inv_w);
   }
-  const uint32_t per = (blockDim.x / 32u) * q.chunk;
-  const uint32_t lp_lo = min(d.L, blockIdx.x * per), lp_hi = min(d.L, lp_lo + per);
+  const uint32_t per = (blockDim.x / 32u) * q.chunk;  // a shard works its own LPs [lp_begin, lp_end)
+  const uint32_t lp_lo = min(d.lp_end, d.lp_begin + blockIdx.x * per), lp_hi = min(d.lp_end, lp_lo + per);
   lab_window_body(d, q, s, m, smem_raw, red, lp_lo, lp_hi, false);
 }
 
@@ -1000,6 +1030,14 @@ static __global__ void lab_populate_kernel(PholdDev d, LabDev q, uint32_t per_lp
   uint32_t mn = kInfBits;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t lp = (uint32_t)(i / per_lp), k = (uint32_t)(i % per_lp);
+    if (lp < d.lp_begin || lp >= d.lp_end) {  // another shard's LP: outputs only
+      if (k == 0) {
+        d.count[lp] = 0;
+        d.csum[lp] = 0;
+        d.ohash[lp] = 0;
+      }
+      continue;
+    }
     gpq_item e;
     if (src) {
       e = src[i];
@@ -1036,6 +1074,25 @@ static __global__ void lab_populate_kernel(PholdDev d, LabDev q, uint32_t per_lp
   if (threadIdx.x == 0 && mn != kInfBits) atomicMin(&d.ctrl->mins[0], mn);
 }
 
+// A shard's handed-over children of window s (made by other shards, all for this shard's
+// LPs), filed as if this shard had pushed them during window s: bucket or spill list of the
+// window's parity.
+static __global__ void lab_inject_kernel(PholdDev d, LabDev q, const gpq_item* __restrict__ items, uint64_t n,
+                                         uint32_t s) {
+  const float m = gpq_u2f(d.ctrl->mins[s % 3u]);
+  const LabWin w = lab_window(d, q, s, m);
+  const LabCtx x{d.p, d.L, 0u, &d.ctrl->err, &d.ctrl->errs[(s + 1u) % 3u]};
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const gpq_item it = items[i];
+    if (it.lp < d.lp_begin || it.lp >= d.lp_end) {
+      gpq_set_error(&d.ctrl->err, GPQ_ERR_INVALID);
+      continue;
+    }
+    const uint32_t tb = gpq_f2u(it.ts);
+    lab_push(x, q, it.lp, lab_key(tb, it.id), lab_bucket(tb, w.inv_w), w);
+  }
+}
+
 // End of run: committed total, pending events (the live keys of the buckets + the spill
 // list of the last window) and the order-sensitive digest.  One warp per LP.
 static __global__ void lab_finalize_kernel(PholdDev d, LabDev q, PholdAcc* acc) {
@@ -1048,7 +1105,7 @@ static __global__ void lab_finalize_kernel(PholdDev d, LabDev q, PholdAcc* acc) 
   const uint32_t NB = 1u << q.nb_log2, C = 1u << q.c_log2;
   uint64_t pend = 0, pcs = 0, dig = 0, com = 0;
   uint32_t pmin = kInfBits;
-  for (uint32_t lp = blockIdx.x * wpb + (threadIdx.x >> 5); lp < d.L; lp += nwarps) {
+  for (uint32_t lp = d.lp_begin + blockIdx.x * wpb + (threadIdx.x >> 5); lp < d.lp_end; lp += nwarps) {  // a shard: its LPs
     const size_t lpb = (size_t)lp << q.nb_log2;
     for (uint32_t b0 = 0; b0 < NB; b0 += 32) {
       const uint32_t c = (b0 + lane < NB) ? min(q.cnt[lpb + b0 + lane], C) : 0u;

@@ -807,9 +807,8 @@ gpq_status gpq_phold_shard_create(const gpq_phold_config* cfg, uint32_t rank, ui
   GPQ_CHECK_ARG(cfg && out, "NULL argument");
   *out = nullptr;
   GPQ_CHECK_ARG(world >= 1 && rank < world, "need world >= 1 and rank < world");
-  GPQ_CHECK_ARG(cfg->queue_kind == GPQ_QUEUE_LHQ || cfg->queue_kind == GPQ_QUEUE_LSQ ||
-                    (cfg->queue_kind == GPQ_QUEUE_LAQ && cfg->laq_mode != 2),
-                "sharded runs take the per-LP queue kinds (LAQ sorted or selection form, LHQ, LSQ)");
+  GPQ_CHECK_ARG(cfg->queue_kind == GPQ_QUEUE_LHQ || cfg->queue_kind == GPQ_QUEUE_LSQ || cfg->queue_kind == GPQ_QUEUE_LAQ,
+                "sharded runs take the per-LP queue kinds (LAQ in any form, LHQ, LSQ)");
   GPQ_CHECK_ARG(cfg->num_lps >= world, "need at least one LP per shard");
   gpq_phold* h = nullptr;
   gpq_status r = gpq_phold_create(cfg, &h);
@@ -821,10 +820,11 @@ gpq_status gpq_phold_shard_create(const gpq_phold_config* cfg, uint32_t rank, ui
   h->shard_lps = (uint32_t)(((uint64_t)L + world - 1) / world);
   h->lp_begin = std::min<uint32_t>(L, rank * h->shard_lps);
   h->lp_end = (uint32_t)std::min<uint64_t>(L, (uint64_t)h->lp_begin + h->shard_lps);
-  // default: as many handed-over children per destination as this shard's insert buffers hold
+  // default: as many handed-over children per destination as this shard's insert buffers
+  // hold (the bucketed form: as many as its LPs hold pending events)
+  const uint64_t per_lp = h->is_lab ? h->cfg.events_per_lp : h->cfg.insert_capacity;
   h->out_cap = outbox_capacity ? outbox_capacity
-                               : (uint32_t)std::min<uint64_t>((uint64_t)(h->lp_end - h->lp_begin) * h->cfg.insert_capacity,
-                                                              1u << 26);
+                               : (uint32_t)std::min<uint64_t>((uint64_t)(h->lp_end - h->lp_begin) * per_lp, 1u << 26);
   cudaError_t e = cudaMalloc(&h->outbox, std::max<uint64_t>(1, (uint64_t)world * h->out_cap) * sizeof(gpq_item));
   if (e == cudaSuccess) e = cudaMalloc(&h->out_n, world * sizeof(uint32_t));
   if (e != cudaSuccess) {
@@ -865,14 +865,17 @@ gpq_status gpq_phold_shard_window(gpq_phold* h, float global_min, float* local_m
   const uint32_t mb = gpq_f2u(global_min);
   GPQ_CUDA_TRY(cudaMemcpyAsync(&h->ctrl->mins[s % 3], &mb, sizeof(mb), cudaMemcpyHostToDevice, st));
   GPQ_CUDA_TRY(cudaMemsetAsync(h->out_n, 0, h->world * sizeof(uint32_t), st));
-  const uint32_t gpb = h->block / h->ks.group;  // LPs per CTA and round
+  const uint32_t gpb = h->is_lab ? lab_plain_lps_per_cta(h->block, h->lab.chunk)
+                                 : h->block / h->ks.group;  // LPs per CTA and round
   const uint32_t grid = std::max(1u, (h->lp_end - h->lp_begin + gpb - 1) / gpb);
   PholdDev d = h->dev();
   LpQueueDev q = h->lq();
   InsDev ib = h->ins();
   uint32_t phase = s;
   void* args[] = {&d, &q, &ib, &phase};
-  GPQ_CUDA_TRY(cudaLaunchKernel(h->ks.window, dim3(grid), dim3(h->block), args, h->window_smem(), st));
+  void* lab_args[] = {&d, &h->lab, &phase};
+  GPQ_CUDA_TRY(cudaLaunchKernel(h->ks.window, dim3(grid), dim3(h->block), h->is_lab ? lab_args : args,
+                                h->window_smem(), st));
   ++h->phase;
   GPQ_CUDA_TRY(cudaMemcpyAsync(h->h_ctrl, h->ctrl, sizeof(PholdCtrl), cudaMemcpyDeviceToHost, st));
   GPQ_CUDA_TRY(cudaMemcpyAsync(out_counts, h->out_n, h->world * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
@@ -911,7 +914,10 @@ gpq_status gpq_phold_shard_inject(gpq_phold* h, const gpq_item* items, uint64_t 
     src = h->inject_buf;
   }
   const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, 4096));
-  phold_inject_kernel<<<grid, 256, 0, st>>>(h->dev(), h->ins(), src, n, (h->phase - 1) & 1u);
+  if (h->is_lab)
+    lab_inject_kernel<<<grid, 256, 0, st>>>(h->dev(), h->lab, src, n, h->phase - 1);
+  else
+    phold_inject_kernel<<<grid, 256, 0, st>>>(h->dev(), h->ins(), src, n, (h->phase - 1) & 1u);
   GPQ_CUDA_TRY(cudaGetLastError());
   GPQ_CUDA_TRY(cudaMemcpyAsync(h->h_ctrl, h->ctrl, sizeof(PholdCtrl), cudaMemcpyDeviceToHost, st));
   GPQ_CUDA_TRY(cudaStreamSynchronize(st));

@@ -275,13 +275,15 @@ GPQ_API gpq_status gpq_phold_restore(gpq_phold* h, const void* buf, uint64_t siz
  *   window(global minimum) -> the shard's safe events run; children for other shards'
  *     LPs wait in the outbox ([world][capacity] device items, counts per destination);
  *     local minimum (pending events and all children, handed over or not);
- *   inject(the items other shards handed to this one) -> merged in the next window;
+ *   inject(the items other shards handed to this one) -> merged in the next window (the
+ *     bucketed local array queue files them at once, as if pushed in the window run);
  *   repeat while the global minimum is below end_time.
  * A child is never safe in its parent's window, so handing children over between windows
  * changes no result: the shards' committed counts, pending events and digests add up
  * (final minimum: the minimum) to those of the unsharded run.  Per-LP queue kinds only
- * (LAQ sorted or selection form, LHQ, LSQ).  outbox_capacity 0 = the shard's LPs times
- * insert_capacity per destination.  gpq_phold_result_get gives the shard's part. */
+ * (LAQ in every form, LHQ, LSQ).  outbox_capacity 0 = the shard's LPs times
+ * insert_capacity (bucketed form: events_per_lp) per destination.  gpq_phold_result_get
+ * gives the shard's part. */
 GPQ_API gpq_status gpq_phold_shard_create(const gpq_phold_config* cfg, uint32_t rank, uint32_t world,
                                           uint32_t outbox_capacity, gpq_phold** out);
 GPQ_API gpq_status gpq_phold_shard_range(gpq_phold* h, uint32_t* lp_begin, uint32_t* lp_end, uint32_t* outbox_capacity);

@@ -211,9 +211,12 @@ GPU_CASES = [dict(num_lps=3000, events_per_lp=8, lookahead=0.5, end_time=40.0, s
 
 def _gpu_cfg(case, queue):
     import gpupq_b200 as G
+    laq_mode = 0
+    if queue == "laqb":  # the local array queue's bucketed form
+        queue, laq_mode = "laq", 2
     return G.make_phold_config(case["num_lps"], case["events_per_lp"], case["lookahead"], case["end_time"],
                                case["seed"], dest_mode=case["dest_mode"], ring_width=case.get("ring_width", 16),
-                               queue=queue, capacity=256, insert_capacity=64, loop="plain")
+                               queue=queue, capacity=256, insert_capacity=64, loop="plain", laq_mode=laq_mode)
 
 
 def _alone(case, queue):
@@ -244,7 +247,7 @@ def _assert_oracle(res, case):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("queue", ["laq", "lhq", "lsq"])
+@pytest.mark.parametrize("queue", ["laq", "laqb", "lhq", "lsq"])
 @pytest.mark.parametrize("world", [1, 2, 3])
 @pytest.mark.parametrize("case", range(len(GPU_CASES)))
 def test_device_shards_in_one_process(gpu_lib, case, world, queue):
@@ -263,7 +266,7 @@ def test_device_shards_in_one_process(gpu_lib, case, world, queue):
     _assert_oracle(res, c)
 
 
-def _device_worker(rank, world, port, case, q):
+def _device_worker(rank, world, port, case, q, queue="laq"):
     import datetime
     import torch.distributed as dist
     sys.path.insert(0, ROOT)
@@ -272,7 +275,7 @@ def _device_worker(rank, world, port, case, q):
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
     try:
-        with S.PholdShard(_gpu_cfg(case, "laq"), rank, world) as sh:
+        with S.PholdShard(_gpu_cfg(case, queue), rank, world) as sh:
             res = S.run_distributed(sh, case["end_time"])
         if rank == 0:
             q.put(res)
@@ -281,19 +284,20 @@ def _device_worker(rank, world, port, case, q):
 
 
 @pytest.mark.gpu
-def test_device_shards_over_gloo(gpu_lib):
+@pytest.mark.parametrize("queue", ["laq", "laqb"])
+def test_device_shards_over_gloo(gpu_lib, queue):
     c = GPU_CASES[1]
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_device_worker, args=(r, 2, port, c, q)) for r in range(2)]
+    procs = [ctx.Process(target=_device_worker, args=(r, 2, port, c, q, queue)) for r in range(2)]
     for p in procs:
         p.start()
     res = q.get(timeout=300)
     for p in procs:
         p.join(120)
         assert p.exitcode == 0
-    want = _alone(c, "laq")
+    want = _alone(c, queue)
     for k in KEYS:
         assert res[k] == want[k], (k, res[k], want[k])
     _assert_oracle(res, c)
