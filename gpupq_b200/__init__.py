@@ -110,6 +110,7 @@ _SIGS = {
     "gpq_phold_shard_window": ([_VP, ctypes.c_float, ctypes.POINTER(ctypes.c_float), _VP, _VP], ctypes.c_int),
     "gpq_phold_shard_outbox": ([_VP, ctypes.POINTER(_VP), ctypes.POINTER(ctypes.c_uint32)], ctypes.c_int),
     "gpq_phold_shard_inject": ([_VP, _VP, ctypes.c_uint64, ctypes.c_int, _VP], ctypes.c_int),
+    "gpq_phold_shard_connect": ([_VP, _VP, ctypes.c_uint32], ctypes.c_int),
     "gpq_phold_launch_info": ([_VP, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32),
                                ctypes.POINTER(ctypes.c_uint32)], ctypes.c_int),
     "gpq_phold_run_static": ([ctypes.POINTER(PholdConfig), _VP, _VP, _VP, _VP, ctypes.POINTER(PholdResult), _VP],

@@ -49,6 +49,14 @@ struct LabDev {
   uint32_t chunk;             // LPs per warp chunk (lab_chunk_lps)
 };
 
+// One shard's bucket arrays, for another shard's direct hand-over.
+struct LabPeer {
+  unsigned long long* keys;
+  uint32_t* cnt;
+  unsigned long long* spill;
+  uint32_t* scnt;
+};
+
 static constexpr uint32_t kLabSafeCap = 32;  // safe keys of one LP per window ranked in shared memory
 
 __host__ __device__ inline size_t lab_group_smem_bytes() { return (size_t)kLabSafeCap * 8; }
@@ -100,21 +108,8 @@ struct LabCtx {
   gpq_item* outbox = nullptr;
   uint32_t* out_n = nullptr;
   uint32_t out_cap = 0, shard_lps = 1, lp_begin = 0, lp_end = 0xffffffffu;
+  const LabPeer* peers = nullptr;  // direct hand-over: every shard's bucket arrays
 };
-
-// A child of another shard's LP into the outbox; returns false for a local child.
-__device__ __forceinline__ bool lab_handover(const LabCtx& x, const gpq_item& ch) {
-  if (x.outbox == nullptr || (ch.lp >= x.lp_begin && ch.lp < x.lp_end)) return false;
-  const uint32_t dest = ch.lp / x.shard_lps;
-  const uint32_t slot = atomicAdd(&x.out_n[dest], 1u);
-  if (slot < x.out_cap) {
-    x.outbox[(size_t)dest * x.out_cap + slot] = ch;
-  } else {
-    gpq_set_error(x.err, GPQ_ERR_INSERT_FULL);
-    atomicOr(x.err_slot, 1u);
-  }
-  return true;
-}
 
 __device__ __forceinline__ void lab_fail(const LabCtx& x, uint32_t code) {
   gpq_set_error(x.err, code);
@@ -176,6 +171,34 @@ __device__ __forceinline__ void lab_push(const LabCtx& x, const LabDev& q, uint3
   }
 }
 
+// A child of another shard's LP: filed straight into that shard's buckets (connected
+// shards: the same append rule as a local child -- every shard runs window w with the same
+// bound and bucket geometry, and an append lands at or above j1, which the owner does not
+// compact during the window), or into the outbox.  Returns false for a local child.
+__device__ __forceinline__ bool lab_handover(const LabCtx& x, const LabDev& q, const LabWin& w, const gpq_item& ch) {
+  if (x.outbox == nullptr || (ch.lp >= x.lp_begin && ch.lp < x.lp_end)) return false;
+  const uint32_t dest = ch.lp / x.shard_lps;
+  if (x.peers != nullptr) {
+    const LabPeer P = x.peers[dest];
+    LabDev qd = q;
+    qd.keys = P.keys;
+    qd.cnt = P.cnt;
+    qd.spill = P.spill;
+    qd.scnt = P.scnt;
+    const uint32_t cb = gpq_f2u(ch.ts);
+    lab_push(x, qd, ch.lp, lab_key(cb, ch.id), lab_bucket(cb, w.inv_w), w);
+    return true;
+  }
+  const uint32_t slot = atomicAdd(&x.out_n[dest], 1u);
+  if (slot < x.out_cap) {
+    x.outbox[(size_t)dest * x.out_cap + slot] = ch;
+  } else {
+    gpq_set_error(x.err, GPQ_ERR_INSERT_FULL);
+    atomicOr(x.err_slot, 1u);
+  }
+  return true;
+}
+
 // Process one staged event: per-LP hashes into the slot accumulators, the child into its
 // bucket.  Returns the child's timestamp bits.
 __device__ __forceinline__ uint32_t lab_process_event(const LabCtx& x, const LabDev& q, const PholdStage& st,
@@ -188,7 +211,7 @@ __device__ __forceinline__ uint32_t lab_process_event(const LabCtx& x, const Lab
   atomicAdd(&st.ohash[slot], (unsigned long long)gpq_seq_hash(h, (uint64_t)st.seq0[slot] + idx));
   const gpq_item ch = lab_child(x, e);
   const uint32_t cb = gpq_f2u(ch.ts);
-  if (!lab_handover(x, ch)) lab_push(x, q, ch.lp, lab_key(cb, ch.id), lab_bucket(cb, w.inv_w), w);
+  if (!lab_handover(x, q, w, ch)) lab_push(x, q, ch.lp, lab_key(cb, ch.id), lab_bucket(cb, w.inv_w), w);
   return cb;
 }
 
@@ -625,7 +648,7 @@ __device__ __forceinline__ uint32_t lab_event_batch(const LabCtx& x, const LabDe
         const gpq_item ch = lab_child(x, e);
         const uint32_t cb = gpq_f2u(ch.ts);
         mn = min(mn, cb);
-        if (!lab_handover(x, ch)) {
+        if (!lab_handover(x, q, w, ch)) {
           key[u] = lab_key(cb, ch.id);
           lp[u] = ch.lp;
           jb[u] = lab_bucket(cb, w.inv_w);
@@ -944,6 +967,7 @@ __device__ __forceinline__ void lab_window_body(const PholdDev& d, const LabDev&
     x.shard_lps = d.shard_lps;
     x.lp_begin = d.lp_begin;
     x.lp_end = d.lp_end;
+    x.peers = static_cast<const LabPeer*>(d.peers);
   }
   const uint32_t warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const LabWarpSmem sm = lab_warp_smem(smem_raw + (size_t)warp * lab_warp_smem_bytes());

@@ -67,6 +67,7 @@ struct gpq_phold {
   // destination shard
   bool sharded = false;
   uint32_t rank = 0, world = 1, lp_begin = 0, lp_end = 0, shard_lps = 0, out_cap = 0;
+  LabPeer* lab_peers = nullptr;  // connected bucketed shards: [world] bucket arrays (device)
   gpq_item* outbox = nullptr;   // [world][out_cap]
   uint32_t* out_n = nullptr;    // [world]
   gpq_item* inject_buf = nullptr;
@@ -97,6 +98,7 @@ struct gpq_phold {
     d.out_cap = out_cap;
     d.outbox = sharded ? outbox : nullptr;
     d.out_n = out_n;
+    d.peers = sharded ? lab_peers : nullptr;
     return d;
   }
   LpQueueDev lq() const {
@@ -137,7 +139,7 @@ struct gpq_phold {
   ~gpq_phold() {
     for (void* p : {(void*)items, (void*)qa, (void*)qb, (void*)qc, (void*)links, (void*)freestk, (void*)ibuf,
                     (void*)icnt, (void*)count, (void*)csum, (void*)ohash, (void*)ctrl, (void*)acc, (void*)staging,
-                    (void*)outbox, (void*)out_n, (void*)inject_buf})
+                    (void*)outbox, (void*)out_n, (void*)inject_buf, (void*)lab_peers})
       if (p) cudaFree(p);
     if (h_ctrl) cudaFreeHost(h_ctrl);
     if (gaq) gpq::gaq_engine_destroy(gaq);
@@ -925,6 +927,30 @@ gpq_status gpq_phold_shard_inject(gpq_phold* h, const gpq_item* items, uint64_t 
     gpq::set_last_error("sharded PHOLD: handed-over items rejected (error %u)", h->h_ctrl->err);
     return (gpq_status)h->h_ctrl->err;
   }
+  return GPQ_OK;
+}
+
+gpq_status gpq_phold_shard_connect(gpq_phold* h, gpq_phold* const* shards, uint32_t world) {
+  GPQ_CHECK_ARG(h && h->sharded && shards, "not a shard handle or NULL argument");
+  GPQ_CHECK_ARG(h->is_lab, "direct hand-over connects the bucketed local array queue's shards (laq_mode 2)");
+  GPQ_CHECK_ARG(world == h->world, "world differs from the shard's");
+  std::vector<LabPeer> tab(world);
+  for (uint32_t r = 0; r < world; ++r) {
+    const gpq_phold* o = shards[r];
+    GPQ_CHECK_ARG(o && o->sharded && o->is_lab && o->rank == r && o->world == world, "shards[r] must be shard r");
+    GPQ_CHECK_ARG(std::memcmp(&o->cfg, &h->cfg, sizeof(h->cfg)) == 0, "every shard must run the same configuration");
+    if (o->device != h->device) {  // another GPU: its memory through peer access
+      int can = 0;
+      GPQ_CUDA_TRY(cudaDeviceCanAccessPeer(&can, h->device, o->device));
+      GPQ_CHECK_ARG(can, "no peer access between the shards' GPUs");
+      const cudaError_t e = cudaDeviceEnablePeerAccess(o->device, 0);
+      if (e != cudaSuccess && e != cudaErrorPeerAccessAlreadyEnabled) GPQ_CUDA_TRY(e);
+      (void)cudaGetLastError();
+    }
+    tab[r] = LabPeer{o->lab.keys, o->lab.cnt, o->lab.spill, o->lab.scnt};
+  }
+  if (h->lab_peers == nullptr) GPQ_CUDA_TRY(cudaMalloc(&h->lab_peers, world * sizeof(LabPeer)));
+  GPQ_CUDA_TRY(cudaMemcpy(h->lab_peers, tab.data(), world * sizeof(LabPeer), cudaMemcpyHostToDevice));
   return GPQ_OK;
 }
 

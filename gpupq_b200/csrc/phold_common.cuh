@@ -38,6 +38,10 @@ struct PholdDev {
   uint32_t out_cap;
   gpq_item* outbox;
   uint32_t* out_n;
+  // Sharded runs of the bucketed local array queue connected for direct hand-over: every
+  // shard's bucket arrays ([world] LabPeer, lab.cuh); a child for another shard's LP is
+  // filed straight into that shard's buckets.  nullptr: hand-over through the outbox.
+  const void* peers;
 };
 
 // A group of G consecutive lanes of one warp working on one LP.

@@ -126,6 +126,27 @@ def combine(parts):
     return out
 
 
+def connect(shards):
+    """Direct hand-over between the bucketed local array queue's shards of one process
+    (gpq_phold_shard_connect): a child for another shard's LP is filed straight into that
+    shard's buckets by the window that makes it, so windows need no exchange -- only the
+    minimum over shards."""
+    arr = (ctypes.c_void_p * len(shards))(*[s._h.value for s in shards])
+    for s in shards:
+        check(lib().gpq_phold_shard_connect(s._h, ctypes.cast(arr, ctypes.c_void_p), len(shards)),
+              "gpq_phold_shard_connect")
+
+
+def run_local_direct(shards, end_time):
+    """Drive connected shards of one process (see connect) to the end of the run: per
+    window every shard runs with the global minimum, then the minimum over the shards'
+    local minima; returns the combined result."""
+    m = min(s.populate() for s in shards)
+    while m < end_time:
+        m = min(s.window(m)[0] for s in shards)
+    return combine([s.result() for s in shards])
+
+
 def run_local(shards, end_time):
     """Drive the shards of one process (shard r at position r) to the end of the run;
     returns the combined result."""

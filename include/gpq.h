@@ -293,6 +293,14 @@ GPQ_API gpq_status gpq_phold_shard_window(gpq_phold* h, float global_min, float*
 GPQ_API gpq_status gpq_phold_shard_outbox(gpq_phold* h, gpq_item** items, uint32_t* capacity);
 GPQ_API gpq_status gpq_phold_shard_inject(gpq_phold* h, const gpq_item* items, uint64_t n, int on_device,
                                           void* stream);
+/* Direct hand-over for the bucketed local array queue's shards (laq_mode 2) of one
+ * process: shards[r] is shard r of the same run (same configuration), on this GPU or on a
+ * GPU this one has peer access to (enabled here).  Afterwards the shard's windows file a
+ * child of another shard's LP straight into that shard's time buckets (stores into its
+ * memory; the same append rule as a local child), so no outbox, exchange or inject is
+ * needed between windows -- only the minimum over the shards' local minima.  Call it for
+ * every shard, after all of them are created and before the first window. */
+GPQ_API gpq_status gpq_phold_shard_connect(gpq_phold* h, gpq_phold* const* shards, uint32_t world);
 
 /* Launch geometry of the last gpq_phold_run: persistent grid (CTAs), CTA size, and the
  * number of kernel launches the run made (1 for the persistent loop, one per window

@@ -266,6 +266,42 @@ def test_device_shards_in_one_process(gpu_lib, case, world, queue):
     _assert_oracle(res, c)
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("world", [2, 3])
+@pytest.mark.parametrize("case", range(len(GPU_CASES)))
+def test_device_shards_direct_hand_over(gpu_lib, case, world):
+    """Bucketed shards connected for direct hand-over: children are filed straight into the
+    destination shard's buckets by the window that makes them; no exchange between windows."""
+    from gpupq_b200 import shard as S
+    c = GPU_CASES[case]
+    shards = [S.PholdShard(_gpu_cfg(c, "laqb"), r, world) for r in range(world)]
+    try:
+        S.connect(shards)
+        res = S.run_local_direct(shards, c["end_time"])
+    finally:
+        for s in shards:
+            s.close()
+    want = _alone(c, "laqb")
+    for k in KEYS:
+        assert res[k] == want[k], (k, res[k], want[k])
+    assert res["status"] == 0
+    _assert_oracle(res, c)
+
+
+@pytest.mark.gpu
+def test_direct_hand_over_refuses_other_forms(gpu_lib):
+    import ctypes
+    import gpupq_b200 as G
+    from gpupq_b200 import shard as S
+    shards = [S.PholdShard(_gpu_cfg(GPU_CASES[0], "laq"), r, 2) for r in range(2)]
+    try:
+        arr = (ctypes.c_void_p * 2)(*[s._h.value for s in shards])
+        assert G.lib().gpq_phold_shard_connect(shards[0]._h, ctypes.cast(arr, ctypes.c_void_p), 2) == 1
+    finally:
+        for s in shards:
+            s.close()
+
+
 def _device_worker(rank, world, port, case, q, queue="laq"):
     import datetime
     import torch.distributed as dist
