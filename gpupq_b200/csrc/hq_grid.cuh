@@ -1043,35 +1043,63 @@ __device__ void hqg_sort_and_process(const PholdDev& d, const HqgDev& g, const g
   }
 }
 
-// A batch of c <= kHqgKeyTile events root[0, c) in one phase: LP-range buckets, so that
-// every LP's events of the batch are in one CTA, which collects their (lp, position) keys
-// by scanning the batch, sorts them in shared memory and processes them in order
-// (hqg_process_keys).  Ends with a barrier.
-__device__ void hqg_process_scan(const PholdDev& d, const HqgDev& g, const gpq_item* root, uint32_t c, uint32_t base,
+static constexpr uint32_t kHqgScanBatchMax = 2 * kHqgKeyTile;  // batches the one-phase form scans
+
+// A batch of c <= kHqgScanBatchMax events root[0, c) in one phase: LP-range buckets (one
+// per CTA), so that every LP's events of the batch are in one CTA, which collects their
+// (lp, position) keys by scanning the batch, sorts them in shared memory and processes
+// them in order (hqg_sort_and_process).  Every CTA also counts every bucket while it
+// scans, so all of them see the same largest bucket: when one holds more keys than a tile,
+// nothing is processed and false is returned (in every CTA, without a barrier).  Else ends
+// with a barrier.
+__device__ bool hqg_process_scan(const PholdDev& d, const HqgDev& g, const gpq_item* root, uint32_t c, uint32_t base,
                                  const HqgIns& ins, unsigned char* smem, HqgSync& s) {
   const uint32_t L = d.L;
   const uint32_t B = min(gridDim.x, max(1u, c / 64u));
   unsigned long long* sa = reinterpret_cast<unsigned long long*>(smem);
   unsigned long long* sb = sa + hqg_tile_cap<HqgKeyOps>();
-  __shared__ uint32_t s_n;
-  for (uint32_t b = blockIdx.x; b < B; b += gridDim.x) {
-    const uint32_t lo = hqg_lp_first(b, B, L), hi = hqg_lp_first(b + 1, B, L);
-    if (threadIdx.x == 0) s_n = 0;
-    __syncthreads();
-    hqg_cta_scan<8>(c, [root](uint32_t i) { return root[i].lp; }, [&](uint32_t i, uint32_t lp, bool valid) {
-      const bool take = valid && lp >= lo && lp < hi;
-      const uint32_t slot = hqg_warp_slot(&s_n, take);
-      if (take && slot < kHqgKeyTile) sa[hqg_pad<HqgKeyOps>(slot)] = ((unsigned long long)lp << 32) | i;
-    });
-    __syncthreads();
-    uint32_t n = s_n;
-    if (n > kHqgKeyTile) {  // cannot happen (n <= c <= kHqgKeyTile); reported, not written
-      if (threadIdx.x == 0) gpq_set_error(&d.ctrl->err, GPQ_ERR_INSERT_FULL);
-      n = 0;
-    }
-    hqg_sort_and_process(d, g, root, sa, sb, n, lo, hi - lo, base, ins, hqg_aux(smem));
+  __shared__ uint32_t s_n, s_hist[kHqgMaxBuckets], s_first[kHqgMaxBuckets + 1];
+  __shared__ int s_big;
+  const uint32_t b = blockIdx.x;  // this CTA's bucket (B <= gridDim.x)
+  // a batch that fits a tile cannot overflow a bucket; a larger one is counted per bucket
+  // (bucket of an LP: a float estimate corrected against the buckets' first LPs)
+  const bool count = c > kHqgKeyTile;
+  for (uint32_t k = threadIdx.x; k <= B; k += blockDim.x) {
+    if (k < B) s_hist[k] = 0u;
+    s_first[k] = hqg_lp_first(k, B, L);
   }
+  if (threadIdx.x == 0) s_n = 0;
+  __syncthreads();
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t lo_b = s_first[min(b, B)], hi_b = s_first[min(b + 1, B)];
+  const float scale = (float)B / (float)L;
+  hqg_cta_scan<8>(c, [root](uint32_t i) { return root[i].lp; }, [&](uint32_t i, uint32_t lp, bool valid) {
+    if (count) {
+      uint32_t bk = 0x80000000u | lane;
+      if (valid) {
+        bk = min(B - 1, __float2uint_rd((float)lp * scale));
+        while (bk > 0 && lp < s_first[bk]) --bk;
+        while (lp >= s_first[bk + 1]) ++bk;
+      }
+      const uint32_t peers = __match_any_sync(GPQ_FULL_MASK, bk);
+      if (valid && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&s_hist[bk], (uint32_t)__popc(peers));
+    }
+    const bool take = valid && lp >= lo_b && lp < hi_b;
+    const uint32_t slot = hqg_warp_slot(&s_n, take);
+    if (take && slot < kHqgKeyTile) sa[hqg_pad<HqgKeyOps>(slot)] = ((unsigned long long)lp << 32) | i;
+  });
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t mx = 0;
+    if (count)
+      for (uint32_t k = 0; k < B; ++k) mx = max(mx, s_hist[k]);
+    s_big = mx > kHqgKeyTile;
+  }
+  __syncthreads();
+  if (s_big) return false;
+  if (b < B) hqg_sort_and_process(d, g, root, sa, sb, s_n, lo_b, hi_b - lo_b, base, ins, hqg_aux(smem));
   hqg_bar(s);
+  return true;
 }
 
 // A batch whose keys the insert phase filed into BP LP-range lists (counts pc, none above
@@ -1304,13 +1332,14 @@ static __global__ void __launch_bounds__(kHqgThreads, 1) hqg_phold_kernel(PholdD
       const gpq_item* root = q.root + q.off;
       const uint32_t c = hqg_cta_search(0, q.cnt0, [root, lim](uint32_t i) { return gpq_f2u(root[i].ts) >= lim; });
       if (c == 0) break;
-      // LP-range lists for a large batch (a heap whose root holds every item)
+      // LP-range lists for the batch (a heap whose root holds every item; other heaps scan
+      // the batch in each CTA or take the general path)
       bool from_lists = false;
       uint32_t BP = 0;
       if (g.pcnt != nullptr && blockIdx.x == 0)  // the next window's range counts start at zero
         for (uint32_t k = threadIdx.x; k < kHqgMaxBuckets; k += blockDim.x)
           g.pcnt[((steps + 1u) & 1u) * kHqgMaxBuckets + k] = 0u;
-      if (c > kHqgKeyTile && g.plist != nullptr && q.last == 0) {
+      if (g.plist != nullptr && q.last == 0) {  // the root holds every item: file the batch
         uint32_t* pc = g.pcnt + (steps & 1u) * kHqgMaxBuckets;
         BP = min(gridDim.x, max(1u, c / 64u));
         hqg_file_batch(d, g, root, c, BP, pc, smem, s);
@@ -1340,11 +1369,14 @@ static __global__ void __launch_bounds__(kHqgThreads, 1) hqg_phold_kernel(PholdD
         ins.icnt = g.icnt + (steps & 1u) * kHqgMaxBuckets;
         ins.ilist = g.ilist;
       }
+      bool done = false;
       if (from_lists) {
         hqg_process_lists(d, g, root, s_pc, BP, nch, ins, smem, s);
-      } else if (c <= kHqgKeyTile) {
-        hqg_process_scan(d, g, root, c, nch, ins, smem, s);
-      } else {
+        done = true;
+      } else if (c <= kHqgScanBatchMax) {
+        done = hqg_process_scan(d, g, root, c, nch, ins, smem, s);
+      }
+      if (!done) {
         hqg_ranks(d, g, root, c, smem, s);
         for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < c; i0 += hqg_nthreads()) {
           const uint32_t i = i0 + threadIdx.x;

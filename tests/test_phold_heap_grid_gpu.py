@@ -103,6 +103,10 @@ def test_step_api_resumes(gpu_lib):
     dict(num_lps=3000, events_per_lp=6, lookahead=20.0, end_time=60.0, seed=17, dest_mode=1, ring_width=4),
     # many events of one LP in one batch (two LPs, long queues)
     dict(num_lps=2, events_per_lp=3000, lookahead=0.5, end_time=3.0, seed=5, dest_mode=0),
+    # two LPs, batches of nearly the whole population (16,384): in windows where one LP's
+    # share passes 8,192 its LP-range bucket outgrows a key tile, and the one-phase batch
+    # gives way to the general path
+    dict(num_lps=2, events_per_lp=8192, lookahead=50.0, end_time=400.0, seed=5, dest_mode=0),
 ])
 def test_edge_shapes(gpu_lib, cfgd):
     o = _oracle(cfgd)
