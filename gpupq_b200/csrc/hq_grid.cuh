@@ -20,7 +20,10 @@
 //   * the root has two buffers and an offset: a batch's removal advances the offset, and
 //     every merge into the root writes the other buffer;
 //   * the refill takes the largest items of the last node(s) -- suffixes of sorted nodes,
-//     so one merge of at most two runs replaces a sort.
+//     so one merge of at most two runs replaces a sort;
+//   * when the root holds every item (the global array queue's layout; the reference's
+//     256 K root on small populations), a window is three phases over bucket lists that
+//     each phase fills for the next, instead of grid-wide sorts (see the list section).
 // A batch's per-LP ranks (the order-sensitive hash needs each event's position in its
 // LP's sequence) come from a sort of (lp, position) keys: an event's rank is its LP's
 // count so far plus its distance from the first key of its LP.
@@ -703,13 +706,13 @@ __device__ bool hqg_insert_scan(const HqgDev& g, HqgState& q, const gpq_item* C,
 
 // ---------------------------------------------------------------------------------------
 // Bucket lists passed between phases (heaps whose root holds every item, the global
-// array queue's layout).  The batch phase files every child into a bucket of the root's
-// remainder R (splitters: R's quantiles, as in the one-phase insert); the insert phase
-// sorts each bucket in shared memory, streams its R slice past it and, while writing the
-// new root, files the next batch's (lp, position) keys into LP-range lists (the next
-// bound follows from the smallest child, which the batch phase records).  A window then
-// costs two phases whose CTAs read only their own buckets.  A list that overflows sends
-// the phase down the paths above (the children are also kept in h.ch).
+// array queue's layout).  A window is three phases whose CTAs read only their own
+// buckets: the batch's (lp, position) keys filed into LP-range lists by equal slices of
+// the batch; each LP range sorted and processed by one CTA, which files every child into
+// a bucket of the root's remainder R (splitters: R's quantiles, as in the one-phase
+// insert); each insert bucket's children sorted in shared memory and merged with its R
+// slice into the root's other buffer.  A list that overflows sends its phase down the
+// paths above (the children are also kept in h.ch).
 
 static constexpr uint32_t kHqgListCapI = kHqgTile;     // children per insert bucket
 static constexpr uint32_t kHqgListCapP = kHqgKeyTile;  // keys per LP-range bucket
@@ -717,9 +720,7 @@ static constexpr uint32_t kHqgMaxBuckets = 160;        // >= the grid (one CTA p
 
 struct HqgLists {
   bool ins;     // this window's children are filed in the insert lists
-  bool proc;    // unused
   uint32_t BI;  // insert buckets
-  uint32_t BP;  // unused
 };
 
 // LP-range buckets: LP lp belongs to bucket floor(lp * B / L), whose first LP is
@@ -1295,7 +1296,7 @@ static __global__ void __launch_bounds__(kHqgThreads, 1) hqg_phold_kernel(PholdD
   q.cnt0 = h.cnt[0];
   q.cntl = q.last > 0 ? h.cnt[q.last] : 0u;
   uint32_t steps = 0, nch = 0, ovf_seen = 0;
-  HqgLists lists{false, false, 0u, 0u};
+  HqgLists lists{false, 0u};
   __shared__ gpq_item s_spl[kHqgMaxBuckets];
   __shared__ uint32_t s_pc[kHqgMaxBuckets];
   __shared__ int s_pc_ovf;
