@@ -106,6 +106,19 @@ __device__ __forceinline__ bool hqg_bar(HqgSync& s) {
 }
 
 __device__ __forceinline__ uint32_t hqg_tid() { return blockIdx.x * blockDim.x + threadIdx.x; }
+
+// Asynchronous 16-byte copies from this GPU's global memory into the CTA's shared memory
+// (cp.async, no cluster multicast), completed per thread by commit groups.
+__device__ __forceinline__ void hqg_cp16(void* smem_dst, const void* gsrc) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(smem_dst)),
+               "l"(gsrc)
+               : "memory");
+}
+__device__ __forceinline__ void hqg_cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void hqg_cp_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 __device__ __forceinline__ uint32_t hqg_nthreads() { return gridDim.x * blockDim.x; }
 
 // ---------------------------------------------------------------------------------------
@@ -1159,23 +1172,27 @@ __device__ bool hqg_insert_lists(const HqgDev& g, HqgState& q, uint32_t nch, uin
     for (uint32_t j = threadIdx.x; j < nc; j += blockDim.x) sa[hqg_pad<HqgItemOps>(j)] = src[j];
     __syncthreads();
     const gpq_item* X = hqg_bin_sort_items(sa, sb, nc, L, aux) ? sb : hqg_cta_sort<HqgItemOps>(sa, sb, nc);
-    gpq_item* Y = (X == sa) ? sb : sa;  // two staging halves for R's tiles
+    gpq_item* Y = (X == sa) ? sb : sa;  // two of the three staging buffers for R's tiles
     const uint32_t r0 = (uint32_t)((uint64_t)b * nr / BI), r1 = (uint32_t)((uint64_t)(b + 1) * nr / BI);
     const uint32_t nrb = r1 - r0, base = r0 + s_pre[b];
-    // R's slice in tiles of kStreamTile staged in shared memory (the next tile's loads in
-    // flight while the current one merges); each tile merged with the children between its
-    // first item and the next tile's (merge path, kHqgIpt outputs a thread).  chis[t]: the
-    // children below tile t + 1's first item, for all tiles at once.
-    constexpr uint32_t kStreamTile = 2048, kPerT = kStreamTile / kHqgThreads;
-    static_assert(kStreamTile % kHqgThreads == 0, "stream tile");
-    constexpr uint32_t kHalf = kStreamTile + kStreamTile / kHqgIpt;  // padded half of a tile
+    // R's slice in tiles of kStreamTile, copied into shared memory asynchronously two tiles
+    // ahead (three staging buffers: the two halves of the free tile and the auxiliary
+    // area); each tile merged with the children between its first item and the next tile's
+    // (merge path, kHqgIpt outputs a thread).  chis[t]: the children below tile t + 1's
+    // first item, for all tiles at once.
+    constexpr uint32_t kStreamTile = 2048;
+    constexpr uint32_t kHalf = kStreamTile + kStreamTile / kHqgIpt;  // a padded tile
+    constexpr uint32_t kChis = 2048;                                 // words at the end of aux
+    static_assert(kHalf * sizeof(gpq_item) <= (kHqgAux - kChis) * sizeof(uint32_t), "third staging buffer");
     const uint32_t ntiles = (nrb + kStreamTile - 1) / kStreamTile;
-    // aux: the tiles' child counts at its end (kChis words), the merged output of a tile
-    // before it (padded; a tile whose output is larger is stored directly)
-    constexpr uint32_t kChis = 2048;
-    constexpr uint32_t kOutCap = ((kHqgAux - kChis) * 4u / sizeof(gpq_item)) * kHqgIpt / (kHqgIpt + 1);
     uint32_t* chis = aux + (kHqgAux - kChis);
-    gpq_item* ostage = reinterpret_cast<gpq_item*>(aux);
+    gpq_item* const stg[3] = {Y, Y + kHalf, reinterpret_cast<gpq_item*>(aux)};
+    auto issue = [&](uint32_t tt, gpq_item* Yh) {  // tile tt's copies, one group per thread
+      const uint32_t t0 = tt * kStreamTile;
+      for (uint32_t i = threadIdx.x; i < kStreamTile; i += blockDim.x)
+        if (t0 + i < nrb) hqg_cp16(&Yh[hqg_pad<HqgItemOps>(i)], &R[r0 + t0 + i]);
+      hqg_cp_commit();
+    };
     uint32_t cpos = 0;  // children below the current tile's first item
     for (uint32_t tb = 0; tb < ntiles; tb += kChis) {  // boundaries, kChis at a time
       const uint32_t tcnt = min(kChis, ntiles - tb);
@@ -1193,48 +1210,22 @@ __device__ bool hqg_insert_lists(const HqgDev& g, HqgState& q, uint32_t nch, uin
         }
         chis[t] = chi;
       }
-      gpq_item pre[kPerT];
-      auto fetch = [&](uint32_t tt) {
-        const uint32_t t0 = tt * kStreamTile;
-#pragma unroll
-        for (uint32_t u = 0; u < kPerT; ++u) {
-          const uint32_t i = t0 + u * blockDim.x + threadIdx.x;
-          if (i < nrb) pre[u] = R[r0 + i];
-        }
-      };
-      auto stage = [&](uint32_t tt, gpq_item* Yh) {
-        const uint32_t t0 = tt * kStreamTile;
-#pragma unroll
-        for (uint32_t u = 0; u < kPerT; ++u) {
-          const uint32_t i = u * blockDim.x + threadIdx.x;
-          if (t0 + i < nrb) Yh[hqg_pad<HqgItemOps>(i)] = pre[u];
-        }
-      };
-      fetch(tb);
-      stage(tb, Y);
-      __syncthreads();
+      issue(tb, stg[0]);
+      if (tcnt > 1) issue(tb + 1, stg[1]); else hqg_cp_commit();
       for (uint32_t t = 0; t < tcnt; ++t) {
+        hqg_cp_wait<1>();  // this tile's copies have landed (the next one's may be in flight)
+        __syncthreads();
         const uint32_t tt = tb + t, t0 = tt * kStreamTile;
-        gpq_item* Yh = Y + (t & 1u) * kHalf;
-        if (t + 1 < tcnt) fetch(tt + 1);  // in flight during the merge
+        const gpq_item* Yh = stg[t % 3];
+        if (t + 2 < tcnt) issue(tt + 2, stg[(t + 2) % 3]); else hqg_cp_commit();  // read in the last round
         const uint32_t tn = min(kStreamTile, nrb - t0), chi = chis[t], cn = chi - cpos, total = tn + cn;
         gpq_item* dst = out + base + t0 + cpos;
-        const bool staged = total <= kOutCap;
-        for (uint32_t o0 = threadIdx.x * kHqgIpt; o0 < total; o0 += blockDim.x * kHqgIpt) {
-          if (staged)
-            hqg_merge_run<HqgItemOps>(Yh, 0, tn, X, cpos, cn, o0,
-                                      [&](uint32_t k, const gpq_item& v) { ostage[hqg_pad<HqgItemOps>(o0 + k)] = v; });
-          else
-            hqg_merge_run<HqgItemOps>(Yh, 0, tn, X, cpos, cn, o0, [&](uint32_t k, const gpq_item& v) { dst[o0 + k] = v; });
-        }
-        if (t + 1 < tcnt) stage(tt + 1, Y + ((t + 1) & 1u) * kHalf);
-        __syncthreads();
-        if (staged) {  // coalesced stores
-          for (uint32_t i = threadIdx.x; i < total; i += blockDim.x) dst[i] = ostage[hqg_pad<HqgItemOps>(i)];
-          __syncthreads();
-        }
+        for (uint32_t o0 = threadIdx.x * kHqgIpt; o0 < total; o0 += blockDim.x * kHqgIpt)
+          hqg_merge_run<HqgItemOps>(Yh, 0, tn, X, cpos, cn, o0, [&](uint32_t k, const gpq_item& v) { dst[o0 + k] = v; });
         cpos = chi;
       }
+      hqg_cp_wait<0>();
+      __syncthreads();
     }
     for (uint32_t j = cpos + threadIdx.x; j < nc; j += blockDim.x) out[base + nrb + j] = X[hqg_pad<HqgItemOps>(j)];
     __syncthreads();
