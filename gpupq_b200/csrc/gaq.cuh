@@ -254,12 +254,62 @@ __device__ __forceinline__ bool mp_stage_inputs(gpq_item* s, const gpq_item* A, 
   return __syncthreads_and(mbar_wait_bounded(bar, 0, err)) != 0;
 }
 
+// Shared-memory slot of key j in the merge's key array: one pad word per 32 keys, so that
+// the lanes of a warp, kMpPer keys apart, read 32 different banks.
+__device__ __forceinline__ uint32_t mp_kp(uint32_t j) { return j + (j >> 5); }
+
+// mp_search over the padded keys k (A = keys [0, na), B = keys [na, na + nb)).
+__device__ __forceinline__ uint32_t mp_search_keys(const uint32_t* k, uint32_t na, uint32_t nb, uint32_t diag) {
+  uint32_t lo = diag > nb ? diag - nb : 0u, hi = min(diag, na);
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (k[mp_kp(mid)] <= k[mp_kp(na + diag - 1 - mid)]) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+// Merges the staged s[0, la) and s[la, la + lb) (A first on ties) into out[0, la + lb).
+// The merge runs on the timestamp keys, copied into a padded array (each thread's kMpPer
+// outputs are consecutive, so the lanes' positions are kMpPer keys apart; items read at
+// that stride would all fall in one bank group), and produces only the source slot of
+// each output; the CTA then writes the tile in output order, each thread gathering its
+// items from the staged inputs.  All threads (kMpThreads).
+__device__ __forceinline__ void mp_merge_tile(const gpq_item* s, uint32_t la, uint32_t lb, uint32_t* kp, uint16_t* src,
+                                              gpq_item* out) {
+  const uint32_t len = la + lb;
+  for (uint32_t j = threadIdx.x; j < len; j += kMpThreads) kp[mp_kp(j)] = gpq_f2u(s[j].ts);
+  __syncthreads();
+  const uint32_t my0 = threadIdx.x * kMpPer;
+  if (my0 < len) {
+    uint32_t ia = mp_search_keys(kp, la, lb, my0);
+    uint32_t ib = my0 - ia;
+    uint32_t ka = ia < la ? kp[mp_kp(ia)] : 0u, kb = ib < lb ? kp[mp_kp(la + ib)] : 0u;
+#pragma unroll
+    for (uint32_t k = 0; k < kMpPer; ++k) {
+      if (my0 + k < len) {
+        if (ib >= lb || (ia < la && ka <= kb)) {
+          src[my0 + k] = (uint16_t)ia;
+          if (++ia < la) ka = kp[mp_kp(ia)];
+        } else {
+          src[my0 + k] = (uint16_t)(la + ib);
+          if (++ib < lb) kb = kp[mp_kp(la + ib)];
+        }
+      }
+    }
+  }
+  __syncthreads();
+  for (uint32_t x = threadIdx.x; x < len; x += kMpThreads) out[x] = s[src[x]];
+}
+
 // Merge path: CTA b writes outputs [b*kMpTile, (b+1)*kMpTile) of merge(A, B), its inputs
 // located by the precomputed splits and staged by TMA.
 static __global__ void mp_merge_kernel(const gpq_item* __restrict__ A, uint32_t na, const gpq_item* __restrict__ B,
                                        uint32_t nb, gpq_item* out, const uint32_t* __restrict__ split, uint32_t* err) {
   __shared__ __align__(16) gpq_item s[kMpTile];
+  __shared__ uint32_t kp[kMpTile + kMpTile / 32];
+  __shared__ uint16_t src[kMpTile];
   __shared__ __align__(8) uint64_t bar;
+  static_assert(kMpTile <= 65536, "source slots are 16 bits wide");
   const uint32_t total = na + nb;
   const uint32_t d0 = blockIdx.x * kMpTile;
   const uint32_t d1 = min(d0 + kMpTile, total);
@@ -267,27 +317,7 @@ static __global__ void mp_merge_kernel(const gpq_item* __restrict__ A, uint32_t 
   const uint32_t b0 = d0 - a0, b1 = d1 - a1;
   const uint32_t la = a1 - a0, lb = b1 - b0;
   if (!mp_stage_inputs(s, A, a0, la, B, b0, lb, &bar, err)) return;
-  // each thread merges its kMpPer outputs into registers, the tile goes back to shared
-  // memory in output order, and the CTA writes it with coalesced stores
-  const uint32_t my0 = threadIdx.x * kMpPer, len = la + lb;
-  gpq_item r[kMpPer];
-  if (my0 < len) {
-    uint32_t ia = mp_search(s, la, s + la, lb, my0);
-    uint32_t ib = my0 - ia;
-#pragma unroll
-    for (uint32_t k = 0; k < kMpPer; ++k) {
-      if (my0 + k < len) {
-        const bool take_a = ib >= lb || (ia < la && gpq_f2u(s[ia].ts) <= gpq_f2u(s[la + ib].ts));
-        r[k] = take_a ? s[ia++] : s[la + ib++];
-      }
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (uint32_t k = 0; k < kMpPer; ++k)
-    if (my0 + k < len) s[my0 + k] = r[k];
-  __syncthreads();
-  for (uint32_t x = threadIdx.x; x < len; x += kMpThreads) out[d0 + x] = s[x];
+  mp_merge_tile(s, la, lb, kp, src, out + d0);
 }
 
 // GAQ engine state visible to kernels.
@@ -675,25 +705,15 @@ static __global__ void gaq_win_merge_kernel(gpq_item* arr0, gpq_item* arr1, cons
   gpq_item* out = w->cur ? arr0 : arr1;
   extern __shared__ __align__(16) unsigned char mp_smem[];
   gpq_item* s = reinterpret_cast<gpq_item*>(mp_smem);  // [kMpTile] inputs
-  gpq_item* o = s + kMpTile;                           // [kMpTile] merged, then stored coalesced
+  __shared__ uint32_t kp[kMpTile + kMpTile / 32];
+  __shared__ uint16_t src[kMpTile];
   const uint32_t d1 = min(d0 + kMpTile, total);
   const uint32_t a0 = split[blockIdx.x], a1 = split[blockIdx.x + 1];
   const uint32_t b0 = d0 - a0, b1 = d1 - a1;
   const uint32_t la = a1 - a0, lb = b1 - b0;
   __shared__ __align__(8) uint64_t bar;
   if (!mp_stage_inputs(s, A, a0, la, B, b0, lb, &bar, err)) return;
-  const uint32_t my0 = threadIdx.x * kMpPer;
-  if (my0 < la + lb) {
-    uint32_t ia = mp_search(s, la, s + la, lb, my0);
-    uint32_t ib = my0 - ia;
-    const uint32_t lim = min(my0 + kMpPer, la + lb);
-    for (uint32_t q = my0; q < lim; ++q) {
-      const bool take_a = ib >= lb || (ia < la && gpq_f2u(s[ia].ts) <= gpq_f2u(s[la + ib].ts));
-      o[q] = take_a ? s[ia++] : s[la + ib++];
-    }
-  }
-  __syncthreads();
-  for (uint32_t x = threadIdx.x; x < la + lb; x += kMpThreads) out[d0 + x] = o[x];
+  mp_merge_tile(s, la, lb, kp, src, out + d0);
 }
 
 static __global__ void gaq_win_end_kernel(GaqWin* w) {

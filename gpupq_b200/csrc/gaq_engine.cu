@@ -150,7 +150,7 @@ gpq_status gaq_engine_create(const gpq_phold_config& c, GaqEngine** out) {
   // the bulk sort's tiles (kRsTile) and the window loop's smaller ones (kWinRsTile)
   if ((e = cudaMalloc(&g->hist, engine_hist_words(g->cap) * sizeof(uint32_t))) != cudaSuccess)
     return fail(e);
-  if ((e = gpq::raise_smem_limit(gaq_win_merge_kernel, (int)(2 * kMpTile * sizeof(gpq_item)))) != cudaSuccess)
+  if ((e = gpq::raise_smem_limit(gaq_win_merge_kernel, (int)(kMpTile * sizeof(gpq_item)))) != cudaSuccess)
     return fail(e);
   if ((e = cudaMalloc(&g->acc, 8 * sizeof(unsigned long long))) != cudaSuccess) return fail(e);
   if ((e = cudaMallocHost(&g->h_info, 8 * sizeof(uint32_t))) != cudaSuccess) return fail(e);
@@ -240,7 +240,7 @@ static gpq_status gaq_capture(GaqEngine* g, const PholdDev& d, cudaStream_t st) 
   }
   gaq_win_splits_kernel<<<(mgrid + 1 + 255) / 256, 256, 0, st>>>(g->arr[0], g->arr[1], g->ch, g->ch_tmp, g->win,
                                                                   g->split);
-  gaq_win_merge_kernel<<<mgrid, kMpThreads, 2 * kMpTile * sizeof(gpq_item), st>>>(g->arr[0], g->arr[1], g->ch,
+  gaq_win_merge_kernel<<<mgrid, kMpThreads, kMpTile * sizeof(gpq_item), st>>>(g->arr[0], g->arr[1], g->ch,
                                                                                   g->ch_tmp, g->win, g->split,
                                                                                   &d.ctrl->err);
   gaq_win_end_kernel<<<1, 32, 0, st>>>(g->win);
