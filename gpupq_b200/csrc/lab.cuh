@@ -200,7 +200,9 @@ __device__ __forceinline__ bool lab_handover(const LabCtx& x, const LabDev& q, c
 }
 
 // Process one staged event: per-LP hashes into the slot accumulators, the child into its
-// bucket.  Returns the child's timestamp bits.
+// bucket (kShard: a child of another shard's LP is handed over).  Returns the child's
+// timestamp bits.
+template <bool kShard>
 __device__ __forceinline__ uint32_t lab_process_event(const LabCtx& x, const LabDev& q, const PholdStage& st,
                                                       const gpq_item e, const LabWin& w) {
   const uint32_t slot = e.aux >> 16;
@@ -211,7 +213,7 @@ __device__ __forceinline__ uint32_t lab_process_event(const LabCtx& x, const Lab
   atomicAdd(&st.ohash[slot], (unsigned long long)gpq_seq_hash(h, (uint64_t)st.seq0[slot] + idx));
   const gpq_item ch = lab_child(x, e);
   const uint32_t cb = gpq_f2u(ch.ts);
-  if (!lab_handover(x, q, w, ch)) lab_push(x, q, ch.lp, lab_key(cb, ch.id), lab_bucket(cb, w.inv_w), w);
+  if (!(kShard && lab_handover(x, q, w, ch))) lab_push(x, q, ch.lp, lab_key(cb, ch.id), lab_bucket(cb, w.inv_w), w);
   return cb;
 }
 
@@ -250,7 +252,7 @@ __device__ __forceinline__ unsigned long long lab_cand(const unsigned long long*
 // re-file the spill list, store the number of safe events in nsafe_out[slot], and return
 // the LP's next minimum (ts bits) min'ed with any child processed here.  All lanes of the
 // group, convergent.
-template <int G>
+template <int G, bool kShard>
 __device__ uint32_t lab_lp_stage(const LabCtx& x, const LabDev& q, uint32_t lp, uint32_t slot, const LabWin& w,
                                  unsigned long long* skeys, const PholdStage& st, const LaneGroup<G>& g, const LabMeta& mt, uint32_t* nsafe_out) {
   const uint32_t L = x.L;
@@ -317,7 +319,7 @@ __device__ uint32_t lab_lp_stage(const LabCtx& x, const LabDev& q, uint32_t lp, 
           hole.aux = kStageHole;
           st.ev[base + rank] = hole;
         }
-        cmin = min(cmin, lab_process_event(x, q, st, e, w));
+        cmin = min(cmin, lab_process_event<kShard>(x, q, st, e, w));
       }
     };
     if (nsafe <= kLabSafeCap) {
@@ -626,7 +628,7 @@ __device__ __forceinline__ uint32_t lab_scan_above(const LabDev& q, uint32_t lp,
 // staged event x, or one whose aux is kStageHole): hashes into the LP accumulators and the
 // children first, then all bucket reservations (independent atomics in flight together),
 // then the stores.  Returns the children's minimum.
-template <class Get>
+template <bool kShard, class Get>
 __device__ __forceinline__ uint32_t lab_event_batch(const LabCtx& x, const LabDev& q, const PholdStage& st,
                                                     uint32_t ns, uint32_t x0, uint32_t stride, const LabWin& w, Get get) {
   constexpr int U = 4;
@@ -648,7 +650,7 @@ __device__ __forceinline__ uint32_t lab_event_batch(const LabCtx& x, const LabDe
         const gpq_item ch = lab_child(x, e);
         const uint32_t cb = gpq_f2u(ch.ts);
         mn = min(mn, cb);
-        if (!lab_handover(x, q, w, ch)) {
+        if (!(kShard && lab_handover(x, q, w, ch))) {
           key[u] = lab_key(cb, ch.id);
           lp[u] = ch.lp;
           jb[u] = lab_bucket(cb, w.inv_w);
@@ -694,6 +696,7 @@ __device__ __forceinline__ unsigned long long lab_load_cand(const LabCtx& x, con
 
 // One window for the chunk [lp0, lp0 + n) of one warp (outputs in sm.ls_*).  Returns this
 // lane's part of the chunk minimum (LP next minima and children).  All lanes of the warp.
+template <bool kShard = false>
 static __device__ uint32_t lab_warp_window(const LabCtx& x, const LabDev& q, const LabWin& w, uint32_t lp0, uint32_t n,
                                     const LabWarpSmem& sm) {
   const uint32_t lane = threadIdx.x & 31u;
@@ -865,7 +868,7 @@ static __device__ uint32_t lab_warp_window(const LabCtx& x, const LabDev& q, con
         e.lp = lp0 + lo;
         e.id = (uint32_t)key;
         e.aux = (lo << 16) | rank;
-        mn = min(mn, lab_process_event(x, q, st, e, w));
+        mn = min(mn, lab_process_event<kShard>(x, q, st, e, w));
       }
     }
     // next-minimum scan of the LPs with nothing live at or below j1, when one of the two
@@ -902,7 +905,7 @@ static __device__ uint32_t lab_warp_window(const LabCtx& x, const LabDev& q, con
     for (uint32_t lpi = 0; lpi < n; ++lpi) {
       const uint32_t lp = lp0 + lpi;
       const LabMeta mt = lab_load_meta(x, q, lp, w, g.gl);
-      mn = min(mn, lab_lp_stage<32>(x, q, lp, lpi, w, sm.cand, st, g, mt, sm.lp_nsafe));
+      mn = min(mn, lab_lp_stage<32, kShard>(x, q, lp, lpi, w, sm.cand, st, g, mt, sm.lp_nsafe));
     }
     __syncwarp();
   }
@@ -920,11 +923,11 @@ static __device__ uint32_t lab_warp_window(const LabCtx& x, const LabDev& q, con
       e.aux = ((uint32_t)(sm.cseg[k] >> 3) << 16) | (c >> 16);
       return e;
     };
-    for (uint32_t x0 = lane; x0 < ns; x0 += 128u) mn = min(mn, lab_event_batch(x, q, st, ns, x0, 32u, w, get));
+    for (uint32_t x0 = lane; x0 < ns; x0 += 128u) mn = min(mn, lab_event_batch<kShard>(x, q, st, ns, x0, 32u, w, get));
   } else {
     const uint32_t ns = min(sm.misc[0], kLabItemStageCap);
     auto get = [&](uint32_t y) { return sm.stage[y]; };
-    for (uint32_t x0 = lane; x0 < ns; x0 += 128u) mn = min(mn, lab_event_batch(x, q, st, ns, x0, 32u, w, get));
+    for (uint32_t x0 = lane; x0 < ns; x0 += 128u) mn = min(mn, lab_event_batch<kShard>(x, q, st, ns, x0, 32u, w, get));
   }
   if (common) {
     if (scan_lpi != ~0u && scan_min != kInfBits) atomicMin(&sm.lp_nmin[scan_lpi], scan_min);
@@ -955,12 +958,13 @@ static __device__ uint32_t lab_warp_window(const LabCtx& x, const LabDev& q, con
 // One window for the LPs [lp_lo, lp_hi) of this CTA, split evenly among its warps.  Folds
 // the CTA's minimum into mins[(s+1)%3].  `resident`: every warp owns at most one chunk,
 // whose outputs stay in shared memory between windows.
+template <bool kShard>
 __device__ __forceinline__ void lab_window_body(const PholdDev& d, const LabDev& q, uint32_t s, float m,
                                                 unsigned char* smem_raw, uint32_t* red, uint32_t lp_lo,
                                                 uint32_t lp_hi, bool resident) {
   const LabWin w = lab_window(d, q, s, m);
   LabCtx x{d.p, d.L, 0u, &d.ctrl->err, &d.ctrl->errs[(s + 1u) % 3u]};
-  if (d.outbox != nullptr) {
+  if (kShard && d.outbox != nullptr) {
     x.outbox = d.outbox;
     x.out_n = d.out_n;
     x.out_cap = d.out_cap;
@@ -977,7 +981,7 @@ __device__ __forceinline__ void lab_window_body(const PholdDev& d, const LabDev&
   for (uint32_t c0 = wlo; c0 < whi; c0 += q.chunk) {
     const uint32_t n = min(q.chunk, whi - c0);
     if (!resident) lab_state_load(d, sm, c0, n);
-    mn = min(mn, lab_warp_window(x, q, w, c0, n, sm));
+    mn = min(mn, lab_warp_window<kShard>(x, q, w, c0, n, sm));
     if (!resident) lab_state_store(d, sm, c0, n);
   }
   mn = block_min_u32(mn, red);
@@ -987,7 +991,9 @@ __device__ __forceinline__ void lab_window_body(const PholdDev& d, const LabDev&
 // LPs a CTA of `block` threads covers in one launch of the plain form.
 __host__ __device__ inline uint32_t lab_plain_lps_per_cta(uint32_t block, uint32_t chunk) { return (block / 32u) * chunk; }
 
-// Plain form: one launch per window.
+// Plain form: one launch per window (kShard: the window of one shard of a sharded run,
+// children of other shards' LPs handed over).
+template <bool kShard>
 static __global__ void __launch_bounds__(1024, 1) lab_window_kernel(PholdDev d, LabDev q, uint32_t s) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ uint32_t red[32];
@@ -1003,7 +1009,7 @@ static __global__ void __launch_bounds__(1024, 1) lab_window_kernel(PholdDev d, 
   }
   const uint32_t per = (blockDim.x / 32u) * q.chunk;  // a shard works its own LPs [lp_begin, lp_end)
   const uint32_t lp_lo = min(d.lp_end, d.lp_begin + blockIdx.x * per), lp_hi = min(d.lp_end, lp_lo + per);
-  lab_window_body(d, q, s, m, smem_raw, red, lp_lo, lp_hi, false);
+  lab_window_body<kShard>(d, q, s, m, smem_raw, red, lp_lo, lp_hi, false);
 }
 
 // Persistent form: all windows in one cooperative launch, a bounded grid barrier per window.
@@ -1032,7 +1038,7 @@ static __global__ void __launch_bounds__(1024, 1) lab_persistent_kernel(PholdDev
       d.ctrl->steps += 1ull;
       q.wj[s & 3u] = lab_bucket(gpq_f2u(GPQ_FADD(m, d.p.lookahead)), q.inv_w);
     }
-    lab_window_body(d, q, s, m, smem_raw, red, lp_lo, lp_hi, resident);
+    lab_window_body<false>(d, q, s, m, smem_raw, red, lp_lo, lp_hi, resident);
     target += gridDim.x;
     if (!grid_barrier(&d.ctrl->bar, target, d.spin_limit, &d.ctrl->err)) {
       s += 1u;
@@ -1179,14 +1185,17 @@ static __global__ void lab_finalize_kernel(PholdDev d, LabDev q, PholdAcc* acc) 
   }
 }
 
-// Kernel pointers (host-side dispatch).  The window is warp-owned for every lanes_per_lp.
+// Kernel pointers (host-side dispatch).  The window is warp-owned for every lanes_per_lp;
+// a shard of a sharded run (which runs window by window) takes the window that hands
+// children over, every other run the one without that code.
 struct LabKernelSet {
   const void* window;
   const void* persistent;
 };
 
-inline bool lab_kernel_set(uint32_t group, LabKernelSet* out) {
+inline bool lab_kernel_set(uint32_t group, LabKernelSet* out, bool sharded = false) {
   if (group != 4 && group != 8 && group != 16 && group != 32) return false;
-  *out = {(const void*)lab_window_kernel, (const void*)lab_persistent_kernel};
+  *out = {sharded ? (const void*)lab_window_kernel<true> : (const void*)lab_window_kernel<false>,
+          (const void*)lab_persistent_kernel};
   return true;
 }

@@ -819,6 +819,16 @@ gpq_status gpq_phold_shard_create(const gpq_phold_config* cfg, uint32_t rank, ui
   h->sharded = true;
   h->rank = rank;
   h->world = world;
+  if (h->is_lab) {  // the window that hands children of other shards' LPs over
+    lab_kernel_set(h->cfg.lanes_per_lp, &h->lks, true);
+    h->ks.window = h->lks.window;
+    cudaError_t e = gpq::raise_smem_limit(h->ks.window, (int)h->window_smem());
+    if (e != cudaSuccess) {
+      gpq::set_last_error("gpq_phold_shard_create: %s", cudaGetErrorString(e));
+      gpq_phold_destroy(h);
+      return GPQ_ERR_CUDA;
+    }
+  }
   h->shard_lps = (uint32_t)(((uint64_t)L + world - 1) / world);
   h->lp_begin = std::min<uint32_t>(L, rank * h->shard_lps);
   h->lp_end = (uint32_t)std::min<uint64_t>(L, (uint64_t)h->lp_begin + h->shard_lps);
