@@ -70,6 +70,31 @@ __device__ __forceinline__ bool grid_barrier(unsigned long long* ctr, unsigned l
   return ok != 0;
 }
 
+// The same barrier with a lighter arrival: thread 0 arrives with a release reduction (the
+// CTA's writes, ordered before it by the block barrier, become visible at GPU scope before
+// the arrival; no wait for a returned value), polls with acquire loads, and the block
+// barrier after the poll orders every thread's later reads after the other CTAs' writes.
+__device__ __forceinline__ bool grid_barrier_release(unsigned long long* ctr, unsigned long long target,
+                                                     uint64_t spin_limit, uint32_t* err) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ok = 1;
+    asm volatile("red.release.gpu.global.add.u64 [%0], 1;" ::"l"(ctr) : "memory");
+    uint64_t it = 0;
+    while (ld_acquire_u64(ctr) < target) {
+      if (++it > spin_limit) {
+        gpq_set_error(err, GPQ_ERR_TIMEOUT);
+        ok = 0;
+        break;
+      }
+      __nanosleep(32);
+    }
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
 // Block-wide min of a u32 (all threads call; result valid in all threads).
 __device__ __forceinline__ uint32_t block_min_u32(uint32_t v, uint32_t* scratch /* >= 32 */) {
   v = warp_min_u32(v);

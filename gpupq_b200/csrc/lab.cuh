@@ -959,10 +959,10 @@ static __device__ uint32_t lab_warp_window(const LabCtx& x, const LabDev& q, con
 // the CTA's minimum into mins[(s+1)%3].  `resident`: every warp owns at most one chunk,
 // whose outputs stay in shared memory between windows.
 template <bool kShard>
-__device__ __forceinline__ void lab_window_body(const PholdDev& d, const LabDev& q, uint32_t s, float m,
+__device__ __forceinline__ void lab_window_body(const PholdDev& d, const LabDev& q, uint32_t s, float m, uint32_t j1p,
                                                 unsigned char* smem_raw, uint32_t* red, uint32_t lp_lo,
                                                 uint32_t lp_hi, bool resident) {
-  const LabWin w = lab_window(d, q, s, m);
+  const LabWin w = lab_window_of(d.p, q.inv_w, s, m, j1p);
   LabCtx x{d.p, d.L, 0u, &d.ctrl->err, &d.ctrl->errs[(s + 1u) % 3u]};
   if (kShard && d.outbox != nullptr) {
     x.outbox = d.outbox;
@@ -1009,7 +1009,7 @@ static __global__ void __launch_bounds__(1024, 1) lab_window_kernel(PholdDev d, 
   }
   const uint32_t per = (blockDim.x / 32u) * q.chunk;  // a shard works its own LPs [lp_begin, lp_end)
   const uint32_t lp_lo = min(d.lp_end, d.lp_begin + blockIdx.x * per), lp_hi = min(d.lp_end, lp_lo + per);
-  lab_window_body<kShard>(d, q, s, m, smem_raw, red, lp_lo, lp_hi, false);
+  lab_window_body<kShard>(d, q, s, m, ld_relaxed_u32(&q.wj[(s + 3u) & 3u]), smem_raw, red, lp_lo, lp_hi, false);
 }
 
 // Persistent form: all windows in one cooperative launch, a bounded grid barrier per window.
@@ -1027,20 +1027,25 @@ static __global__ void __launch_bounds__(1024, 1) lab_persistent_kernel(PholdDev
   if (resident) lab_state_load(d, sm, wlo, whi - wlo);
   unsigned long long target = 0;
   uint32_t s = s0;
+  // j1 of the previous window: read once, then carried in registers (every CTA computes
+  // what block 0 records in q.wj for the plain form and the next launch)
+  uint32_t j1p = ld_relaxed_u32(&q.wj[(s0 + 3u) & 3u]);
   for (;; ++s) {
     const uint32_t mb = ld_relaxed_u32(&d.ctrl->mins[s % 3u]);
     const uint32_t eb = ld_relaxed_u32(&d.ctrl->errs[s % 3u]);
     const float m = gpq_u2f(mb);
     if (!(m < d.p.end_time) || eb != 0u || (max_steps != 0u && s - s0 >= max_steps)) break;
+    const uint32_t j1 = lab_bucket(gpq_f2u(GPQ_FADD(m, d.p.lookahead)), q.inv_w);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       d.ctrl->mins[(s + 2u) % 3u] = kInfBits;
       d.ctrl->errs[(s + 2u) % 3u] = 0u;
       d.ctrl->steps += 1ull;
-      q.wj[s & 3u] = lab_bucket(gpq_f2u(GPQ_FADD(m, d.p.lookahead)), q.inv_w);
+      q.wj[s & 3u] = j1;
     }
-    lab_window_body<false>(d, q, s, m, smem_raw, red, lp_lo, lp_hi, resident);
+    lab_window_body<false>(d, q, s, m, j1p, smem_raw, red, lp_lo, lp_hi, resident);
+    j1p = j1;
     target += gridDim.x;
-    if (!grid_barrier(&d.ctrl->bar, target, d.spin_limit, &d.ctrl->err)) {
+    if (!grid_barrier_release(&d.ctrl->bar, target, d.spin_limit, &d.ctrl->err)) {
       s += 1u;
       break;
     }
