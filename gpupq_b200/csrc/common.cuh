@@ -44,38 +44,14 @@ __device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t* p) {
 
 // Grid-wide barrier for a cooperative (co-resident) launch.  `ctr` counts arrivals
 // and is never reset during a launch: barrier number b completes when the counter
-// reaches nblocks * (b + 1).  The wait is bounded by `spin_limit` polls; on timeout
-// the error word gets GPQ_ERR_TIMEOUT and the function returns false, so no block
-// ever spins forever.
+// reaches nblocks * (b + 1).  Thread 0 arrives with a release reduction (the CTA's
+// writes, ordered before it by the block barrier, become visible at GPU scope before the
+// arrival; no wait for a returned value) and polls with acquire loads; the block barrier
+// after the poll orders every thread's later reads after the other CTAs' writes.  The wait
+// is bounded by `spin_limit` polls; on timeout the error word gets GPQ_ERR_TIMEOUT and the
+// function returns false, so no block ever spins forever.
 __device__ __forceinline__ bool grid_barrier(unsigned long long* ctr, unsigned long long target,
                                              uint64_t spin_limit, uint32_t* err) {
-  __shared__ int ok;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    ok = 1;
-    __threadfence();
-    atomicAdd(ctr, 1ull);
-    uint64_t it = 0;
-    while (ld_acquire_u64(ctr) < target) {
-      if (++it > spin_limit) {
-        gpq_set_error(err, GPQ_ERR_TIMEOUT);
-        ok = 0;
-        break;
-      }
-      __nanosleep(32);
-    }
-    __threadfence();
-  }
-  __syncthreads();
-  return ok != 0;
-}
-
-// The same barrier with a lighter arrival: thread 0 arrives with a release reduction (the
-// CTA's writes, ordered before it by the block barrier, become visible at GPU scope before
-// the arrival; no wait for a returned value), polls with acquire loads, and the block
-// barrier after the poll orders every thread's later reads after the other CTAs' writes.
-__device__ __forceinline__ bool grid_barrier_release(unsigned long long* ctr, unsigned long long target,
-                                                     uint64_t spin_limit, uint32_t* err) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {

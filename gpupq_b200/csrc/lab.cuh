@@ -1045,7 +1045,7 @@ static __global__ void __launch_bounds__(1024, 1) lab_persistent_kernel(PholdDev
     lab_window_body<false>(d, q, s, m, j1p, smem_raw, red, lp_lo, lp_hi, resident);
     j1p = j1;
     target += gridDim.x;
-    if (!grid_barrier_release(&d.ctrl->bar, target, d.spin_limit, &d.ctrl->err)) {
+    if (!grid_barrier(&d.ctrl->bar, target, d.spin_limit, &d.ctrl->err)) {
       s += 1u;
       break;
     }
