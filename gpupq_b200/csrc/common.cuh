@@ -71,6 +71,33 @@ __device__ __forceinline__ bool grid_barrier(unsigned long long* ctr, unsigned l
   return ok != 0;
 }
 
+// grid_barrier whose arrival also publishes a CTA-wide minimum: the CTA's threads min'ed
+// their values into the shared word *smin before the call; thread 0 folds it into *gmin
+// with one atomicMin (released with the arrival) and resets *smin to all ones.
+__device__ __forceinline__ bool grid_barrier_min(unsigned long long* ctr, unsigned long long target,
+                                                 uint64_t spin_limit, uint32_t* err, uint32_t* smin, uint32_t* gmin) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ok = 1;
+    const uint32_t v = *smin;
+    *smin = 0xffffffffu;
+    if (v != 0xffffffffu) atomicMin(gmin, v);
+    asm volatile("red.release.gpu.global.add.u64 [%0], 1;" ::"l"(ctr) : "memory");
+    uint64_t it = 0;
+    while (ld_acquire_u64(ctr) < target) {
+      if (++it > spin_limit) {
+        gpq_set_error(err, GPQ_ERR_TIMEOUT);
+        ok = 0;
+        break;
+      }
+      __nanosleep(32);
+    }
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
 // Block-wide min of a u32 (all threads call; result valid in all threads).
 __device__ __forceinline__ uint32_t block_min_u32(uint32_t v, uint32_t* scratch /* >= 32 */) {
   v = warp_min_u32(v);

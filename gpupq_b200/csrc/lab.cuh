@@ -955,9 +955,10 @@ static __device__ uint32_t lab_warp_window(const LabCtx& x, const LabDev& q, con
   return mn;
 }
 
-// One window for the LPs [lp_lo, lp_hi) of this CTA, split evenly among its warps.  Folds
-// the CTA's minimum into mins[(s+1)%3].  `resident`: every warp owns at most one chunk,
-// whose outputs stay in shared memory between windows.
+// One window for the LPs [lp_lo, lp_hi) of this CTA, split evenly among its warps.  Each
+// warp min's its part of the next window's minimum into red[0] (shared); the caller
+// publishes the CTA's minimum to mins[(s+1)%3].  `resident`: every warp owns at most one
+// chunk, whose outputs stay in shared memory between windows.
 template <bool kShard>
 __device__ __forceinline__ void lab_window_body(const PholdDev& d, const LabDev& q, uint32_t s, float m, uint32_t j1p,
                                                 unsigned char* smem_raw, uint32_t* red, uint32_t lp_lo,
@@ -984,8 +985,8 @@ __device__ __forceinline__ void lab_window_body(const PholdDev& d, const LabDev&
     mn = min(mn, lab_warp_window<kShard>(x, q, w, c0, n, sm));
     if (!resident) lab_state_store(d, sm, c0, n);
   }
-  mn = block_min_u32(mn, red);
-  if (threadIdx.x == 0 && mn != kInfBits) atomicMin(&d.ctrl->mins[(s + 1u) % 3u], mn);
+  mn = warp_min_u32(mn);
+  if ((threadIdx.x & 31u) == 0 && mn != kInfBits) atomicMin(&red[0], mn);  // the CTA's minimum (kInfBits: none)
 }
 
 // LPs a CTA of `block` threads covers in one launch of the plain form.
@@ -1009,7 +1010,11 @@ static __global__ void __launch_bounds__(1024, 1) lab_window_kernel(PholdDev d, 
   }
   const uint32_t per = (blockDim.x / 32u) * q.chunk;  // a shard works its own LPs [lp_begin, lp_end)
   const uint32_t lp_lo = min(d.lp_end, d.lp_begin + blockIdx.x * per), lp_hi = min(d.lp_end, lp_lo + per);
+  if (threadIdx.x == 0) red[0] = kInfBits;
+  __syncthreads();
   lab_window_body<kShard>(d, q, s, m, ld_relaxed_u32(&q.wj[(s + 3u) & 3u]), smem_raw, red, lp_lo, lp_hi, false);
+  __syncthreads();
+  if (threadIdx.x == 0 && red[0] != kInfBits) atomicMin(&d.ctrl->mins[(s + 1u) % 3u], red[0]);
 }
 
 // Persistent form: all windows in one cooperative launch, a bounded grid barrier per window.
@@ -1025,6 +1030,8 @@ static __global__ void __launch_bounds__(1024, 1) lab_persistent_kernel(PholdDev
   const bool resident = (per + nw - 1u) / nw <= q.chunk;
   const LabWarpSmem sm = lab_warp_smem(smem_raw + (size_t)warp * lab_warp_smem_bytes());
   if (resident) lab_state_load(d, sm, wlo, whi - wlo);
+  if (threadIdx.x == 0) red[0] = kInfBits;  // the CTA's part of the next window's minimum
+  __syncthreads();
   unsigned long long target = 0;
   uint32_t s = s0;
   // j1 of the previous window: read once, then carried in registers (every CTA computes
@@ -1045,7 +1052,7 @@ static __global__ void __launch_bounds__(1024, 1) lab_persistent_kernel(PholdDev
     lab_window_body<false>(d, q, s, m, j1p, smem_raw, red, lp_lo, lp_hi, resident);
     j1p = j1;
     target += gridDim.x;
-    if (!grid_barrier(&d.ctrl->bar, target, d.spin_limit, &d.ctrl->err)) {
+    if (!grid_barrier_min(&d.ctrl->bar, target, d.spin_limit, &d.ctrl->err, &red[0], &d.ctrl->mins[(s + 1u) % 3u])) {
       s += 1u;
       break;
     }
