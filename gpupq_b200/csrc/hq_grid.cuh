@@ -201,17 +201,18 @@ __device__ __forceinline__ uint32_t hqg_split(const typename Ops::T* XA, uint32_
   return lo;
 }
 
-// Outputs [dg, dg + kPer) of merge(A, B) (A, B as above; fewer at the end) to out(k, v),
-// k = 0, 1, ...  The two heads are kept in registers: one shared-memory load per output.
+// Outputs [dg, dg + per) of merge(A, B) (A, B as above; fewer at the end; per defaults to
+// kPer) to out(k, v), k = 0, 1, ...  The two heads are kept in registers: one shared-memory
+// load per output.
 template <class Ops, class Out>
 __device__ __forceinline__ void hqg_merge_run(const typename Ops::T* XA, uint32_t aoff, uint32_t na,
                                               const typename Ops::T* XB, uint32_t boff, uint32_t nb, uint32_t dg,
-                                              Out out) {
+                                              Out out, uint32_t per = Ops::kPer) {
   using T = typename Ops::T;
   uint32_t ia = hqg_split<Ops>(XA, aoff, na, XB, boff, nb, dg), ib = dg - ia;
   T a = ia < na ? XA[hqg_pad<Ops>(aoff + ia)] : Ops::maxv();
   T b = ib < nb ? XB[hqg_pad<Ops>(boff + ib)] : Ops::maxv();
-  const uint32_t n = min(Ops::kPer, na + nb - dg);
+  const uint32_t n = min(per, na + nb - dg);
   for (uint32_t k = 0; k < n; ++k) {
     const bool take_a = ib >= nb || (ia < na && !Ops::less(b, a));
     if (take_a) {
@@ -1220,8 +1221,12 @@ __device__ bool hqg_insert_lists(const HqgDev& g, HqgState& q, uint32_t nch, uin
         if (t + 2 < tcnt) issue(tt + 2, stg[(t + 2) % 3]); else hqg_cp_commit();  // read in the last round
         const uint32_t tn = min(kStreamTile, nrb - t0), chi = chis[t], cn = chi - cpos, total = tn + cn;
         gpq_item* dst = out + base + t0 + cpos;
-        for (uint32_t o0 = threadIdx.x * kHqgIpt; o0 < total; o0 += blockDim.x * kHqgIpt)
-          hqg_merge_run<HqgItemOps>(Yh, 0, tn, X, cpos, cn, o0, [&](uint32_t k, const gpq_item& v) { dst[o0 + k] = v; });
+        // every thread one run of about total / blockDim outputs (at most kHqgIpt, the
+        // padding's stride, so the lanes' heads stay in different bank groups)
+        const uint32_t per = min(kHqgIpt, (total + blockDim.x - 1u) / blockDim.x);
+        for (uint32_t o0 = threadIdx.x * per; o0 < total; o0 += blockDim.x * per)
+          hqg_merge_run<HqgItemOps>(Yh, 0, tn, X, cpos, cn, o0, [&](uint32_t k, const gpq_item& v) { dst[o0 + k] = v; },
+                                    per);
         cpos = chi;
       }
       hqg_cp_wait<0>();
