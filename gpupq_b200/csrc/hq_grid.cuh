@@ -1135,16 +1135,55 @@ __device__ void hqg_process_lists(const PholdDev& d, const HqgDev& g, const gpq_
   hqg_bar(s);
 }
 
+// The items root[lo, hi) filed into BP LP-range lists (counts pc, zero before the window)
+// for hqg_process_lists: the CTA counts its keys per range in shared memory, reserves each
+// range's share with one atomic and writes them.
+__device__ void hqg_file_range(const HqgDev& g, const gpq_item* root, uint32_t lo, uint32_t hi, uint32_t BP,
+                               uint32_t* pc, uint32_t L, uint32_t* aux) {
+  __shared__ uint32_t s_pb[kHqgMaxBuckets];
+  for (uint32_t p0 = lo; p0 < hi; p0 += kHqgAux) {
+    const uint32_t pn = min(kHqgAux, hi - p0);
+    for (uint32_t k = threadIdx.x; k < BP; k += blockDim.x) s_pb[k] = 0u;
+    __syncthreads();
+    for (uint32_t p = threadIdx.x; p < pn; p += blockDim.x) {
+      const uint32_t bk = hqg_lp_bucket(root[p0 + p].lp, BP, L);
+      aux[p] = (bk << 16) | atomicAdd(&s_pb[bk], 1u);
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < BP; k += blockDim.x) s_pb[k] = s_pb[k] ? atomicAdd(&pc[k], s_pb[k]) : 0u;
+    __syncthreads();
+    for (uint32_t p = threadIdx.x; p < pn; p += blockDim.x) {
+      const uint32_t sv = aux[p], bk = sv >> 16, slot = s_pb[bk] + (sv & 0xffffu);
+      if (slot < kHqgListCapP) g.plist[(size_t)bk * kHqgListCapP + slot] = ((unsigned long long)root[p0 + p].lp << 32) | (p0 + p);
+    }
+    __syncthreads();
+  }
+}
+
 // The children of the last batch, filed in BI insert lists (this window's counts ic), into
 // the root (all of whose items stay: R = root[off, off + cnt0)): CTA b sorts its list in
 // shared memory and streams R's slice b past it -- an R item lands at (slice start +
 // children below the slice + its index + children below it), the children between two R
 // items right after the first -- into the root's other buffer.  Returns false, with
 // nothing written, when a list overflowed.
+//
+// pre.on: the next window's batch is also filed into its LP-range lists (pre.BP ranges,
+// counts pre.pc) here, so that the window needs no filing phase: the new root's head is the
+// smaller of R's head and the smallest child (in the first non-empty list), which fixes the
+// window's bound; each CTA's outputs below it are a prefix of its output range, filed by
+// that CTA after its merge.
+struct HqgPre {
+  bool on;
+  float la, T;   // lookahead and end time: the bound is min(head + la, T)
+  uint32_t BP;   // LP ranges
+  uint32_t* pc;  // their counts (zeroed before the window)
+};
+
 __device__ bool hqg_insert_lists(const HqgDev& g, HqgState& q, uint32_t nch, uint32_t BI, const uint32_t* ic,
-                                 uint32_t L, unsigned char* smem, HqgSync& s) {
+                                 uint32_t L, const HqgPre& pre, unsigned char* smem, HqgSync& s) {
   __shared__ uint32_t s_pre[kHqgMaxBuckets + 1];
   __shared__ int s_ovf;
+  __shared__ uint32_t s_b0, s_red[32];
   uint32_t* aux = hqg_aux(smem);
   const gpq_item* R = q.root + q.off;
   const uint32_t nr = q.cnt0;
@@ -1164,6 +1203,23 @@ __device__ bool hqg_insert_lists(const HqgDev& g, HqgState& q, uint32_t nch, uin
   }
   __syncthreads();
   if (s_ovf) return false;  // the same decision in every block: nothing written
+  uint32_t lim = 0;  // pre.on: the next window's bound (ts bits), the same in every block
+  if (pre.on) {
+    if (threadIdx.x == 0) {
+      uint32_t b0 = BI;
+      for (uint32_t k = 0; k < BI && b0 == BI; ++k)
+        if (s_pre[k + 1] > s_pre[k]) b0 = k;
+      s_b0 = b0;
+    }
+    __syncthreads();
+    uint32_t mn = (threadIdx.x == 0 && nr > 0) ? gpq_f2u(R[0].ts) : kInfBits;
+    if (s_b0 < BI) {
+      const gpq_item* l0 = g.ilist + (size_t)s_b0 * kHqgListCapI;
+      for (uint32_t j = threadIdx.x; j < s_pre[s_b0 + 1] - s_pre[s_b0]; j += blockDim.x) mn = min(mn, gpq_f2u(l0[j].ts));
+    }
+    mn = block_min_u32(mn, s_red);
+    lim = min(gpq_f2u(GPQ_FADD(gpq_u2f(mn), pre.la)), gpq_f2u(pre.T));
+  }
   gpq_item* sa = reinterpret_cast<gpq_item*>(smem);
   gpq_item* sb = sa + hqg_tile_cap<HqgItemOps>();
   gpq_item* out = q.spare;
@@ -1234,6 +1290,12 @@ __device__ bool hqg_insert_lists(const HqgDev& g, HqgState& q, uint32_t nch, uin
     }
     for (uint32_t j = cpos + threadIdx.x; j < nc; j += blockDim.x) out[base + nrb + j] = X[hqg_pad<HqgItemOps>(j)];
     __syncthreads();
+    if (pre.on) {  // this CTA's outputs below the bound: R's and the children's below it
+      const uint32_t nR = hqg_cta_search(0, nrb, [R, r0, lim](uint32_t i) { return gpq_f2u(R[r0 + i].ts) >= lim; });
+      const uint32_t nX =
+          hqg_cta_search(0, nc, [X, lim](uint32_t i) { return gpq_f2u(X[hqg_pad<HqgItemOps>(i)].ts) >= lim; });
+      hqg_file_range(g, out, base, base + nR + nX, pre.BP, pre.pc, L, aux);
+    }
   }
   if (!hqg_bar(s)) return false;
   q.swap_root();
@@ -1241,34 +1303,12 @@ __device__ bool hqg_insert_lists(const HqgDev& g, HqgState& q, uint32_t nch, uin
   return true;
 }
 
-// The batch root[0, c) filed into BP LP-range lists (counts pc, zero on entry) for
-// hqg_process_lists: each CTA takes an equal slice of the batch, counts its keys per range
-// in shared memory, reserves each range's share with one atomic and writes them.  Ends
-// with a barrier.
+// hqg_file_range over equal slices of the batch root[0, c), one per CTA; ends with a barrier.
 __device__ void hqg_file_batch(const PholdDev& d, const HqgDev& g, const gpq_item* root, uint32_t c, uint32_t BP,
                                uint32_t* pc, unsigned char* smem, HqgSync& s) {
-  __shared__ uint32_t s_pb[kHqgMaxBuckets];
-  uint32_t* aux = hqg_aux(smem);
-  const uint32_t L = d.L;
   const uint32_t per = (c + gridDim.x - 1) / gridDim.x;
   const uint32_t lo = min(c, blockIdx.x * per), hi = min(c, lo + per);
-  for (uint32_t p0 = lo; p0 < hi; p0 += kHqgAux) {
-    const uint32_t pn = min(kHqgAux, hi - p0);
-    for (uint32_t k = threadIdx.x; k < BP; k += blockDim.x) s_pb[k] = 0u;
-    __syncthreads();
-    for (uint32_t p = threadIdx.x; p < pn; p += blockDim.x) {
-      const uint32_t bk = hqg_lp_bucket(root[p0 + p].lp, BP, L);
-      aux[p] = (bk << 16) | atomicAdd(&s_pb[bk], 1u);
-    }
-    __syncthreads();
-    for (uint32_t k = threadIdx.x; k < BP; k += blockDim.x) s_pb[k] = s_pb[k] ? atomicAdd(&pc[k], s_pb[k]) : 0u;
-    __syncthreads();
-    for (uint32_t p = threadIdx.x; p < pn; p += blockDim.x) {
-      const uint32_t sv = aux[p], bk = sv >> 16, slot = s_pb[bk] + (sv & 0xffffu);
-      if (slot < kHqgListCapP) g.plist[(size_t)bk * kHqgListCapP + slot] = ((unsigned long long)root[p0 + p].lp << 32) | (p0 + p);
-    }
-    __syncthreads();
-  }
+  hqg_file_range(g, root, lo, hi, BP, pc, d.L, hqg_aux(smem));
   hqg_bar(s);
 }
 
@@ -1292,6 +1332,9 @@ static __global__ void __launch_bounds__(kHqgThreads, 1) hqg_phold_kernel(PholdD
   q.cnt0 = h.cnt[0];
   q.cntl = q.last > 0 ? h.cnt[q.last] : 0u;
   uint32_t steps = 0, nch = 0, ovf_seen = 0;
+  uint32_t c_last = 0;    // size of the last batch
+  bool prefiled = false;  // this window's batch was filed by the insert phase (pre_bp ranges)
+  uint32_t pre_bp = 0;
   HqgLists lists{false, 0u};
   __shared__ gpq_item s_spl[kHqgMaxBuckets];
   __shared__ uint32_t s_pc[kHqgMaxBuckets];
@@ -1304,8 +1347,18 @@ static __global__ void __launch_bounds__(kHqgThreads, 1) hqg_phold_kernel(PholdD
         for (uint32_t k = threadIdx.x; k < kHqgMaxBuckets; k += blockDim.x)
           g.icnt[((steps + 1u) & 1u) * kHqgMaxBuckets + k] = 0u;
       if (lists.ins) {
-        done = hqg_insert_lists(g, q, nch, lists.BI, g.icnt + (steps & 1u) * kHqgMaxBuckets, d.L, smem, s);
+        // a batch of a large share of the root (C1-like windows) is filed while the children
+        // are merged; a small one (a long array) is filed by equal slices in a phase of its own
+        HqgPre pre{};
+        pre.on = g.plist != nullptr && q.last == 0 && 4ull * c_last >= (uint64_t)q.cnt0 + nch;
+        pre.la = d.p.lookahead;
+        pre.T = d.p.end_time;
+        pre.BP = min(gridDim.x, max(1u, c_last / 64u));
+        pre.pc = g.pcnt + ((steps + 1u) & 1u) * kHqgMaxBuckets;
+        done = hqg_insert_lists(g, q, nch, lists.BI, g.icnt + (steps & 1u) * kHqgMaxBuckets, d.L, pre, smem, s);
         if (!s.ok) break;
+        prefiled = done && pre.on;
+        pre_bp = pre.BP;
       }
       lists.ins = false;
       if (!done) {
@@ -1328,6 +1381,8 @@ static __global__ void __launch_bounds__(kHqgThreads, 1) hqg_phold_kernel(PholdD
     while (s.ok) {  // batches of the window
       const gpq_item* root = q.root + q.off;
       const uint32_t c = hqg_cta_search(0, q.cnt0, [root, lim](uint32_t i) { return gpq_f2u(root[i].ts) >= lim; });
+      const bool use_pre = prefiled;  // only the window's first batch
+      prefiled = false;
       if (c == 0) break;
       // LP-range lists for the batch (a heap whose root holds every item; other heaps scan
       // the batch in each CTA or take the general path)
@@ -1338,9 +1393,13 @@ static __global__ void __launch_bounds__(kHqgThreads, 1) hqg_phold_kernel(PholdD
           g.pcnt[((steps + 1u) & 1u) * kHqgMaxBuckets + k] = 0u;
       if (g.plist != nullptr && q.last == 0) {  // the root holds every item: file the batch
         uint32_t* pc = g.pcnt + (steps & 1u) * kHqgMaxBuckets;
-        BP = min(gridDim.x, max(1u, c / 64u));
-        hqg_file_batch(d, g, root, c, BP, pc, smem, s);
-        if (!s.ok) break;
+        if (use_pre) {  // filed by the insert phase
+          BP = pre_bp;
+        } else {
+          BP = min(gridDim.x, max(1u, c / 64u));
+          hqg_file_batch(d, g, root, c, BP, pc, smem, s);
+          if (!s.ok) break;
+        }
         for (uint32_t k = threadIdx.x; k < BP; k += blockDim.x) s_pc[k] = ld_relaxed_u32(&pc[k]);
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -1398,6 +1457,7 @@ static __global__ void __launch_bounds__(kHqgThreads, 1) hqg_phold_kernel(PholdD
       }
       lists.ins = ins.on;
       lists.BI = ins.BI;
+      c_last = c;
       nch += c;
       q.off += c;
       q.cnt0 -= c;
