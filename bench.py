@@ -636,8 +636,9 @@ def run_case(name):
                 r = a.solve(q)
             print(a.stats(), int(r["expanded"].sum()), int(r["pops"].sum()), int((r["status"] != 0).sum()))
     elif name == "astar_plain_2048":
+        # the bench line's tuned shape: 1,024 shards of 64 x 64, f-window 1, one CTA per SM
         g = G.astar_grid(2048, 2048, 0.2, 3)
-        with G.AStar(tile=64) as a:
+        with G.AStar(tile=64, window=1, ctas_per_sm=1) as a:
             for _ in range(2):
                 r = a.solve(g)
             print(a.stats(), int(r[0]["expanded"]))
