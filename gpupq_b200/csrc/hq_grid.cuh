@@ -1235,7 +1235,7 @@ __device__ bool hqg_insert_lists(const HqgDev& g, HqgState& q, uint32_t nch, uin
     // R's slice in tiles of kStreamTile, copied into shared memory asynchronously two tiles
     // ahead (three staging buffers: the two halves of the free tile and the auxiliary
     // area); each tile merged with the children between its first item and the next tile's
-    // (merge path, kHqgIpt outputs a thread).  chis[t]: the children below tile t + 1's
+    // (merge path, an equal run of outputs a thread).  chis[t]: the children below tile t + 1's
     // first item, for all tiles at once.
     constexpr uint32_t kStreamTile = 2048;
     constexpr uint32_t kHalf = kStreamTile + kStreamTile / kHqgIpt;  // a padded tile
