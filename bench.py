@@ -684,10 +684,13 @@ def run_case(name):
             for _ in range(2):
                 r = a.solve(m, agents)
             print(a.last_ms(), int(r["pops"].sum()))
-    elif name == "phold_batched_36":
+    elif name in ("phold_batched_36", "phold_batched_36_buckets"):
+        # the PHOLD runs among the first 0.1 s of the served stream, in a sorted-ring session
+        # or (..._buckets) in a time-bucket session
         reqs, n = G.serve_stream(99, 2000.0, 0.1)
         runs = [reqs[i].phold for i in range(n) if reqs[i].kind == G.REQ_PHOLD][:40]
-        with G.PholdSession(max_lps=sum(r.num_lps for r in runs), max_instances=len(runs)) as s:
+        with G.PholdSession(max_lps=sum(r.num_lps for r in runs), max_instances=len(runs),
+                            bucketed=name.endswith("_buckets")) as s:
             for _ in range(2):
                 for r in runs:
                     s.admit(r)
@@ -718,7 +721,8 @@ def main():
     ap.add_argument("--no-forms", action="store_true", help="skip the A*, batched and served sections")
     ap.add_argument("--served-seconds", type=float, default=1.0, help="length of the served request stream")
     ap.add_argument("--case", default=None,
-                    choices=["astar_batched_1000", "astar_plain_2048", "phold_batched_36", "gaq_sort_32m",
+                    choices=["astar_batched_1000", "astar_plain_2048", "phold_batched_36", "phold_batched_36_buckets",
+                             "gaq_sort_32m",
                              "astar_ref_2048", "phold_c1_heap", "gaq_array_c2_t20"],
                     help="run one small named workload twice and exit (profiling captures)")
     args = ap.parse_args()
