@@ -684,6 +684,15 @@ def run_case(name):
             for _ in range(2):
                 r = a.solve(m, agents)
             print(a.last_ms(), int(r["pops"].sum()))
+    elif name == "served_held_rates":
+        # the served mix at offered rates one B200 holds, over longer streams
+        import json
+        for rate, secs in ((600.0, 30.0), (800.0, 20.0)):
+            reqs, n = G.serve_stream(99, rate, secs)
+            out, st = G.serve(reqs, n, mode=G.SERVE_BATCHED, realtime=True, budget=120 << 30, tile=64)
+            bad = sum(1 for i in range(n) if out[i].status != 0)
+            print(json.dumps({"offered_rate": rate, "seconds": secs, "requests": n, "bad_status": bad,
+                              **{k: (round(v, 4) if isinstance(v, float) else v) for k, v in st.items()}}))
     elif name in ("phold_batched_36", "phold_batched_36_buckets"):
         # the PHOLD runs among the first 0.1 s of the served stream, in a sorted-ring session
         # or (..._buckets) in a time-bucket session
@@ -723,7 +732,7 @@ def main():
     ap.add_argument("--case", default=None,
                     choices=["astar_batched_1000", "astar_plain_2048", "phold_batched_36", "phold_batched_36_buckets",
                              "gaq_sort_32m",
-                             "astar_ref_2048", "phold_c1_heap", "gaq_array_c2_t20"],
+                             "astar_ref_2048", "phold_c1_heap", "gaq_array_c2_t20", "served_held_rates"],
                     help="run one small named workload twice and exit (profiling captures)")
     args = ap.parse_args()
     if args.case:
