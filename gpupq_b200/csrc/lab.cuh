@@ -694,6 +694,11 @@ __device__ __forceinline__ unsigned long long lab_load_cand(const LabCtx& x, con
   return q.spill[((size_t)w.prevb * x.L + lp) * q.F + i];
 }
 
+// y / d for the small operands of a warp chunk (y < 2^16 / d): inv = ceil(2^16 / d), and
+// the error of the scaled reciprocal, below y / 2^16 < 1 / d, never reaches the next integer.
+__device__ __forceinline__ uint32_t lab_recip16(uint32_t d) { return (65536u + d - 1u) / d; }
+__device__ __forceinline__ uint32_t lab_div16(uint32_t y, uint32_t inv) { return (y * inv) >> 16; }
+
 // One window for the chunk [lp0, lp0 + n) of one warp (outputs in sm.ls_*).  Returns this
 // lane's part of the chunk minimum (LP next minima and children).  All lanes of the warp.
 template <bool kShard = false>
@@ -732,8 +737,9 @@ static __device__ uint32_t lab_warp_window(const LabCtx& x, const LabDev& q, con
   uint32_t K = 0xffffffffu;
   if (S <= kLabSegMax) {
     // P1: range-bucket and spill counts, and the counts of the two buckets above j1
+    const uint32_t inv2 = lab_recip16(S + 2u);
     for (uint32_t y = lane; y < n * (S + 2u); y += 32u) {
-      const uint32_t lpi = y / (S + 2u), r = y - lpi * (S + 2u), lp = lp0 + lpi;
+      const uint32_t lpi = lab_div16(y, inv2), r = y - lpi * (S + 2u), lp = lp0 + lpi;
       if (r < S) {
         uint32_t raw, c;
         if (r < nr) {
@@ -762,8 +768,9 @@ static __device__ uint32_t lab_warp_window(const LabCtx& x, const LabDev& q, con
   if (K <= kLabCandCap) {
     // the source of every candidate slot: each (LP, source) segment writes its code
     // (LP index << 3 | source) over its slots
+    const uint32_t invs = lab_recip16(S);
     for (uint32_t y = lane; y < n * S; y += 32u) {
-      const uint32_t a = sm.seg_off[y], b = sm.seg_off[y + 1u], lpi = y / S;
+      const uint32_t a = sm.seg_off[y], b = sm.seg_off[y + 1u], lpi = lab_div16(y, invs);
       const uint16_t code = (uint16_t)((lpi << 3) | (y - lpi * S));
       for (uint32_t k = a; k < b; ++k) sm.cseg[k] = code;
     }
@@ -842,12 +849,24 @@ static __device__ uint32_t lab_warp_window(const LabCtx& x, const LabDev& q, con
     __syncwarp();
     const uint32_t nsafe = lab_warp_scan(sm.lp_soff, n);
     if (lane == 0) sm.misc[0] = nsafe;
+    // LP of every staging position below kLabStageCap (a byte map in seg_kept, free after P5)
+    uint8_t* spl = reinterpret_cast<uint8_t*>(sm.seg_kept);
+    static_assert(kLabWarpLps * kLabSegMax * 4 >= kLabStageCap && kLabWarpLps <= 256, "staging map");
+    if (lane < n) {
+      const uint32_t e = min(sm.lp_soff[lane + 1u], kLabStageCap);
+      for (uint32_t u = sm.lp_soff[lane]; u < e; ++u) spl[u] = (uint8_t)lane;
+    }
+    __syncwarp();
     // P6: rank each safe key among its LP's safe keys and stage it at (LP offset + rank)
     for (uint32_t u = lane; u < nsafe; u += 32u) {
       uint32_t lo = 0, hi = n;  // LP: lp_soff[lo] <= u < lp_soff[lo + 1]
-      while (hi - lo > 1u) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (sm.lp_soff[mid] <= u) lo = mid; else hi = mid;
+      if (u < kLabStageCap) {
+        lo = spl[u];
+      } else {
+        while (hi - lo > 1u) {
+          const uint32_t mid = (lo + hi) >> 1;
+          if (sm.lp_soff[mid] <= u) lo = mid; else hi = mid;
+        }
       }
       const uint16_t* li = sm.sidx + lo * kLabSafePerLp;
       const uint32_t ns_lp = sm.lp_nsafe[lo];
