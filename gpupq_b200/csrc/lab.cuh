@@ -473,12 +473,13 @@ static constexpr uint32_t kLabCandCap = 256;   // candidate keys per warp chunk 
 static constexpr uint32_t kLabStageCap = 128;  // staged events per warp chunk (4-byte entries)
 static constexpr uint32_t kLabSafePerLp = 32;  // safe keys of one LP ranked on the common path
 static constexpr uint32_t kLabItemStageCap = kLabStageCap * 4 / 16;  // staged items on the general path
+static_assert(kLabCandCap <= 256 && kLabSafePerLp <= 256 && kLabWarpLps <= 65536, "staging entry fields");
 
 struct LabWarpSmem {
   unsigned long long* ls_csum;   // [kLabWarpLps] LP checksum
   unsigned long long* ls_ohash;  // [kLabWarpLps] LP order-sensitive hash
   unsigned long long* cand;      // [kLabCandCap] candidate keys (general path: the safe-key list)
-  uint32_t* cstage;              // [kLabStageCap] staged events: candidate index | rank << 16
+  uint32_t* cstage;              // [kLabStageCap] staged events: candidate index | rank << 8 | LP index << 16
   gpq_item* stage;               // [kLabItemStageCap] staged items on the general path (same bytes as cstage)
   uint32_t* ls_cnt;              // [kLabWarpLps] LP committed count (before the window: the sequence base)
   uint32_t* seg_raw;             // [kLabWarpLps * kLabSegMax] bucket count / spill count as read
@@ -873,10 +874,11 @@ static __device__ uint32_t lab_warp_window(const LabCtx& x, const LabDev& q, con
       const uint32_t k = li[u - sm.lp_soff[lo]];
       const unsigned long long key = sm.cand[k];
       uint32_t rank = 0;
+#pragma unroll 4  // the keys' loads overlap
       for (uint32_t y = 0; y < ns_lp; ++y) rank += (sm.cand[li[y]] < key) ? 1u : 0u;
       const uint32_t pos = sm.lp_soff[lo] + rank;
       if (pos < kLabStageCap) {
-        sm.cstage[pos] = k | (rank << 16);
+        sm.cstage[pos] = k | (rank << 8) | (lo << 16);
       } else {
         gpq_item e;
         e.ts = gpq_u2f((uint32_t)(key >> 32));
@@ -929,13 +931,13 @@ static __device__ uint32_t lab_warp_window(const LabCtx& x, const LabDev& q, con
   if (common) {
     const uint32_t ns = min(sm.misc[0], kLabStageCap);
     auto get = [&](uint32_t y) {
-      const uint32_t c = sm.cstage[y], k = c & 0xffffu;
-      const unsigned long long key = sm.cand[k];
+      const uint32_t c = sm.cstage[y], lpi = c >> 16;
+      const unsigned long long key = sm.cand[c & 0xffu];
       gpq_item e;
       e.ts = gpq_u2f((uint32_t)(key >> 32));
-      e.lp = lp0 + (sm.cseg[k] >> 3);
+      e.lp = lp0 + lpi;
       e.id = (uint32_t)key;
-      e.aux = ((uint32_t)(sm.cseg[k] >> 3) << 16) | (c >> 16);
+      e.aux = (lpi << 16) | ((c >> 8) & 0xffu);
       return e;
     };
     for (uint32_t x0 = lane; x0 < ns; x0 += 128u) mn = min(mn, lab_event_batch<kShard>(x, q, st, ns, x0, 32u, w, get));
