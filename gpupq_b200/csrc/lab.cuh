@@ -798,6 +798,7 @@ static __device__ uint32_t lab_warp_window(const LabCtx& x, const LabDev& q, con
     __syncwarp();
     // P4a (read-only): safe candidates into their LP's list; the minimum and the "stays at
     // or below j1" flag of each LP
+#pragma unroll 4
     for (uint32_t k = lane; k < K; k += 32u) {
       const uint32_t sg = sm.cseg[k], lpi = sg >> 3, r = sg & 7u;
       const uint32_t t = (uint32_t)(sm.cand[k] >> 32);
