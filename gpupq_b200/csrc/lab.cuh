@@ -737,27 +737,40 @@ static __device__ uint32_t lab_warp_window(const LabCtx& x, const LabDev& q, con
 
   uint32_t K = 0xffffffffu;
   if (S <= kLabSegMax) {
-    // P1: range-bucket and spill counts, and the counts of the two buckets above j1
-    const uint32_t inv2 = lab_recip16(S + 2u);
-    for (uint32_t y = lane; y < n * (S + 2u); y += 32u) {
-      const uint32_t lpi = lab_div16(y, inv2), r = y - lpi * (S + 2u), lp = lp0 + lpi;
-      if (r < S) {
-        uint32_t raw, c;
+    // P1: range-bucket and spill counts, and the counts of the two buckets above j1 (every
+    // load of a lane issued before any of its stores, so that they are in flight together)
+    const uint32_t inv2 = lab_recip16(S + 2u), ny = n * (S + 2u);
+    constexpr uint32_t kP1 = (kLabWarpLps * (kLabSegMax + 2u) + 31u) / 32u;
+    uint32_t raw[kP1];
+#pragma unroll
+    for (uint32_t u = 0; u < kP1; ++u) {
+      const uint32_t y = lane + 32u * u;
+      raw[u] = 0u;
+      if (y < ny) {
+        const uint32_t lpi = lab_div16(y, inv2), r = y - lpi * (S + 2u), lp = lp0 + lpi;
         if (r < nr) {
-          raw = ld_relaxed_u32(&q.cnt[((size_t)lp << q.nb_log2) + ((w.j0 + r) & nbm)]);
-          c = min(raw, C);
+          raw[u] = ld_relaxed_u32(&q.cnt[((size_t)lp << q.nb_log2) + ((w.j0 + r) & nbm)]);
+        } else if (r == nr) {
+          raw[u] = q.scnt[(size_t)w.prevb * L + lp];
         } else {
-          raw = q.scnt[(size_t)w.prevb * L + lp];
-          c = min(raw, q.F);
+          const uint32_t j = w.j1 + 1u + (r - S);
+          if (j - w.j0 < NB) raw[u] = ld_relaxed_u32(&q.cnt[((size_t)lp << q.nb_log2) + (j & nbm)]);
         }
-        const uint32_t y = lpi * S + r;
-        sm.seg_raw[y] = raw;
-        sm.seg_off[y] = c;
-        sm.seg_kept[y] = 0u;
-      } else {
-        const uint32_t j = w.j1 + 1u + (r - S);
-        sm.nx_cnt[lpi * 2u + (r - S)] =
-            (j - w.j0 < NB) ? min(ld_relaxed_u32(&q.cnt[((size_t)lp << q.nb_log2) + (j & nbm)]), C) : 0u;
+      }
+    }
+#pragma unroll
+    for (uint32_t u = 0; u < kP1; ++u) {
+      const uint32_t y = lane + 32u * u;
+      if (y < ny) {
+        const uint32_t lpi = lab_div16(y, inv2), r = y - lpi * (S + 2u);
+        if (r < S) {
+          const uint32_t ys = lpi * S + r;
+          sm.seg_raw[ys] = raw[u];
+          sm.seg_off[ys] = min(raw[u], r < nr ? C : q.F);
+          sm.seg_kept[ys] = 0u;
+        } else {
+          sm.nx_cnt[lpi * 2u + (r - S)] = min(raw[u], C);
+        }
       }
     }
     __syncwarp();
