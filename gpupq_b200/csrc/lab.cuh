@@ -780,17 +780,17 @@ static __device__ uint32_t lab_warp_window(const LabCtx& x, const LabDev& q, con
 
   uint32_t scan_min = kInfBits, scan_lpi = ~0u;
   if (K <= kLabCandCap) {
-    // the source of every candidate slot: each (LP, source) segment writes its code
-    // (LP index << 3 | source) over its slots
-    const uint32_t invs = lab_recip16(S);
-    for (uint32_t y = lane; y < n * S; y += 32u) {
-      const uint32_t a = sm.seg_off[y], b = sm.seg_off[y + 1u], lpi = lab_div16(y, invs);
-      const uint16_t code = (uint16_t)((lpi << 3) | (y - lpi * S));
-      for (uint32_t k = a; k < b; ++k) sm.cseg[k] = code;
-    }
-    __syncwarp();
-    // P3: candidate keys, up to 8 per lane, all loads in flight together
-    {
+    if (q.c_log2 <= 4u) {
+      // buckets of at most 16 slots: each (LP, source) segment writes its code (LP index << 3 |
+      // source) over its candidate slots, and the candidate loads read it
+      const uint32_t invs = lab_recip16(S);
+      for (uint32_t y = lane; y < n * S; y += 32u) {
+        const uint32_t a = sm.seg_off[y], b = sm.seg_off[y + 1u], lpi = lab_div16(y, invs);
+        const uint16_t code = (uint16_t)((lpi << 3) | (y - lpi * S));
+        for (uint32_t k = a; k < b; ++k) sm.cseg[k] = code;
+      }
+      __syncwarp();
+      // P3: candidate keys, up to 8 per lane, all loads in flight together
       constexpr uint32_t U = kLabCandCap / 32u;
       unsigned long long v[U];
 #pragma unroll
@@ -806,6 +806,37 @@ static __device__ uint32_t lab_warp_window(const LabCtx& x, const LabDev& q, con
       for (uint32_t u = 0; u < U; ++u) {
         const uint32_t k = lane + 32u * u;
         if (k < K) sm.cand[k] = v[u];
+      }
+    } else {
+      // larger buckets (long segments, few LPs a chunk): each candidate finds its segment
+      // by a search next to its load
+      constexpr uint32_t U = kLabCandCap / 32u;
+      unsigned long long v[U];
+      uint32_t sg[U];
+#pragma unroll
+      for (uint32_t u = 0; u < U; ++u) {
+        const uint32_t k = lane + 32u * u;
+        sg[u] = ~0u;
+        v[u] = 0;
+        if (k < K) {
+          uint32_t lo = 0, hi = n;  // LP: seg_off[lo * S] <= k < seg_off[hi * S]
+          while (hi - lo > 1u) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (sm.seg_off[mid * S] <= k) lo = mid; else hi = mid;
+          }
+          uint32_t r = 0;
+          while (r + 1u < S && sm.seg_off[lo * S + r + 1u] <= k) ++r;
+          sg[u] = (lo << 3) | r;
+          v[u] = lab_load_cand(x, q, w, nr, lp0 + lo, r, k - sm.seg_off[lo * S + r]);
+        }
+      }
+#pragma unroll
+      for (uint32_t u = 0; u < U; ++u) {
+        if (sg[u] != ~0u) {
+          const uint32_t k = lane + 32u * u;
+          sm.cand[k] = v[u];
+          sm.cseg[k] = (uint16_t)sg[u];
+        }
       }
     }
     __syncwarp();
